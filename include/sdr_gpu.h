@@ -1,0 +1,255 @@
+/*
+ * sdr_gpu.h — C ABI of the B200 (sm_100a) FLIP/PIC substep of uselessgoddess/sdr.
+ *
+ * This is the drop-in boundary: every entry point replaces one piece of the
+ * reference's Rust API (paths are within the reference project). A Rust
+ * `extern "C"` block binds these one to one.
+ *
+ * Conventions
+ *  - Opaque handles, created and destroyed explicitly by the caller.
+ *  - Every call returns an int status (SDR_OK = 0). No exceptions or longjmp
+ *    cross this boundary. sdr_last_error() returns a thread-local message for
+ *    the most recent failure on the calling thread.
+ *  - All buffers are host memory owned by the caller; outputs are copied into
+ *    them. No torch, CUDA or C++ types appear in the signatures.
+ *  - One solver handle per host thread at a time; calls on one handle are not
+ *    re-entrant. Each handle owns its CUDA stream on the current device.
+ *  - Units are SI (metres, seconds, m^3/s), like the reference's Solver.
+ */
+#ifndef SDR_GPU_H
+#define SDR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDR_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+    SDR_OK = 0,
+    SDR_ERR_INVALID = 1,        /* bad argument (null pointer, size mismatch, bad params) */
+    SDR_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    SDR_ERR_OOM = 3,            /* device allocation failed */
+    SDR_ERR_CAPACITY = 4,       /* particle or work-list capacity exceeded */
+    SDR_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+    SDR_ERR_NO_DEVICE = 6,      /* no CUDA device or the library was built for another arch */
+    SDR_ERR_BUFFER = 7          /* caller buffer too small; required size reported */
+};
+
+/* Cell labels (src/pressure.rs:24-32). */
+enum { SDR_CELL_SOLID = 0, SDR_CELL_FLUID = 1, SDR_CELL_AIR = 2 };
+
+typedef struct { double x, y, z; } sdr_vec3;
+typedef struct { sdr_vec3 min, max; } sdr_aabb; /* Aabb, src/math.rs:198-257 */
+
+/* FluidParams, src/solver.rs:41-71. */
+typedef struct {
+    double density;
+    sdr_vec3 gravity;
+    double flip_ratio;
+    uint64_t particles_per_cell;
+    double volume_stiffness;
+    int32_t redistribute;
+    int32_t reserved0;
+    double redist_cap_factor;
+} sdr_fluid_params;
+
+/* Needle, src/solver.rs:89-103 (inject_until = +inf injects for the whole run). */
+typedef struct {
+    sdr_vec3 tip;
+    sdr_vec3 axis;
+    double radius;
+    double flow_rate;
+    double inject_until;
+} sdr_needle;
+
+/* SolveParams, src/pressure.rs:36-50. */
+typedef struct {
+    uint64_t max_iters;
+    double tol;
+} sdr_solve_params;
+
+/* A node-grid signed distance field, src/sdf.rs:23-34; data is nx*ny*nz
+ * values, x fastest, phi < 0 inside the cavity. */
+typedef struct {
+    sdr_vec3 origin;
+    double dx;
+    uint64_t nx, ny, nz;
+    const double* data;
+} sdr_sdf_desc;
+
+/* Optional creation settings; pass NULL for defaults. */
+typedef struct {
+    uint64_t max_particles; /* device particle capacity (0 = derive from the cavity volume) */
+    int32_t device;         /* CUDA device ordinal (-1 = current) */
+    int32_t reserved0;
+} sdr_solver_options;
+
+/* Solver's public scalar fields (src/solver.rs:143-167) plus GPU-side counters. */
+typedef struct {
+    double time;
+    uint64_t steps;
+    uint64_t last_pcg_iters;
+    uint64_t last_substeps;
+    uint64_t particles;
+    uint64_t drained;
+    double last_residual;
+    double emit_accum;
+    uint64_t rng_state;
+    uint64_t emitted;        /* particles injected since creation (mass-balance numerator) */
+    uint64_t culled;         /* particles removed outside the outlet (wall tunnelling, out of domain) */
+    uint64_t redistributed;  /* particle moves made by redistribution since creation */
+    uint64_t nx, ny, nz;     /* MAC grid cells */
+    double dx;
+    sdr_vec3 origin;
+} sdr_solver_stats;
+
+/* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */
+typedef struct {
+    uint64_t frame;
+    double time_s;
+    uint64_t particles;
+    double fluid_volume_ml, drained_volume_ml, fill_fraction, wall_coverage;
+    double mean_pressure_pa, max_pressure_pa, max_pressure_mmhg;
+    double wall_pressure_pa, peak_wall_pressure_pa, peak_wall_pressure_mmhg;
+    uint64_t membrane_artifacts;
+    double max_speed_m_s, kinetic_energy;
+    uint64_t pcg_iters;
+} sdr_frame_metrics;
+
+/* Summary, src/metrics.rs:69-97. */
+typedef struct {
+    uint64_t frames;
+    double final_time_s, peak_fill_fraction, final_fill_fraction;
+    double peak_wall_coverage, final_wall_coverage;
+    double peak_membrane_pressure_pa, peak_membrane_pressure_mmhg;
+    double mean_membrane_pressure_pa, mean_membrane_pressure_mmhg;
+    double peak_pressure_pa, peak_pressure_mmhg;
+    uint64_t membrane_artifacts_total;
+    double total_drained_ml, injected_ml, mass_balance;
+} sdr_summary;
+
+typedef struct sdr_solver sdr_solver;
+typedef struct sdr_metrics sdr_metrics;
+
+/* ---------------------------------------------------------------- library */
+int sdr_abi_version(void);
+/* Thread-local message for the last failing call on this thread ("" if none). */
+const char* sdr_last_error(void);
+/* Number of kernel launches this library has issued in this process. */
+uint64_t sdr_kernel_launch_count(void);
+
+/* ---------------------------------------------------------------- solver */
+/* Solver::new (src/solver.rs:184-222): grid covers the SDF bounds at sim_dx;
+ * the static cavity mask is built on the device from the SDF. */
+int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_params* fluid,
+                      const sdr_needle* needle, const sdr_solver_options* options,
+                      sdr_solver** out);
+int sdr_solver_destroy(sdr_solver* s);
+/* Solver::outlet field (src/solver.rs:153); NULL removes the outlet. */
+int sdr_solver_set_outlet(sdr_solver* s, const sdr_aabb* outlet_or_null);
+/* Solver::solve field (src/solver.rs:154). */
+int sdr_solver_set_solve_params(sdr_solver* s, const sdr_solve_params* params);
+/* Solver::needle field (src/solver.rs:150). */
+int sdr_solver_set_needle(sdr_solver* s, const sdr_needle* needle);
+/* Solver::step (src/solver.rs:237-259): CFL sub-stepping with the dt/512 floor. */
+int sdr_solver_step(sdr_solver* s, double dt);
+/* Solver::substep (src/solver.rs:284-310). */
+int sdr_solver_substep(sdr_solver* s, double dt);
+/* Public fields time/steps/last_pcg_iters/last_substeps/drained (solver.rs:155-166). */
+int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
+/* Restore the solver's scalar state (checkpoint / shadow stepping). */
+int sdr_solver_set_scalars(sdr_solver* s, double time, double emit_accum, uint64_t steps,
+                           uint64_t drained, uint64_t rng_state);
+/* ParticleSet positions/velocities (src/particles.rs:13-16), widened to f64,
+ * xyz interleaved; *n_out receives the particle count. SDR_ERR_BUFFER if cap < n. */
+int sdr_solver_copy_particles(sdr_solver* s, double* pos_xyz, double* vel_xyz, size_t cap,
+                              size_t* n_out);
+/* Same, as the device's f32 storage (float xyz triples), e.g. for XYZ frame output. */
+int sdr_solver_copy_particles_f32(sdr_solver* s, float* pos_xyz, float* vel_xyz, size_t cap,
+                                  size_t* n_out);
+/* Replace the particle set (values are rounded to f32 on the device). */
+int sdr_solver_set_particles(sdr_solver* s, const double* pos_xyz, const double* vel_xyz,
+                             size_t n);
+/* Solver::pressure (src/solver.rs:164), nx*ny*nz f64. */
+int sdr_solver_copy_pressure(sdr_solver* s, double* out, size_t cap);
+/* Cell labels of the last classify (u8, SDR_CELL_*). */
+int sdr_solver_copy_cells(sdr_solver* s, uint8_t* out, size_t cap);
+/* Static cavity mask (src/solver.rs:173): 1 where the cell centre has phi < 0. */
+int sdr_solver_copy_cavity_mask(sdr_solver* s, uint8_t* out, size_t cap);
+/* MacGrid faces (src/grid.rs:92-100). which: 0 u, 1 v, 2 w, 3..5 the saved
+ * (post-P2G) copies used by FLIP. f32 values widened to f64. */
+int sdr_solver_copy_face(sdr_solver* s, int which, double* out, size_t cap);
+int sdr_solver_set_face(sdr_solver* s, int which, const double* in, size_t n);
+/* Diagnostics (src/solver.rs:763-890). */
+int sdr_solver_max_pressure(sdr_solver* s, double* out);
+int sdr_solver_mean_pressure(sdr_solver* s, double* out);
+int sdr_solver_max_speed(sdr_solver* s, double* out);
+int sdr_solver_cells_fluid_count(sdr_solver* s, uint64_t* out);
+int sdr_solver_max_particles_per_cell(sdr_solver* s, uint64_t* out);
+/* The P2G counting sort of the last substep: per-particle cell keys and the
+ * stable permutation (sorted slot -> particle index), u32 each. */
+int sdr_solver_copy_sort(sdr_solver* s, uint32_t* keys, uint32_t* perm, size_t cap,
+                         size_t* n_out);
+
+/* Phases of Solver::substep (src/solver.rs:284-310), for per-phase parity tests. */
+enum {
+    SDR_PHASE_EMIT = 0,
+    SDR_PHASE_CLASSIFY = 1,
+    SDR_PHASE_P2G = 2,        /* counting sort + gather; also saves the grid (save_grid) */
+    SDR_PHASE_ADD_FORCES = 4, /* gravity on the working faces */
+    SDR_PHASE_PROJECT = 5,    /* volume_source + project_capturing_with_source */
+    SDR_PHASE_EXTRAPOLATE = 6,
+    SDR_PHASE_G2P = 7,
+    SDR_PHASE_ADVECT = 8,
+    SDR_PHASE_BOUNDS = 9,
+    SDR_PHASE_REDISTRIBUTE = 10,
+    SDR_PHASE_CLOCK = 11
+};
+int sdr_solver_run_phase(sdr_solver* s, int phase, double dt);
+
+/* ---------------------------------------------------------------- metrics */
+/* MetricsCollector::new (src/metrics.rs:119-185): wall mask on the device. */
+int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out);
+int sdr_metrics_destroy(sdr_metrics* m);
+/* MetricsCollector::record (src/metrics.rs:188-316): reductions on the device. */
+int sdr_metrics_record(sdr_metrics* m, sdr_solver* s, uint64_t frame, sdr_frame_metrics* out);
+/* MetricsCollector::summary (src/metrics.rs:324-382). */
+int sdr_metrics_summary(const sdr_metrics* m, sdr_summary* out);
+int sdr_metrics_wall_count(const sdr_metrics* m, uint64_t* out);
+
+/* ---------------------------------------------------------------- geometry */
+/* Grid of Sdf::from_mesh (src/sdf.rs:47-58) for triangles (9 f64 each). */
+int sdr_sdf_mesh_grid(const double* tris, size_t ntri, double dx, double padding,
+                      sdr_vec3* origin, uint64_t dims[3]);
+/* Sdf::from_mesh_in_bounds values (src/sdf.rs:53-86, 187-272): winding-number
+ * sign and closest-point distance per node, on the device. */
+int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double dx,
+                      const uint64_t dims[3], double* out);
+/* SinusParams, src/sinus.rs:26-45 (SI units). */
+typedef struct {
+    sdr_vec3 semi_axes;
+    sdr_vec3 center;
+    double taper;
+    double bumpiness;
+    double socket_x, socket_z;
+    double socket_radius;
+    double socket_depth;
+    double model_dx;
+} sdr_sinus_params;
+/* Sdf::from_fn(SinusParams::implicit) (src/scene.rs:289-297, sinus.rs:89-119), on the device. */
+int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx,
+                       const uint64_t dims[3], double* out);
+/* |signed volume| of the naive-surface-nets mesh of a node field
+ * (src/surface_nets.rs:48-195, src/mesh.rs:63-70): the parametric cavity volume. */
+int sdr_surface_nets_volume(const double* values, const uint64_t dims[3], sdr_vec3 origin,
+                            double dx, double* volume, uint64_t* triangles);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDR_GPU_H */

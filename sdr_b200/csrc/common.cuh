@@ -1,0 +1,237 @@
+// Shared device types and helpers for the sdr B200 substep kernels.
+//
+// Precision contract (FP32 transfers, FP64 solve):
+//  * particle state, MAC faces and SDF samples used by advection are f32;
+//  * cell keys for labels/histograms, the pressure RHS, the MIC(0) factor,
+//    the PCG vectors, dots and residual norms are f64, computed with explicit
+//    round-to-nearest intrinsics so no FMA contraction changes the reference's
+//    operation order (src/pressure.rs:123-609).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sdr {
+
+enum : uint8_t { SOLID = 0, FLUID = 1, AIR = 2 };
+
+constexpr int kInvalid = -1;
+
+// Uncontracted f64 arithmetic (the reference's Rust emits no FMA).
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+struct Aabb {
+    double mn[3], mx[3];
+};
+
+// MAC grid geometry (src/grid.rs:92-100).
+struct Grid {
+    int nx, ny, nz;
+    double dx, ox, oy, oz;
+    float dxf, oxf, oyf, ozf;
+};
+
+// Node-grid SDF (src/sdf.rs:23-34), f32 copy for hot sampling.
+struct Sdf {
+    int nx, ny, nz;
+    float dx, ox, oy, oz;
+    const float* data;
+};
+
+__device__ __forceinline__ bool aabb_contains(const Aabb& b, double x, double y, double z) {
+    // math.rs:249-256 (inclusive)
+    return x >= b.mn[0] && x <= b.mx[0] && y >= b.mn[1] && y <= b.mx[1] && z >= b.mn[2] &&
+           z <= b.mx[2];
+}
+
+// Solver::cell_of (solver.rs:897-908) in f64 on the (f32) particle position:
+// the same arithmetic as the reference applied to the same stored values.
+__device__ __forceinline__ int cell_of(const Grid& g, float px, float py, float pz) {
+    double lx = ddiv(dsub((double)px, g.ox), g.dx);
+    double ly = ddiv(dsub((double)py, g.oy), g.dx);
+    double lz = ddiv(dsub((double)pz, g.oz), g.dx);
+    if (!(lx >= 0.0) || !(ly >= 0.0) || !(lz >= 0.0)) return kInvalid;  // also rejects NaN
+    if (lx >= (double)g.nx || ly >= (double)g.ny || lz >= (double)g.nz) return kInvalid;
+    int i = (int)lx, j = (int)ly, k = (int)lz;
+    return (k * g.ny + j) * g.nx + i;
+}
+
+// clamp_base of grid.rs:25-34 / sdf.rs:136-145 in f32.
+__device__ __forceinline__ void clamp_base(float g, int n, int& i, float& f) {
+    if (!(g > 0.0f)) {  // g <= 0 or NaN
+        i = 0;
+        f = 0.0f;
+    } else if (g >= (float)(n - 1)) {
+        i = n - 2;
+        f = 1.0f;
+    } else {
+        float fl = floorf(g);
+        i = (int)fl;
+        f = g - fl;
+    }
+}
+
+// trilinear_sample (grid.rs:18-47), f32, dims = node counts (x fastest).
+__device__ __forceinline__ float trilerp(const float* __restrict__ a, int nx, int ny, int nz,
+                                         float gx, float gy, float gz) {
+    int i, j, k;
+    float fx, fy, fz;
+    clamp_base(gx, nx, i, fx);
+    clamp_base(gy, ny, j, fy);
+    clamp_base(gz, nz, k, fz);
+    size_t b = ((size_t)k * ny + j) * nx + i;
+    size_t sy = nx, sz = (size_t)nx * ny;
+    float c00 = a[b] * (1.0f - fx) + a[b + 1] * fx;
+    float c10 = a[b + sy] * (1.0f - fx) + a[b + sy + 1] * fx;
+    float c01 = a[b + sz] * (1.0f - fx) + a[b + sz + 1] * fx;
+    float c11 = a[b + sy + sz] * (1.0f - fx) + a[b + sy + sz + 1] * fx;
+    float c0 = c00 * (1.0f - fy) + c10 * fy;
+    float c1 = c01 * (1.0f - fy) + c11 * fy;
+    return c0 * (1.0f - fz) + c1 * fz;
+}
+
+// Same stencil on the difference field (a - b), for the FLIP delta (solver.rs:652-673).
+__device__ __forceinline__ float trilerp_diff(const float* __restrict__ a,
+                                              const float* __restrict__ b, int nx, int ny, int nz,
+                                              float gx, float gy, float gz) {
+    int i, j, k;
+    float fx, fy, fz;
+    clamp_base(gx, nx, i, fx);
+    clamp_base(gy, ny, j, fy);
+    clamp_base(gz, nz, k, fz);
+    size_t o = ((size_t)k * ny + j) * nx + i;
+    size_t sy = nx, sz = (size_t)nx * ny;
+#define D(q) (a[q] - b[q])
+    float c00 = D(o) * (1.0f - fx) + D(o + 1) * fx;
+    float c10 = D(o + sy) * (1.0f - fx) + D(o + sy + 1) * fx;
+    float c01 = D(o + sz) * (1.0f - fx) + D(o + sz + 1) * fx;
+    float c11 = D(o + sy + sz) * (1.0f - fx) + D(o + sy + sz + 1) * fx;
+#undef D
+    float c0 = c00 * (1.0f - fy) + c10 * fy;
+    float c1 = c01 * (1.0f - fy) + c11 * fy;
+    return c0 * (1.0f - fz) + c1 * fz;
+}
+
+struct Faces {
+    const float* u;
+    const float* v;
+    const float* w;
+};
+
+// MacGrid::velocity_at (grid.rs:191), f32.
+__device__ __forceinline__ float3 velocity_at(const Grid& g, Faces f, float px, float py,
+                                              float pz) {
+    float lx = (px - g.oxf) / g.dxf, ly = (py - g.oyf) / g.dxf, lz = (pz - g.ozf) / g.dxf;
+    float3 r;
+    r.x = trilerp(f.u, g.nx + 1, g.ny, g.nz, lx, ly - 0.5f, lz - 0.5f);
+    r.y = trilerp(f.v, g.nx, g.ny + 1, g.nz, lx - 0.5f, ly, lz - 0.5f);
+    r.z = trilerp(f.w, g.nx, g.ny, g.nz + 1, lx - 0.5f, ly - 0.5f, lz);
+    return r;
+}
+
+// Sdf::sample (sdf.rs:134-166), f32.
+__device__ __forceinline__ float sdf_sample(const Sdf& s, float px, float py, float pz) {
+    float lx = (px - s.ox) / s.dx, ly = (py - s.oy) / s.dx, lz = (pz - s.oz) / s.dx;
+    return trilerp(s.data, s.nx, s.ny, s.nz, lx, ly, lz);
+}
+
+// Sdf::gradient (sdf.rs:170-176), f32 central differences.
+__device__ __forceinline__ float3 sdf_gradient(const Sdf& s, float px, float py, float pz) {
+    float h = s.dx;
+    float gx = sdf_sample(s, px + h, py, pz) - sdf_sample(s, px - h, py, pz);
+    float gy = sdf_sample(s, px, py + h, pz) - sdf_sample(s, px, py - h, pz);
+    float gz = sdf_sample(s, px, py, pz + h) - sdf_sample(s, px, py, pz - h);
+    float d = 2.0f * h;
+    return make_float3(gx / d, gy / d, gz / d);
+}
+
+// Vec3::normalize_or_zero (math.rs:73-80), f32.
+__device__ __forceinline__ float3 normalize_or_zero(float3 a) {
+    float len = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    if (len > 1e-12f) return make_float3(a.x / len, a.y / len, a.z / len);
+    return make_float3(0.f, 0.f, 0.f);
+}
+
+// Solver::project_inside (solver.rs:717-732), f32; margin is half a grid cell.
+__device__ __forceinline__ float3 project_inside(const Sdf& s, float margin, float3 p) {
+    for (int it = 0; it < 3; ++it) {
+        float phi = sdf_sample(s, p.x, p.y, p.z);
+        if (phi <= -margin) break;
+        float3 g = normalize_or_zero(sdf_gradient(s, p.x, p.y, p.z));
+        if (sqrtf(g.x * g.x + g.y * g.y + g.z * g.z) == 0.0f) break;
+        float a = phi + margin;
+        p.x -= g.x * a;
+        p.y -= g.y * a;
+        p.z -= g.z * a;
+    }
+    return p;
+}
+
+// hash_jitter (solver.rs:916-930): splitmix64 finaliser -> [-0.3, 0.3)^3, f64.
+__device__ __host__ __forceinline__ double jitter_mix(uint64_t k) {
+    uint64_t z = k + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return ((double)(z >> 11) / (double)(1ULL << 53) - 0.5) * 0.6;
+}
+
+// ---------------------------------------------------------------- block reductions
+template <int BS>
+__device__ __forceinline__ double block_max(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < BS / 32) ? sh[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (l == 0) sh[0] = v;
+    }
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Deterministic f64 block sum: fixed shuffle tree, then warps in index order.
+template <int BS>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < BS / 32) ? sh[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (l == 0) sh[0] = v;
+    }
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+template <int BS>
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < BS / 32) ? sh[l] : 0u;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (l == 0) sh[0] = v;
+    }
+    __syncthreads();
+    uint32_t r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+}  // namespace sdr

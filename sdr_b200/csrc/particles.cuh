@@ -1,0 +1,568 @@
+// Particle-side kernels of Solver::substep (src/solver.rs:284-310):
+// classify + cell keys, the P2G counting sort and fixed-order face gather,
+// G2P (FLIP/PIC) fused with RK2 advection and the bounds flags, the stable
+// compaction of ParticleSet::retain, and the redistribution sweeps.
+#pragma once
+#include "common.cuh"
+
+namespace sdr {
+
+constexpr int kBS = 256;
+
+// ------------------------------------------------------------------ classify
+// Solver::classify (solver.rs:342-371) first half: static labels per cell.
+__global__ void k_base_labels(const uint8_t* __restrict__ base, uint8_t* __restrict__ cells,
+                              size_t n) {
+    size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) cells[c] = base[c];
+}
+
+// Per particle: the f64 cell key of Solver::cell_of (labels, histograms) and
+// the f32 clamped cell the P2G gather bins by (the same f32 arithmetic the
+// gather's weights use, so every contribution lands in the gathered stencil).
+// With mark_fluid, also the second half of classify: Air cells holding a
+// particle that is not in the outlet become Fluid (solver.rs:362-370).
+__global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t n,
+                                int has_outlet, Aabb outlet, int mark_fluid,
+                                uint8_t* __restrict__ cells, int* __restrict__ key_cell,
+                                uint32_t* __restrict__ key_sort, uint32_t* __restrict__ hist_valid,
+                                uint32_t* __restrict__ hist_sort) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float4 q = pos[p];
+    int c = cell_of(g, q.x, q.y, q.z);
+    key_cell[p] = c;
+    if (c >= 0) {
+        atomicAdd(&hist_valid[c], 1u);
+        if (mark_fluid && cells[c] == AIR &&
+            !(has_outlet && aabb_contains(outlet, q.x, q.y, q.z)))
+            cells[c] = FLUID;  // benign race: every writer stores FLUID
+    }
+    float lx = (q.x - g.oxf) / g.dxf, ly = (q.y - g.oyf) / g.dxf, lz = (q.z - g.ozf) / g.dxf;
+    int i = (lx > 0.f) ? min((int)floorf(lx), g.nx - 1) : 0;
+    int j = (ly > 0.f) ? min((int)floorf(ly), g.ny - 1) : 0;
+    int k = (lz > 0.f) ? min((int)floorf(lz), g.nz - 1) : 0;
+    uint32_t ks = ((uint32_t)k * g.ny + j) * g.nx + i;
+    key_sort[p] = ks;
+    atomicAdd(&hist_sort[ks], 1u);
+}
+
+// ------------------------------------------------------------------ counting sort
+// Slot assignment within each cell segment (start from the exclusive scan).
+__global__ void k_sort_scatter(const uint32_t* __restrict__ key, uint32_t n,
+                               uint32_t* __restrict__ fill, uint32_t* __restrict__ perm) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint32_t s = atomicAdd(&fill[key[p]], 1u);
+    perm[s] = p;
+}
+
+// Make each segment ascending in particle index, so the permutation equals a
+// stable counting sort (bit-exact vs a CPU stable sort of the same keys) and
+// the gather's summation order is fixed. Short segments: insertion sort by
+// one thread; long ones are queued for k_sort_long.
+__global__ void k_sort_segments(const uint32_t* __restrict__ start, uint32_t ncell,
+                                uint32_t* __restrict__ perm, uint32_t* __restrict__ long_list,
+                                uint32_t* __restrict__ long_count) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    uint32_t a = start[c], b = start[c + 1];
+    uint32_t len = b - a;
+    if (len < 2) return;
+    if (len > 48) {
+        uint32_t s = atomicAdd(long_count, 1u);
+        long_list[s] = c;
+        return;
+    }
+    for (uint32_t x = a + 1; x < b; ++x) {
+        uint32_t v = perm[x];
+        uint32_t y = x;
+        while (y > a && perm[y - 1] > v) {
+            perm[y] = perm[y - 1];
+            --y;
+        }
+        perm[y] = v;
+    }
+}
+
+// Rank sort of long segments (indices are distinct): one block per segment.
+__global__ void k_sort_long(const uint32_t* __restrict__ start, const uint32_t* __restrict__ long_list,
+                            const uint32_t* __restrict__ long_count, uint32_t* __restrict__ perm,
+                            uint32_t* __restrict__ tmp) {
+    uint32_t nl = *long_count;
+    for (uint32_t q = blockIdx.x; q < nl; q += gridDim.x) {
+        uint32_t c = long_list[q];
+        uint32_t a = start[c], b = start[c + 1];
+        for (uint32_t x = a + threadIdx.x; x < b; x += blockDim.x) {
+            uint32_t v = perm[x];
+            uint32_t r = 0;
+            for (uint32_t y = a; y < b; ++y) r += perm[y] < v;
+            tmp[a + r] = v;
+        }
+        __syncthreads();
+        for (uint32_t x = a + threadIdx.x; x < b; x += blockDim.x) perm[x] = tmp[x];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ P2G gather
+struct P2GArgs {
+    Grid g;
+    const float4* pos;
+    const float4* vel;
+    const uint32_t* start;  // ncell + 1
+    const uint32_t* perm;
+    float* u;
+    float* v;
+    float* w;
+    float* su;
+    float* sv;
+    float* sw;
+    const uint8_t* cells;  // for enforce_solid_faces (may be null)
+    double gdt[3];         // gravity * dt per component (0 = skip)
+    int add_forces;
+    int enforce;
+};
+
+// Is face (i,j,k) of a component next to a Solid cell or the domain edge?
+// (pressure.rs:243-281)
+__device__ __forceinline__ bool solid_at(const Grid& g, const uint8_t* cells, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) return true;
+    return cells[((size_t)k * g.ny + j) * g.nx + i] == SOLID;
+}
+
+// One thread per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]; it owns the u, v
+// and w faces with that index. It visits the 27 cells around the node in
+// fixed (k, j, i) order and, within a cell, particles in ascending index,
+// accumulating the trilinear_scatter weights (grid.rs:52-88) in f64, then
+// normalises (solver.rs:944-952), saves the FLIP copy (save_grid), and
+// optionally adds gravity (add_forces) and zeroes solid faces.
+__global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
+    const Grid& g = a.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i > g.nx) return;
+    const bool hu = j < g.ny && k < g.nz, hv = i < g.nx && k < g.nz, hw = i < g.nx && j < g.ny;
+    double su = 0, wu = 0, sv = 0, wv = 0, sw = 0, ww = 0;
+    for (int ck = max(k - 1, 0); ck <= min(k + 1, g.nz - 1); ++ck)
+        for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj)
+            for (int ci = max(i - 1, 0); ci <= min(i + 1, g.nx - 1); ++ci) {
+                uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx + ci;
+                uint32_t s0 = a.start[c], s1 = a.start[c + 1];
+                for (uint32_t s = s0; s < s1; ++s) {
+                    uint32_t p = a.perm[s];
+                    float4 q = a.pos[p];
+                    float4 vel = a.vel[p];
+                    float lx = (q.x - g.oxf) / g.dxf, ly = (q.y - g.oyf) / g.dxf,
+                          lz = (q.z - g.ozf) / g.dxf;
+                    int i0, j0, k0;
+                    float fx, fy, fz;
+                    if (hu) {
+                        clamp_base(lx, g.nx + 1, i0, fx);
+                        clamp_base(ly - 0.5f, g.ny, j0, fy);
+                        clamp_base(lz - 0.5f, g.nz, k0, fz);
+                        int di = i - i0, dj = j - j0, dk = k - k0;
+                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
+                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
+                                        (dk ? fz : 1.0f - fz);
+                            su = dadd(su, (double)wgt * (double)vel.x);
+                            wu = dadd(wu, (double)wgt);
+                        }
+                    }
+                    if (hv) {
+                        clamp_base(lx - 0.5f, g.nx, i0, fx);
+                        clamp_base(ly, g.ny + 1, j0, fy);
+                        clamp_base(lz - 0.5f, g.nz, k0, fz);
+                        int di = i - i0, dj = j - j0, dk = k - k0;
+                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
+                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
+                                        (dk ? fz : 1.0f - fz);
+                            sv = dadd(sv, (double)wgt * (double)vel.y);
+                            wv = dadd(wv, (double)wgt);
+                        }
+                    }
+                    if (hw) {
+                        clamp_base(lx - 0.5f, g.nx, i0, fx);
+                        clamp_base(ly - 0.5f, g.ny, j0, fy);
+                        clamp_base(lz, g.nz + 1, k0, fz);
+                        int di = i - i0, dj = j - j0, dk = k - k0;
+                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
+                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
+                                        (dk ? fz : 1.0f - fz);
+                            sw = dadd(sw, (double)wgt * (double)vel.z);
+                            ww = dadd(ww, (double)wgt);
+                        }
+                    }
+                }
+            }
+    if (hu) {
+        size_t f = ((size_t)k * g.ny + j) * (g.nx + 1) + i;
+        float val = wu > 1e-12 ? (float)ddiv(su, wu) : 0.0f;
+        a.su[f] = val;
+        if (a.add_forces && a.gdt[0] != 0.0) val = (float)dadd((double)val, a.gdt[0]);
+        if (a.enforce && (solid_at(g, a.cells, i - 1, j, k) || solid_at(g, a.cells, i, j, k))) val = 0.0f;
+        a.u[f] = val;
+    }
+    if (hv) {
+        size_t f = ((size_t)k * (g.ny + 1) + j) * g.nx + i;
+        float val = wv > 1e-12 ? (float)ddiv(sv, wv) : 0.0f;
+        a.sv[f] = val;
+        if (a.add_forces && a.gdt[1] != 0.0) val = (float)dadd((double)val, a.gdt[1]);
+        if (a.enforce && (solid_at(g, a.cells, i, j - 1, k) || solid_at(g, a.cells, i, j, k))) val = 0.0f;
+        a.v[f] = val;
+    }
+    if (hw) {
+        size_t f = ((size_t)k * g.ny + j) * g.nx + i;
+        float val = ww > 1e-12 ? (float)ddiv(sw, ww) : 0.0f;
+        a.sw[f] = val;
+        if (a.add_forces && a.gdt[2] != 0.0) val = (float)dadd((double)val, a.gdt[2]);
+        if (a.enforce && (solid_at(g, a.cells, i, j, k - 1) || solid_at(g, a.cells, i, j, k))) val = 0.0f;
+        a.w[f] = val;
+    }
+}
+
+// Solver::add_forces (solver.rs:593-604) on its own (phase mode).
+__global__ void k_add_forces(float* __restrict__ f, size_t n, double gdt) {
+    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) f[q] = (float)dadd((double)f[q], gdt);
+}
+
+// enforce_solid_faces (pressure.rs:243-281) on its own (phase mode): one
+// thread per node, owning the u/v/w faces with that index.
+__global__ void k_enforce_solid(Grid g, const uint8_t* __restrict__ cells, float* __restrict__ u,
+                                float* __restrict__ v, float* __restrict__ w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i > g.nx) return;
+    if (j < g.ny && k < g.nz && (solid_at(g, cells, i - 1, j, k) || solid_at(g, cells, i, j, k)))
+        u[((size_t)k * g.ny + j) * (g.nx + 1) + i] = 0.0f;
+    if (i < g.nx && k < g.nz && (solid_at(g, cells, i, j - 1, k) || solid_at(g, cells, i, j, k)))
+        v[((size_t)k * (g.ny + 1) + j) * g.nx + i] = 0.0f;
+    if (i < g.nx && j < g.ny && (solid_at(g, cells, i, j, k - 1) || solid_at(g, cells, i, j, k)))
+        w[((size_t)k * g.ny + j) * g.nx + i] = 0.0f;
+}
+
+// ------------------------------------------------------------------ G2P + advect
+struct MoveArgs {
+    Grid g;
+    Sdf sdf;
+    float4* pos;
+    float4* vel;
+    const uint32_t* order;  // processing order (sorted slots -> particle), or null
+    uint32_t n;
+    Faces f;         // projected, extrapolated faces
+    Faces saved;     // post-P2G faces
+    float flip;      // clamp(flip_ratio, 0, 1)
+    float dt;
+    int do_g2p;
+    int do_advect;
+    int do_bounds;   // write keep/drained flags
+    Aabb bb;         // solid.bounds()
+    int has_outlet;
+    Aabb outlet;
+    float cull_phi;  // 0.5 * solid.dx
+    uint32_t* keep;  // 1 = keep (ParticleSet::retain predicate)
+    uint32_t* drained;
+};
+
+// Bounds predicate of enforce_particle_bounds (solver.rs:736-755).
+__device__ __forceinline__ void bounds_flags(const MoveArgs& a, float3 p, uint32_t& keep,
+                                             uint32_t& drained) {
+    drained = 0;
+    if (!aabb_contains(a.bb, p.x, p.y, p.z)) {
+        keep = 0;
+        return;
+    }
+    if (a.has_outlet && aabb_contains(a.outlet, p.x, p.y, p.z)) {
+        keep = 0;
+        drained = 1;
+        return;
+    }
+    keep = sdf_sample(a.sdf, p.x, p.y, p.z) < a.cull_phi ? 1u : 0u;
+}
+
+// Solver::g2p (solver.rs:650-677) fused with Solver::advect (solver.rs:693-711)
+// and the bounds predicate. Both read the pre-advection position and the same
+// grid, so velocity_at(p0) is shared. Particles are visited in sorted-cell
+// order so neighbouring threads read neighbouring faces.
+__global__ void __launch_bounds__(kBS) k_g2p_advect(MoveArgs a) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    uint32_t p = a.order ? a.order[t] : t;
+    const Grid& g = a.g;
+    float4 q = a.pos[p];
+    float3 p0 = make_float3(q.x, q.y, q.z);
+    float3 v0 = velocity_at(g, a.f, p0.x, p0.y, p0.z);
+    if (a.do_g2p) {
+        float lx = (p0.x - g.oxf) / g.dxf, ly = (p0.y - g.oyf) / g.dxf, lz = (p0.z - g.ozf) / g.dxf;
+        float dvx = trilerp_diff(a.f.u, a.saved.u, g.nx + 1, g.ny, g.nz, lx, ly - 0.5f, lz - 0.5f);
+        float dvy = trilerp_diff(a.f.v, a.saved.v, g.nx, g.ny + 1, g.nz, lx - 0.5f, ly, lz - 0.5f);
+        float dvz = trilerp_diff(a.f.w, a.saved.w, g.nx, g.ny, g.nz + 1, lx - 0.5f, ly - 0.5f, lz);
+        float4 v = a.vel[p];
+        float pic = 1.0f - a.flip;
+        v.x = (v.x + dvx) * a.flip + v0.x * pic;
+        v.y = (v.y + dvy) * a.flip + v0.y * pic;
+        v.z = (v.z + dvz) * a.flip + v0.z * pic;
+        a.vel[p] = v;
+    }
+    float3 pn = p0;
+    if (a.do_advect) {
+        float h = 0.5f * a.dt;
+        float3 mid = make_float3(p0.x + v0.x * h, p0.y + v0.y * h, p0.z + v0.z * h);
+        float3 vm = velocity_at(g, a.f, mid.x, mid.y, mid.z);
+        float3 st = make_float3(vm.x * a.dt, vm.y * a.dt, vm.z * a.dt);
+        float len = sqrtf(st.x * st.x + st.y * st.y + st.z * st.z);
+        if (len > g.dxf) {
+            float sc = g.dxf / len;
+            st = make_float3(st.x * sc, st.y * sc, st.z * sc);
+        }
+        float3 c = project_inside(a.sdf, 0.5f * g.dxf, make_float3(p0.x + st.x, p0.y + st.y, p0.z + st.z));
+        if (sdf_sample(a.sdf, c.x, c.y, c.z) <= 0.0f) pn = c;
+        a.pos[p] = make_float4(pn.x, pn.y, pn.z, 0.0f);
+    }
+    if (a.do_bounds) {
+        uint32_t k, d;
+        bounds_flags(a, pn, k, d);
+        a.keep[p] = k;
+        a.drained[p] = d;
+    }
+}
+
+// Bounds flags alone (phase mode, after an external position change).
+__global__ void k_bounds_flags(MoveArgs a) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    float4 q = a.pos[p];
+    uint32_t k, d;
+    bounds_flags(a, make_float3(q.x, q.y, q.z), k, d);
+    a.keep[p] = k;
+    a.drained[p] = d;
+}
+
+// Stable scatter of kept particles (ParticleSet::retain, particles.rs:38-49)
+// plus the drained/culled tallies.
+__global__ void k_compact(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                          const uint32_t* __restrict__ keep, const uint32_t* __restrict__ drained,
+                          const uint32_t* __restrict__ off, uint32_t n, float4* __restrict__ pos2,
+                          float4* __restrict__ vel2, unsigned long long* __restrict__ counters) {
+    __shared__ uint32_t sh[33];
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t d = 0, c = 0;
+    if (p < n) {
+        if (keep[p]) {
+            uint32_t o = off[p];
+            pos2[o] = pos[p];
+            vel2[o] = vel[p];
+        } else {
+            d = drained[p];
+            c = 1 - d;
+        }
+    }
+    uint32_t sd = block_sum_u32<kBS>(d, sh);
+    uint32_t sc = block_sum_u32<kBS>(c, sh);
+    if (threadIdx.x == 0) {
+        if (sd) atomicAdd(&counters[0], (unsigned long long)sd);
+        if (sc) atomicAdd(&counters[1], (unsigned long long)sc);
+    }
+}
+
+// ------------------------------------------------------------------ redistribute
+// Solver::redistribute (solver.rs:454-557). Facts the GPU form relies on:
+//  * a cell sheds only while its count exceeds the cap, and only cells over
+//    the cap at the start of a sweep can ever exceed it (receivers stop at the
+//    cap), so only particles in those cells can move;
+//  * decisions read counts only; positions/velocities of moved particles are
+//    functions of (index, destination cell) and can be written afterwards.
+// So: histogram -> index-ordered candidate list -> sequential decision replay
+// over the candidates in shared memory -> parallel move application.
+
+// n is read from the device (the count after this substep's compaction).
+__global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
+                                int* __restrict__ key_cell, uint32_t* __restrict__ count) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= *n_dev) return;
+    float4 q = pos[p];
+    int c = cell_of(g, q.x, q.y, q.z);
+    key_cell[p] = c;
+    if (c >= 0) atomicAdd(&count[c], 1u);
+}
+
+// Flags over [0, n_upper): zero past the live count so the scan sees exact flags.
+__global__ void k_redist_flag_n(const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
+                                const uint32_t* __restrict__ n_dev, uint32_t n_upper, uint32_t cap,
+                                uint32_t* __restrict__ flag) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_upper) return;
+    if (p >= *n_dev) {
+        flag[p] = 0;
+        return;
+    }
+    int c = key_cell[p];
+    flag[p] = (c >= 0 && count[c] > cap) ? 1u : 0u;
+}
+
+__global__ void k_redist_gather(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                                uint32_t n, uint32_t* __restrict__ cand) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n && flag[p]) cand[off[p]] = p;
+}
+
+constexpr int kRedistTable = 4096;  // shared-memory hash slots (power of two)
+constexpr int kRedistBS = 1024;
+
+struct RedistArgs {
+    Grid g;
+    const int* key_cell;
+    uint32_t* count;         // histogram at sweep start (the fallback path mutates it)
+    const uint8_t* cavity;
+    const uint32_t* cand;    // candidate particles, ascending index
+    const uint32_t* ncand;   // device count
+    uint32_t cand_cap;
+    int* slots;              // 7 per candidate: own cell + 6 neighbours (-1 = none)
+    uint32_t cap;
+    double down[6];          // dir . gdir for -x,+x,-y,+y,-z,+z (f64, solver.rs:490-511)
+    uint32_t* moves;         // pairs (particle, destination cell)
+    uint32_t* nmoves;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761u) & (kRedistTable - 1); }
+
+// One block. Phase 1: all threads insert every referenced cell into a shared
+// hash table and record slots. Phase 2: thread 0 replays the reference's
+// sequential loop over the candidates (index order), mutating counts, exactly
+// as solver.rs:476-555 does. If the table overflows, thread 0 replays against
+// the global counts instead (same result, slower).
+__global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
+    __shared__ int tkey[kRedistTable];
+    __shared__ uint32_t tcnt[kRedistTable];
+    __shared__ uint8_t tcav[kRedistTable];
+    __shared__ int overflow;
+    const uint32_t nc = min(*a.ncand, a.cand_cap);
+    if (threadIdx.x == 0 && *a.ncand > a.cand_cap) atomicOr(a.err, 1u);
+    const Grid& g = a.g;
+    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) tkey[s] = -1;
+    if (threadIdx.x == 0) overflow = 0;
+    __syncthreads();
+    for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
+        int c = a.key_cell[a.cand[m]];
+        int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+        int nb[7] = {c, i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                     j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
+                     k + 1 < g.nz ? c + g.nx * g.ny : -1};
+        for (int q = 0; q < 7; ++q) {
+            int slot = -1;
+            if (nb[q] >= 0) {
+                uint32_t h = rd_hash((uint32_t)nb[q]);
+                for (int probe = 0; probe < kRedistTable; ++probe) {
+                    int prev = atomicCAS(&tkey[h], -1, nb[q]);
+                    if (prev == -1 || prev == nb[q]) {
+                        slot = (int)h;
+                        break;
+                    }
+                    h = (h + 1) & (kRedistTable - 1);
+                }
+                if (slot < 0) overflow = 1;
+            }
+            a.slots[(size_t)m * 7 + q] = slot;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) {
+        int c = tkey[s];
+        if (c >= 0) {
+            tcnt[s] = a.count[c];
+            tcav[s] = a.cavity[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const uint32_t cap = a.cap;
+    uint32_t nm = 0;
+    if (!overflow) {
+        for (uint32_t m = 0; m < nc; ++m) {
+            const int* sl = a.slots + (size_t)m * 7;
+            int s0 = sl[0];
+            if (tcnt[s0] <= cap) continue;
+            int best = -1;
+            double best_down = -INFINITY;
+            uint32_t best_room = 0;
+            for (int q = 1; q < 7; ++q) {
+                int s = sl[q];
+                if (s < 0) continue;
+                if (!tcav[s] || tcnt[s] >= cap) continue;
+                uint32_t room = cap - tcnt[s];
+                double dn = a.down[q - 1];
+                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                    best = s;
+                    best_down = dn;
+                    best_room = room;
+                }
+            }
+            if (best >= 0) {
+                tcnt[s0] -= 1;
+                tcnt[best] += 1;
+                a.moves[2 * nm] = a.cand[m];
+                a.moves[2 * nm + 1] = (uint32_t)tkey[best];
+                ++nm;
+            }
+        }
+    } else {
+        uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
+        for (uint32_t m = 0; m < nc; ++m) {
+            int c = a.key_cell[a.cand[m]];
+            if (cnt[c] <= cap) continue;
+            int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+            int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                         j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
+                         k + 1 < g.nz ? c + g.nx * g.ny : -1};
+            int best = -1;
+            double best_down = -INFINITY;
+            uint32_t best_room = 0;
+            for (int q = 0; q < 6; ++q) {
+                int s = nb[q];
+                if (s < 0 || !a.cavity[s] || cnt[s] >= cap) continue;
+                uint32_t room = cap - cnt[s];
+                double dn = a.down[q];
+                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                    best = s;
+                    best_down = dn;
+                    best_room = room;
+                }
+            }
+            if (best >= 0) {
+                cnt[c] -= 1;
+                cnt[best] += 1;
+                a.moves[2 * nm] = a.cand[m];
+                a.moves[2 * nm + 1] = (uint32_t)best;
+                ++nm;
+            }
+        }
+    }
+    *a.nmoves = nm;
+}
+
+// Apply the recorded moves (solver.rs:545-554): position near the destination
+// cell centre with the index-keyed jitter, pushed inside, and the local grid
+// velocity.
+__global__ void k_redist_apply(Grid g, Sdf sdf, Faces f, const uint32_t* __restrict__ moves,
+                               const uint32_t* __restrict__ nmoves, float4* __restrict__ pos,
+                               float4* __restrict__ vel) {
+    uint32_t nm = *nmoves;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += gridDim.x * blockDim.x) {
+        uint32_t p = moves[2 * m], c = moves[2 * m + 1];
+        int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+        uint64_t key = p;
+        double jx = jitter_mix(key * 3), jy = jitter_mix(key * 3 + 1), jz = jitter_mix(key * 3 + 2);
+        double cx = dadd(g.ox, dmul((double)i + 0.5, g.dx));
+        double cy = dadd(g.oy, dmul((double)j + 0.5, g.dx));
+        double cz = dadd(g.oz, dmul((double)k + 0.5, g.dx));
+        float3 q = make_float3((float)dadd(cx, dmul(jx, g.dx)), (float)dadd(cy, dmul(jy, g.dx)),
+                               (float)dadd(cz, dmul(jz, g.dx)));
+        q = project_inside(sdf, 0.5f * g.dxf, q);
+        float3 v = velocity_at(g, f, q.x, q.y, q.z);
+        pos[p] = make_float4(q.x, q.y, q.z, 0.0f);
+        vel[p] = make_float4(v.x, v.y, v.z, 0.0f);
+    }
+}
+
+}  // namespace sdr

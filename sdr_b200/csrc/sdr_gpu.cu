@@ -1,0 +1,1358 @@
+// sdr_gpu.cu — host orchestration and C ABI of the B200 FLIP/PIC substep.
+//
+// One sdr_solver owns a CUDA stream, the device-resident grid/particle/solve
+// state and a pinned status block. Solver::step's CFL loop and the emission
+// RNG stay on the host in f64 (they are sequential and tiny); every other
+// phase of Solver::substep is a kernel. After each substep one small status
+// copy returns the particle count, counters and the face maxima that the
+// next cfl_dt needs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sdr_gpu.h"
+#include "common.cuh"
+#include "grid.cuh"
+#include "metrics.cuh"
+#include "particles.cuh"
+#include "pressure.cuh"
+#include "scan.cuh"
+#include "sdf.cuh"
+
+using namespace sdr;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? SDR_ERR_OOM : SDR_ERR_CUDA,      \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};               \
+    } while (0)
+
+#define LAUNCH(kern, grid, block, smem, stream, ...)                    \
+    do {                                                                \
+        kern<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);       \
+        g_launches.fetch_add(1, std::memory_order_relaxed);             \
+        CK(cudaGetLastError());                                         \
+    } while (0)
+
+inline unsigned blocks(size_t n, unsigned bs) { return (unsigned)std::max<size_t>(1, (n + bs - 1) / bs); }
+
+template <class T>
+void dalloc(T*& p, size_t n) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    CK(cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)));
+}
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// Device scalars returned to the host after every substep.
+struct DevStatus {
+    uint32_t n;             // particle count
+    uint32_t err;           // device-side error bits
+    unsigned int maxbits[3];
+    int iters;
+    double residual;
+    unsigned long long drained, culled, moves;
+    uint32_t nf;            // fluid cells of the last solve
+    uint32_t ncand;
+    uint32_t nmoves;
+    uint32_t long_count;
+    uint32_t total;         // scratch scan total
+    uint32_t hist_max;
+    unsigned long long fluid_count;
+    unsigned long long wall_count;
+};
+
+__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
+__global__ void k_add_moves(DevStatus* s) { s->moves += s->nmoves; }
+__global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[q] = (float)in[q];
+}
+__global__ void k_pack_particles(const double* __restrict__ xyz, float4* __restrict__ out, size_t n) {
+    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[q] = make_float4((float)xyz[3 * q], (float)xyz[3 * q + 1], (float)xyz[3 * q + 2], 0.f);
+}
+
+// xorshift64 (solver.rs:120-140).
+inline uint64_t rng_next(uint64_t& s) {
+    uint64_t x = s;
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    s = x;
+    return x;
+}
+inline double rng_unit(uint64_t& s) { return (double)(rng_next(s) >> 11) / (double)(1ULL << 53); }
+
+struct V3 {
+    double x, y, z;
+};
+inline V3 vadd(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 vmul(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 vcross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double vlen(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+inline V3 vnorm0(V3 a) {  // math.rs:73-80
+    double l = vlen(a);
+    if (l > 1e-12) return {a.x / l, a.y / l, a.z / l};
+    return {0, 0, 0};
+}
+
+}  // namespace
+
+struct sdr_solver {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Grid g{};
+    size_t ncell = 0, nu = 0, nv = 0, nw = 0;
+    int snx = 0, sny = 0, snz = 0;
+    double sdx = 0, sox = 0, soy = 0, soz = 0;
+    // parameters
+    sdr_fluid_params fluid{};
+    sdr_needle needle{};
+    bool has_outlet = false;
+    Aabb outlet{};
+    uint64_t max_iters = 200;
+    double tol = 1e-6;
+    // scalar state (solver.rs:155-179)
+    double time = 0.0, emit_accum = 0.0, last_residual = 0.0;
+    uint64_t steps = 0, last_pcg_iters = 0, last_substeps = 0, drained = 0;
+    uint64_t rng = 0x5deece66dULL | 1ULL;
+    uint64_t emitted = 0, culled = 0, redistributed = 0;
+    uint32_t n = 0;
+    size_t cap = 0;
+    double grid_speed = 0.0;  // MacGrid::max_speed of the current faces
+    // device state
+    double* sdf64 = nullptr;
+    float* sdf32 = nullptr;
+    float *u = nullptr, *v = nullptr, *w = nullptr, *su = nullptr, *sv = nullptr, *sw = nullptr;
+    float *u2 = nullptr, *v2 = nullptr, *w2 = nullptr;
+    uint8_t *ku = nullptr, *kv = nullptr, *kw = nullptr, *ku2 = nullptr, *kv2 = nullptr, *kw2 = nullptr;
+    uint8_t *cells = nullptr, *base = nullptr, *cavity = nullptr;
+    float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
+    int* key_cell = nullptr;
+    uint32_t *key_sort = nullptr, *perm = nullptr, *ptmp = nullptr, *flag = nullptr, *off = nullptr;
+    uint32_t *drn = nullptr;
+    uint32_t *hist_valid = nullptr, *hist_sort = nullptr, *start = nullptr, *fill = nullptr;
+    uint32_t* long_list = nullptr;
+    uint32_t* tsum = nullptr;
+    size_t tsum_cap = 0;
+    DevStatus* dst = nullptr;
+    DevStatus* hst = nullptr;  // pinned
+    // pressure
+    int nlevels = 0, nchunks = 0;
+    uint32_t *lines_cnt = nullptr, *lv_cell = nullptr, *cflag = nullptr, *coff = nullptr;
+    int *level_start = nullptr, *pos_of_cell = nullptr, *nbr = nullptr, *corder = nullptr,
+        *chunk_start = nullptr;
+    uint8_t *diag = nullptr, *nmask = nullptr;
+    double *b = nullptr, *precon = nullptr, *p = nullptr, *r = nullptr, *z = nullptr, *s = nullptr,
+           *as = nullptr, *q = nullptr, *pq = nullptr, *partials = nullptr, *p_dense = nullptr;
+    // redistribution
+    uint32_t* cand = nullptr;
+    int* slots = nullptr;
+    uint32_t* moves = nullptr;
+    // emission staging (pinned)
+    float4* h_epos = nullptr;
+    float4* h_evel = nullptr;
+    size_t h_ecap = 0;
+    // metrics scratch
+    CellPart* mcell = nullptr;
+    double* mpart = nullptr;
+    size_t mpart_cap = 0;
+    MetricsOut* mout = nullptr;
+    MetricsOut* h_mout = nullptr;
+    bool sorted_valid = false;  // perm/start describe the current particle set
+
+    double particle_volume() const {  // solver.rs:225-228
+        double cell = g.dx * g.dx * g.dx;
+        return cell / (double)std::max<uint64_t>(fluid.particles_per_cell, 1);
+    }
+    double jet_speed() const {  // solver.rs:107-114
+        double area = M_PI * needle.radius * needle.radius;
+        return area > 0.0 ? needle.flow_rate / area : 0.0;
+    }
+    Sdf sdf_f() const { return Sdf{snx, sny, snz, (float)sdx, (float)sox, (float)soy, (float)soz, sdf32}; }
+    SdfD sdf_d() const { return SdfD{snx, sny, snz, sdx, sox, soy, soz, sdf64}; }
+    Faces faces() const { return Faces{u, v, w}; }
+    Faces saved() const { return Faces{su, sv, sw}; }
+    uint32_t* dn() { return &dst->n; }
+
+    void scan(const uint32_t* in, uint32_t* out, size_t n_, uint32_t* total) {
+        if (n_ == 0) {
+            if (total) LAUNCH(k_set_u32, 1, 1, 0, st, total, 0u);
+            return;
+        }
+        uint32_t nt = (uint32_t)((n_ + kScanTile - 1) / kScanTile);
+        if (nt > tsum_cap) {
+            dalloc(tsum, nt);
+            tsum_cap = nt;
+        }
+        LAUNCH(k_scan_tiles, nt, kScanBS, 0, st, in, (uint32_t)n_, tsum);
+        LAUNCH(k_scan_sums, 1, kScanBS, 0, st, tsum, nt, total);
+        LAUNCH(k_scan_apply, nt, kScanBS, 0, st, in, (uint32_t)n_, tsum, out);
+    }
+
+    void ensure_capacity(size_t need) {
+        if (need <= cap) return;
+        size_t ncap = std::max(need + need / 2, cap + cap / 2);
+        ncap = std::max<size_t>(ncap, 1 << 16);
+        CK(cudaStreamSynchronize(st));
+        float4 *np = nullptr, *nv_ = nullptr;
+        CK(cudaMalloc((void**)&np, ncap * sizeof(float4)));
+        CK(cudaMalloc((void**)&nv_, ncap * sizeof(float4)));
+        if (n) {
+            CK(cudaMemcpyAsync(np, pos, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(nv_, vel, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        dfree(pos);
+        dfree(vel);
+        pos = np;
+        vel = nv_;
+        dalloc(pos2, ncap);
+        dalloc(vel2, ncap);
+        dalloc(key_cell, ncap);
+        dalloc(key_sort, ncap);
+        dalloc(perm, ncap);
+        dalloc(ptmp, ncap);
+        dalloc(flag, ncap + 1);
+        dalloc(off, ncap + 1);
+        dalloc(drn, ncap);
+        dalloc(cand, ncap);
+        dalloc(slots, ncap * 7);
+        dalloc(moves, ncap * 2);
+        cap = ncap;
+        sorted_valid = false;
+    }
+
+    void alloc_grid() {
+        size_t nc = ncell;
+        dalloc(u, nu); dalloc(v, nv); dalloc(w, nw);
+        dalloc(su, nu); dalloc(sv, nv); dalloc(sw, nw);
+        dalloc(u2, nu); dalloc(v2, nv); dalloc(w2, nw);
+        dalloc(ku, nu); dalloc(kv, nv); dalloc(kw, nw);
+        dalloc(ku2, nu); dalloc(kv2, nv); dalloc(kw2, nw);
+        CK(cudaMemsetAsync(u, 0, nu * 4, st));
+        CK(cudaMemsetAsync(v, 0, nv * 4, st));
+        CK(cudaMemsetAsync(w, 0, nw * 4, st));
+        CK(cudaMemsetAsync(su, 0, nu * 4, st));
+        CK(cudaMemsetAsync(sv, 0, nv * 4, st));
+        CK(cudaMemsetAsync(sw, 0, nw * 4, st));
+        dalloc(cells, nc); dalloc(base, nc); dalloc(cavity, nc);
+        CK(cudaMemsetAsync(cells, AIR, nc, st));
+        dalloc(hist_valid, nc + 1);
+        dalloc(hist_sort, nc + 1);
+        dalloc(start, nc + 1);
+        dalloc(fill, nc + 1);
+        dalloc(long_list, nc);
+        nlevels = g.nx + g.ny + g.nz - 2;
+        nchunks = (int)((nc + kDotChunk - 1) / kDotChunk);
+        dalloc(lines_cnt, (size_t)nlevels * g.nz + 1);
+        dalloc(level_start, nlevels + 1);
+        dalloc(pos_of_cell, nc);
+        dalloc(lv_cell, nc);
+        dalloc(nbr, nc * 6);
+        dalloc(diag, nc);
+        dalloc(nmask, nc);
+        dalloc(b, nc); dalloc(precon, nc); dalloc(p, nc); dalloc(r, nc); dalloc(z, nc);
+        dalloc(s, nc); dalloc(as, nc); dalloc(q, nc); dalloc(pq, nc);
+        dalloc(partials, nchunks + 1);
+        dalloc(corder, nc);
+        dalloc(chunk_start, nchunks + 1);
+        dalloc(cflag, nc);
+        dalloc(coff, nc);
+        dalloc(p_dense, nc);
+        CK(cudaMemsetAsync(p_dense, 0, nc * 8, st));
+        dalloc(mcell, blocks(nc, kMetBS));
+        dalloc(mout, 1);
+    }
+
+    void free_all() {
+        dfree(sdf64); dfree(sdf32);
+        dfree(u); dfree(v); dfree(w); dfree(su); dfree(sv); dfree(sw); dfree(u2); dfree(v2); dfree(w2);
+        dfree(ku); dfree(kv); dfree(kw); dfree(ku2); dfree(kv2); dfree(kw2);
+        dfree(cells); dfree(base); dfree(cavity);
+        dfree(pos); dfree(vel); dfree(pos2); dfree(vel2);
+        dfree(key_cell); dfree(key_sort); dfree(perm); dfree(ptmp); dfree(flag); dfree(off); dfree(drn);
+        dfree(hist_valid); dfree(hist_sort); dfree(start); dfree(fill); dfree(long_list); dfree(tsum);
+        dfree(dst);
+        dfree(lines_cnt); dfree(lv_cell); dfree(cflag); dfree(coff); dfree(level_start); dfree(pos_of_cell);
+        dfree(nbr); dfree(corder); dfree(chunk_start); dfree(diag); dfree(nmask);
+        dfree(b); dfree(precon); dfree(p); dfree(r); dfree(z); dfree(s); dfree(as); dfree(q); dfree(pq);
+        dfree(partials); dfree(p_dense);
+        dfree(cand); dfree(slots); dfree(moves);
+        dfree(mcell); dfree(mpart); dfree(mout);
+        if (hst) cudaFreeHost(hst);
+        if (h_epos) cudaFreeHost(h_epos);
+        if (h_evel) cudaFreeHost(h_evel);
+        if (h_mout) cudaFreeHost(h_mout);
+        hst = nullptr; h_epos = nullptr; h_evel = nullptr; h_mout = nullptr;
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+
+    void refresh_base() {
+        LAUNCH(k_cavity_and_base, blocks(ncell, 256), 256, 0, st, g, sdf_d(), (int)has_outlet, outlet,
+               cavity, base, 0);
+    }
+
+    // ---------------------------------------------------------------- phases
+    void emit(double dt) {  // solver.rs:313-339
+        double pv = particle_volume();
+        if (pv <= 0.0 || needle.flow_rate <= 0.0 || time >= needle.inject_until) return;
+        emit_accum += needle.flow_rate * dt / pv;
+        double count = std::floor(emit_accum);
+        size_t k = (size_t)count;
+        emit_accum -= count;
+        if (k == 0) return;
+        ensure_capacity((size_t)n + k);
+        if (k > h_ecap) {
+            CK(cudaStreamSynchronize(st));
+            if (h_epos) cudaFreeHost(h_epos);
+            if (h_evel) cudaFreeHost(h_evel);
+            h_epos = h_evel = nullptr;
+            size_t c = std::max<size_t>(k * 2, 4096);
+            CK(cudaMallocHost((void**)&h_epos, c * sizeof(float4)));
+            CK(cudaMallocHost((void**)&h_evel, c * sizeof(float4)));
+            h_ecap = c;
+        }
+        V3 axis = vnorm0({needle.axis.x, needle.axis.y, needle.axis.z});
+        V3 a = std::fabs(axis.x) < 0.9 ? V3{1, 0, 0} : V3{0, 1, 0};  // solver.rs:933-942
+        V3 e1 = vnorm0(vcross(axis, a));
+        V3 e2 = vnorm0(vcross(axis, e1));
+        V3 vv = vmul(axis, jet_speed());
+        V3 tip{needle.tip.x, needle.tip.y, needle.tip.z};
+        for (size_t i = 0; i < k; ++i) {
+            double rr = needle.radius * std::sqrt(rng_unit(rng));
+            double th = 2.0 * M_PI * rng_unit(rng);
+            double along = (rng_unit(rng) - 0.5) * g.dx;
+            V3 ps = vadd(vadd(vadd(tip, vmul(e1, rr * std::cos(th))), vmul(e2, rr * std::sin(th))),
+                         vmul(axis, along));
+            h_epos[i] = make_float4((float)ps.x, (float)ps.y, (float)ps.z, 0.f);
+            h_evel[i] = make_float4((float)vv.x, (float)vv.y, (float)vv.z, 0.f);
+        }
+        CK(cudaMemcpyAsync(pos + n, h_epos, k * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(vel + n, h_evel, k * sizeof(float4), cudaMemcpyHostToDevice, st));
+        // The staging buffers are reused next substep; the status sync at the
+        // end of this substep orders the copies before any reuse.
+        n += (uint32_t)k;
+        emitted += k;
+        LAUNCH(k_set_u32, 1, 1, 0, st, dn(), n);
+        sorted_valid = false;
+    }
+
+    void classify(bool mark) {
+        CK(cudaMemsetAsync(hist_valid, 0, (ncell + 1) * 4, st));
+        CK(cudaMemsetAsync(hist_sort, 0, (ncell + 1) * 4, st));
+        if (mark) LAUNCH(k_base_labels, blocks(ncell, 256), 256, 0, st, base, cells, ncell);
+        if (n)
+            LAUNCH(k_classify_keys, blocks(n, kBS), kBS, 0, st, g, pos, n, (int)has_outlet, outlet,
+                   (int)mark, cells, key_cell, key_sort, hist_valid, hist_sort);
+    }
+
+    void sort() {  // counting sort by the f32 P2G cell key
+        scan(hist_sort, start, ncell + 1, &dst->total);
+        CK(cudaMemcpyAsync(fill, start, ncell * 4, cudaMemcpyDeviceToDevice, st));
+        if (n) LAUNCH(k_sort_scatter, blocks(n, kBS), kBS, 0, st, key_sort, n, fill, perm);
+        CK(cudaMemsetAsync(&dst->long_count, 0, 4, st));
+        LAUNCH(k_sort_segments, blocks(ncell, 256), 256, 0, st, start, (uint32_t)ncell, perm, long_list,
+               &dst->long_count);
+        LAUNCH(k_sort_long, 148, 256, 0, st, start, long_list, &dst->long_count, perm, ptmp);
+        sorted_valid = true;
+    }
+
+    void p2g(double dt, bool fused) {
+        P2GArgs a{};
+        a.g = g;
+        a.pos = pos;
+        a.vel = vel;
+        a.start = start;
+        a.perm = perm;
+        a.u = u; a.v = v; a.w = w;
+        a.su = su; a.sv = sv; a.sw = sw;
+        a.cells = cells;
+        a.gdt[0] = fluid.gravity.x * dt;
+        a.gdt[1] = fluid.gravity.y * dt;
+        a.gdt[2] = fluid.gravity.z * dt;
+        a.add_forces = fused;
+        a.enforce = fused;
+        dim3 grid(blocks(g.nx + 1, kBS), g.ny + 1, g.nz + 1);
+        LAUNCH(k_p2g, grid, kBS, 0, st, a);
+    }
+
+    void add_forces(double dt) {  // solver.rs:593-604
+        if (fluid.gravity.x != 0.0) LAUNCH(k_add_forces, blocks(nu, 256), 256, 0, st, u, nu, fluid.gravity.x * dt);
+        if (fluid.gravity.y != 0.0) LAUNCH(k_add_forces, blocks(nv, 256), 256, 0, st, v, nv, fluid.gravity.y * dt);
+        if (fluid.gravity.z != 0.0) LAUNCH(k_add_forces, blocks(nw, 256), 256, 0, st, w, nw, fluid.gravity.z * dt);
+    }
+
+    void project(double dt, bool enforce) {  // pressure.rs:123-239 + solver.rs:290-300
+        dim3 ngrid(blocks(g.nx + 1, 256), g.ny + 1, g.nz + 1);
+        if (enforce) LAUNCH(k_enforce_solid, ngrid, 256, 0, st, g, cells, u, v, w);
+        size_t nl = (size_t)nlevels * g.nz;
+        LAUNCH(k_lines_count, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt);
+        CK(cudaMemsetAsync(lines_cnt + nl, 0, 4, st));
+        scan(lines_cnt, lines_cnt, nl + 1, &dst->nf);
+        LAUNCH(k_lines_assign, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt, pos_of_cell, lv_cell);
+        LAUNCH(k_level_starts_dev, blocks(nlevels + 1, 256), 256, 0, st, lines_cnt, nlevels, g.nz, &dst->nf,
+               level_start);
+        TableArgs t{};
+        t.g = g;
+        t.cells = cells;
+        t.pos_of_cell = pos_of_cell;
+        t.lv_cell = lv_cell;
+        t.nf = &dst->nf;
+        t.nbr = nbr;
+        t.diag = diag;
+        t.nmask = nmask;
+        t.b = b;
+        t.u = u; t.v = v; t.w = w;
+        t.hist = hist_valid;
+        t.inv_scale = fluid.density * g.dx / dt;
+        double k_vol = fluid.volume_stiffness;
+        t.vs_on = (k_vol > 0.0 && dt > 0.0) ? 1 : 0;
+        t.vs_rest = (double)std::max<uint64_t>(fluid.particles_per_cell, 1);
+        t.vs_k = k_vol;
+        t.vs_unit = g.dx / dt;
+        t.vs_cap = 0.25 * t.vs_unit;
+        LAUNCH(k_tables, blocks(ncell, 256), 256, 0, st, t);
+        LAUNCH(k_fluid_flags, blocks(ncell, 256), 256, 0, st, cells, ncell, cflag);
+        scan(cflag, coff, ncell, nullptr);
+        LAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, chunk_start,
+               nchunks, &dst->nf);
+        CK(cudaMemsetAsync(p_dense, 0, ncell * 8, st));
+        PcgArgs a{};
+        a.nf = &dst->nf;
+        a.nlevels = nlevels;
+        a.nchunks = nchunks;
+        a.level_start = level_start;
+        a.nbr = nbr;
+        a.diag = diag;
+        a.nmask = nmask;
+        a.corder = corder;
+        a.chunk_start = chunk_start;
+        a.b = b;
+        a.precon = precon; a.p = p; a.r = r; a.z = z; a.s = s; a.as = as; a.q = q; a.pq = pq;
+        a.partials = partials;
+        a.tol = tol;
+        a.max_iters = (int)std::min<uint64_t>(max_iters, (uint64_t)INT32_MAX);
+        a.lv_cell = lv_cell;
+        a.p_dense = p_dense;
+        a.out_iters = &dst->iters;
+        a.out_residual = &dst->residual;
+        LAUNCH(k_pcg, 1, kPcgBS, 2 * kPcgWin * sizeof(double), st, a);
+        double coef = dt / (fluid.density * g.dx);
+        LAUNCH(k_gradient, ngrid, 256, 0, st, g, cells, p_dense, coef, u, v, w);
+    }
+
+    void extrapolate() {  // solver.rs:608-647
+        dim3 ngrid(blocks(g.nx + 1, 256), g.ny + 1, g.nz + 1);
+        LAUNCH(k_extrap_valid, ngrid, 256, 0, st, g, cells, ku, kv, kw);
+        CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
+        float *a_u = u, *a_v = v, *a_w = w, *b_u = u2, *b_v = v2, *b_w = w2;
+        uint8_t *a_ku = ku, *a_kv = kv, *a_kw = kw, *b_ku = ku2, *b_kv = kv2, *b_kw = kw2;
+        for (int it = 0; it < 4; ++it) {
+            ExtrapArgs e{g, a_u, a_v, a_w, a_ku, a_kv, a_kw, b_u, b_v, b_w, b_ku, b_kv, b_kw,
+                         it == 3 ? dst->maxbits : nullptr};
+            LAUNCH(k_extrap, ngrid, 256, 0, st, e);
+            std::swap(a_u, b_u); std::swap(a_v, b_v); std::swap(a_w, b_w);
+            std::swap(a_ku, b_ku); std::swap(a_kv, b_kv); std::swap(a_kw, b_kw);
+        }
+        // four sweeps: the result is back in u, v, w
+    }
+
+    void face_max() {
+        CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
+        LAUNCH(k_face_max, 296, 256, 0, st, u, nu, &dst->maxbits[0]);
+        LAUNCH(k_face_max, 296, 256, 0, st, v, nv, &dst->maxbits[1]);
+        LAUNCH(k_face_max, 296, 256, 0, st, w, nw, &dst->maxbits[2]);
+    }
+
+    MoveArgs move_args(double dt) {
+        MoveArgs a{};
+        a.g = g;
+        a.sdf = sdf_f();
+        a.pos = pos;
+        a.vel = vel;
+        a.order = nullptr;
+        a.n = n;
+        a.f = faces();
+        a.saved = saved();
+        a.flip = (float)std::min(1.0, std::max(0.0, fluid.flip_ratio));
+        a.dt = (float)dt;
+        double bmx[3] = {sox + (double)(snx - 1) * sdx, soy + (double)(sny - 1) * sdx, soz + (double)(snz - 1) * sdx};
+        a.bb = Aabb{{sox, soy, soz}, {bmx[0], bmx[1], bmx[2]}};
+        a.has_outlet = has_outlet;
+        a.outlet = outlet;
+        a.cull_phi = (float)(0.5 * sdx);
+        a.keep = flag;
+        a.drained = drn;
+        return a;
+    }
+
+    void g2p_advect(double dt, bool g2p_on, bool advect_on, bool bounds_on, bool use_order) {
+        if (!n) return;
+        MoveArgs a = move_args(dt);
+        a.order = use_order && sorted_valid ? perm : nullptr;
+        a.do_g2p = g2p_on;
+        a.do_advect = advect_on;
+        a.do_bounds = bounds_on;
+        LAUNCH(k_g2p_advect, blocks(n, kBS), kBS, 0, st, a);
+    }
+
+    void compact(bool flags_ready) {  // solver.rs:736-755
+        if (!n) return;
+        if (!flags_ready) {
+            MoveArgs a = move_args(0.0);
+            LAUNCH(k_bounds_flags, blocks(n, kBS), kBS, 0, st, a);
+        }
+        scan(flag, off, n, dn());
+        LAUNCH(k_compact, blocks(n, kBS), kBS, 0, st, pos, vel, flag, drn, off, n, pos2, vel2, &dst->drained);
+        std::swap(pos, pos2);
+        std::swap(vel, vel2);
+        sorted_valid = false;
+    }
+
+    void redistribute(uint32_t n_upper) {  // solver.rs:454-557
+        if (!n_upper) return;
+        uint32_t cap_ = (uint32_t)std::ceil(std::max(fluid.redist_cap_factor, 1.0) *
+                                             (double)std::max<uint64_t>(fluid.particles_per_cell, 1));
+        V3 gd = vnorm0({fluid.gravity.x, fluid.gravity.y, fluid.gravity.z});
+        RedistArgs ra{};
+        ra.g = g;
+        ra.key_cell = key_cell;
+        ra.count = hist_valid;
+        ra.cavity = cavity;
+        ra.cand = cand;
+        ra.ncand = &dst->ncand;
+        ra.cand_cap = (uint32_t)cap;
+        ra.slots = slots;
+        ra.cap = cap_;
+        const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+        for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
+        ra.moves = moves;
+        ra.nmoves = &dst->nmoves;
+        ra.err = &dst->err;
+        for (int sweep = 0; sweep < 4; ++sweep) {
+            CK(cudaMemsetAsync(hist_valid, 0, ncell * 4, st));
+            LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), key_cell, hist_valid);
+            LAUNCH(k_redist_flag_n, blocks(n_upper, kBS), kBS, 0, st, key_cell, hist_valid, dn(), n_upper, cap_,
+                   flag);
+            scan(flag, off, n_upper, &dst->ncand);
+            LAUNCH(k_redist_gather, blocks(n_upper, kBS), kBS, 0, st, flag, off, n_upper, cand);
+            LAUNCH(k_redist_replay, 1, kRedistBS, 0, st, ra);
+            LAUNCH(k_redist_apply, 148, 256, 0, st, g, sdf_f(), faces(), moves, &dst->nmoves, pos, vel);
+            LAUNCH(k_add_moves, 1, 1, 0, st, dst);
+        }
+        sorted_valid = false;
+    }
+
+    void sync_status() {
+        CK(cudaMemcpyAsync(hst, dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        n = hst->n;
+        drained = hst->drained;
+        culled = hst->culled;
+        redistributed = hst->moves;
+        if (hst->err) throw Fail{SDR_ERR_CAPACITY, "device work list overflow (error bits " + std::to_string(hst->err) + ")"};
+    }
+
+    void read_grid_speed() {
+        float mu, mv, mw;
+        std::memcpy(&mu, &hst->maxbits[0], 4);
+        std::memcpy(&mv, &hst->maxbits[1], 4);
+        std::memcpy(&mw, &hst->maxbits[2], 4);
+        double a = mu, b_ = mv, c = mw;
+        grid_speed = std::sqrt(a * a + b_ * b_ + c * c);  // grid.rs:202-206
+    }
+
+    void substep(double dt) {  // solver.rs:284-310
+        emit(dt);
+        classify(true);
+        sort();
+        p2g(dt, true);
+        project(dt, false);
+        extrapolate();
+        g2p_advect(dt, true, true, true, true);
+        uint32_t n_before = n;
+        compact(true);
+        if (fluid.redistribute) redistribute(n_before);
+        sync_status();
+        last_pcg_iters = (uint64_t)hst->iters;
+        last_residual = hst->residual;
+        read_grid_speed();
+        time += dt;
+        steps += 1;
+    }
+
+    double cfl_dt() const {  // solver.rs:262-281
+        double jet = time < needle.inject_until ? jet_speed() : 0.0;
+        double gl = std::sqrt(fluid.gravity.x * fluid.gravity.x + fluid.gravity.y * fluid.gravity.y +
+                              fluid.gravity.z * fluid.gravity.z);
+        double gg = std::sqrt(gl * g.dx);
+        double speed = std::fmax(std::fmax(std::fmax(grid_speed, jet), gg), 1e-6);
+        return std::fmin(g.dx / speed, 0.01);
+    }
+
+    void step(double dt) {  // solver.rs:237-259
+        const uint32_t MAX_SUBSTEPS = 512;
+        double floor_ = dt / (double)MAX_SUBSTEPS;
+        double remaining = dt;
+        uint32_t taken = 0;
+        while (remaining > 1e-12) {
+            double sub = std::fmin(std::fmax(cfl_dt(), floor_), remaining);
+            substep(sub);
+            remaining -= sub;
+            ++taken;
+        }
+        last_substeps = taken;
+    }
+
+    void run_phase(int ph, double dt) {
+        switch (ph) {
+            case SDR_PHASE_EMIT: emit(dt); break;
+            case SDR_PHASE_CLASSIFY: classify(true); break;
+            case SDR_PHASE_P2G:
+                classify(false);
+                sort();
+                p2g(dt, false);
+                break;
+            case SDR_PHASE_ADD_FORCES: add_forces(dt); break;
+            case SDR_PHASE_PROJECT:
+                classify(false);  // refresh the per-cell counts of the volume source
+                project(dt, true);
+                break;
+            case SDR_PHASE_EXTRAPOLATE: extrapolate(); break;
+            case SDR_PHASE_G2P: g2p_advect(dt, true, false, false, false); break;
+            case SDR_PHASE_ADVECT: g2p_advect(dt, false, true, false, false); break;
+            case SDR_PHASE_BOUNDS: compact(false); break;
+            case SDR_PHASE_REDISTRIBUTE:
+                if (fluid.redistribute) redistribute(n);
+                break;
+            case SDR_PHASE_CLOCK:
+                time += dt;
+                steps += 1;
+                break;
+            default: throw Fail{SDR_ERR_INVALID, "unknown phase"};
+        }
+        if (ph != SDR_PHASE_CLOCK) {
+            sync_status();
+            if (ph == SDR_PHASE_PROJECT) {
+                last_pcg_iters = (uint64_t)hst->iters;
+                last_residual = hst->residual;
+            }
+            if (ph == SDR_PHASE_EXTRAPOLATE) read_grid_speed();
+        }
+    }
+};
+
+struct sdr_metrics {
+    sdr_solver* owner = nullptr;
+    double cavity_volume = 0;
+    uint8_t *is_wall = nullptr, *washed = nullptr, *wet = nullptr;
+    uint64_t wall_count = 0;
+    std::vector<sdr_frame_metrics> history;
+    double injected_ml = 0.0;
+};
+
+// ---------------------------------------------------------------- helpers
+namespace {
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        g_err.clear();
+        return SDR_OK;
+    } catch (const Fail& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return SDR_ERR_OOM;
+    } catch (...) {
+        g_err = "unknown error";
+        return SDR_ERR_CUDA;
+    }
+}
+
+void require(bool c, const char* msg) {
+    if (!c) throw Fail{SDR_ERR_INVALID, msg};
+}
+
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        cudaGetDevice(&prev);
+        if (dev >= 0 && dev != prev) CK(cudaSetDevice(dev));
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void check_device() {
+    int nd = 0;
+    cudaError_t e = cudaGetDeviceCount(&nd);
+    if (e != cudaSuccess || nd == 0)
+        throw Fail{SDR_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e)};
+}
+
+}  // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+int sdr_abi_version(void) { return SDR_ABI_VERSION; }
+const char* sdr_last_error(void) { return g_err.c_str(); }
+uint64_t sdr_kernel_launch_count(void) { return g_launches.load(); }
+
+int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_params* fluid,
+                      const sdr_needle* needle, const sdr_solver_options* options, sdr_solver** out) {
+    return guard([&] {
+        require(sdf && fluid && needle && out, "null argument");
+        require(sdf->data && sdf->nx >= 2 && sdf->ny >= 2 && sdf->nz >= 2, "SDF needs >= 2 nodes per axis");
+        require(sdf->dx > 0 && sim_dx > 0, "dx must be positive");
+        *out = nullptr;
+        check_device();
+        int dev = options ? options->device : -1;
+        DeviceScope ds(dev);
+        sdr_solver* s = new sdr_solver();
+        try {
+            CK(cudaGetDevice(&s->device));
+            cudaDeviceProp prop;
+            CK(cudaGetDeviceProperties(&prop, s->device));
+            if (prop.major != 10)
+                throw Fail{SDR_ERR_NO_DEVICE, "this library is built for sm_100a (B200); device is sm_" +
+                                                  std::to_string(prop.major) + std::to_string(prop.minor)};
+            CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+            CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(2 * kPcgWin * sizeof(double))));
+            s->fluid = *fluid;
+            s->needle = *needle;
+            s->snx = (int)sdf->nx; s->sny = (int)sdf->ny; s->snz = (int)sdf->nz;
+            s->sdx = sdf->dx;
+            s->sox = sdf->origin.x; s->soy = sdf->origin.y; s->soz = sdf->origin.z;
+            // Solver::new grid (solver.rs:185-190)
+            double bx = s->sox + (double)(s->snx - 1) * s->sdx, by = s->soy + (double)(s->sny - 1) * s->sdx,
+                   bz = s->soz + (double)(s->snz - 1) * s->sdx;
+            double sx = bx - s->sox, sy = by - s->soy, sz = bz - s->soz;
+            size_t nx = (size_t)std::fmax(std::ceil(sx / sim_dx), 1.0);
+            size_t ny = (size_t)std::fmax(std::ceil(sy / sim_dx), 1.0);
+            size_t nz = (size_t)std::fmax(std::ceil(sz / sim_dx), 1.0);
+            require(nx * ny * nz < (size_t)INT32_MAX / 8, "grid too large");
+            require(nx >= 2 && ny >= 2 && nz >= 2, "grid needs >= 2 cells per axis");
+            Grid& g = s->g;
+            g.nx = (int)nx; g.ny = (int)ny; g.nz = (int)nz;
+            g.dx = sim_dx; g.ox = s->sox; g.oy = s->soy; g.oz = s->soz;
+            g.dxf = (float)sim_dx; g.oxf = (float)g.ox; g.oyf = (float)g.oy; g.ozf = (float)g.oz;
+            s->ncell = nx * ny * nz;
+            s->nu = (nx + 1) * ny * nz;
+            s->nv = nx * (ny + 1) * nz;
+            s->nw = nx * ny * (nz + 1);
+            size_t sn = sdf->nx * sdf->ny * sdf->nz;
+            dalloc(s->sdf64, sn);
+            dalloc(s->sdf32, sn);
+            CK(cudaMemcpyAsync(s->sdf64, sdf->data, sn * 8, cudaMemcpyHostToDevice, s->st));
+            LAUNCH(k_f64_to_f32, blocks(sn, 256), 256, 0, s->st, s->sdf64, s->sdf32, sn);
+            dalloc(s->dst, 1);
+            CK(cudaMemsetAsync(s->dst, 0, sizeof(DevStatus), s->st));
+            CK(cudaMallocHost((void**)&s->hst, sizeof(DevStatus)));
+            CK(cudaMallocHost((void**)&s->h_mout, sizeof(MetricsOut)));
+            std::memset(s->hst, 0, sizeof(DevStatus));
+            s->alloc_grid();
+            LAUNCH(k_cavity_and_base, blocks(s->ncell, 256), 256, 0, s->st, g, s->sdf_d(), 0, Aabb{}, s->cavity,
+                   s->base, 1);
+            size_t want = options && options->max_particles ? options->max_particles
+                                                             : std::min<size_t>(s->ncell * 2, 1 << 22);
+            s->ensure_capacity(std::max<size_t>(want, 1 << 16));
+            CK(cudaStreamSynchronize(s->st));
+        } catch (...) {
+            s->free_all();
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int sdr_solver_destroy(sdr_solver* s) {
+    return guard([&] {
+        if (!s) return;
+        DeviceScope ds(s->device);
+        if (s->st) cudaStreamSynchronize(s->st);
+        s->free_all();
+        delete s;
+    });
+}
+
+int sdr_solver_set_outlet(sdr_solver* s, const sdr_aabb* o) {
+    return guard([&] {
+        require(s, "null solver");
+        DeviceScope ds(s->device);
+        s->has_outlet = o != nullptr;
+        if (o) s->outlet = Aabb{{o->min.x, o->min.y, o->min.z}, {o->max.x, o->max.y, o->max.z}};
+        s->refresh_base();
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int sdr_solver_set_solve_params(sdr_solver* s, const sdr_solve_params* p) {
+    return guard([&] {
+        require(s && p, "null argument");
+        s->max_iters = p->max_iters;
+        s->tol = p->tol;
+    });
+}
+
+int sdr_solver_set_needle(sdr_solver* s, const sdr_needle* nd) {
+    return guard([&] {
+        require(s && nd, "null argument");
+        s->needle = *nd;
+    });
+}
+
+int sdr_solver_step(sdr_solver* s, double dt) {
+    return guard([&] {
+        require(s, "null solver");
+        require(std::isfinite(dt) && dt >= 0.0, "dt must be finite and non-negative");
+        DeviceScope ds(s->device);
+        s->step(dt);
+    });
+}
+
+int sdr_solver_substep(sdr_solver* s, double dt) {
+    return guard([&] {
+        require(s, "null solver");
+        require(std::isfinite(dt) && dt > 0.0, "dt must be finite and positive");
+        DeviceScope ds(s->device);
+        s->substep(dt);
+    });
+}
+
+int sdr_solver_run_phase(sdr_solver* s, int phase, double dt) {
+    return guard([&] {
+        require(s, "null solver");
+        DeviceScope ds(s->device);
+        s->run_phase(phase, dt);
+    });
+}
+
+int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* o) {
+    return guard([&] {
+        require(s && o, "null argument");
+        o->time = s->time;
+        o->steps = s->steps;
+        o->last_pcg_iters = s->last_pcg_iters;
+        o->last_substeps = s->last_substeps;
+        o->particles = s->n;
+        o->drained = s->drained;
+        o->last_residual = s->last_residual;
+        o->emit_accum = s->emit_accum;
+        o->rng_state = s->rng;
+        o->emitted = s->emitted;
+        o->culled = s->culled;
+        o->redistributed = s->redistributed;
+        o->nx = s->g.nx; o->ny = s->g.ny; o->nz = s->g.nz;
+        o->dx = s->g.dx;
+        o->origin = sdr_vec3{s->g.ox, s->g.oy, s->g.oz};
+    });
+}
+
+int sdr_solver_set_scalars(sdr_solver* s, double time, double emit_accum, uint64_t steps, uint64_t drained,
+                           uint64_t rng_state) {
+    return guard([&] {
+        require(s, "null solver");
+        DeviceScope ds(s->device);
+        s->time = time;
+        s->emit_accum = emit_accum;
+        s->steps = steps;
+        s->rng = rng_state;
+        s->drained = drained;
+        unsigned long long d = drained;
+        CK(cudaMemcpyAsync(&s->dst->drained, &d, sizeof(d), cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int sdr_solver_copy_particles(sdr_solver* s, double* pos_xyz, double* vel_xyz, size_t cap, size_t* n_out) {
+    return guard([&] {
+        require(s, "null solver");
+        if (n_out) *n_out = s->n;
+        if (cap < s->n) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the particle count"};
+        DeviceScope ds(s->device);
+        std::vector<float4> tmp(s->n);
+        for (int which = 0; which < 2; ++which) {
+            double* dstp = which == 0 ? pos_xyz : vel_xyz;
+            if (!dstp || !s->n) continue;
+            CK(cudaMemcpyAsync(tmp.data(), which == 0 ? s->pos : s->vel, s->n * sizeof(float4),
+                               cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (size_t i = 0; i < s->n; ++i) {
+                dstp[3 * i] = tmp[i].x;
+                dstp[3 * i + 1] = tmp[i].y;
+                dstp[3 * i + 2] = tmp[i].z;
+            }
+        }
+    });
+}
+
+int sdr_solver_copy_particles_f32(sdr_solver* s, float* pos_xyz, float* vel_xyz, size_t cap, size_t* n_out) {
+    return guard([&] {
+        require(s, "null solver");
+        if (n_out) *n_out = s->n;
+        if (cap < s->n) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the particle count"};
+        DeviceScope ds(s->device);
+        if (!s->n) return;
+        for (int which = 0; which < 2; ++which) {
+            float* dstp = which == 0 ? pos_xyz : vel_xyz;
+            if (!dstp) continue;
+            CK(cudaMemcpy2DAsync(dstp, 3 * sizeof(float), which == 0 ? s->pos : s->vel, sizeof(float4),
+                                 3 * sizeof(float), s->n, cudaMemcpyDeviceToHost, s->st));
+        }
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int sdr_solver_set_particles(sdr_solver* s, const double* pos_xyz, const double* vel_xyz, size_t n) {
+    return guard([&] {
+        require(s && (n == 0 || (pos_xyz && vel_xyz)), "null argument");
+        require(n < (size_t)UINT32_MAX / 2, "too many particles");
+        DeviceScope ds(s->device);
+        s->ensure_capacity(n);
+        if (n) {
+            double* tmp = nullptr;
+            CK(cudaMalloc((void**)&tmp, n * 3 * sizeof(double)));
+            try {
+                CK(cudaMemcpyAsync(tmp, pos_xyz, n * 24, cudaMemcpyHostToDevice, s->st));
+                LAUNCH(k_pack_particles, blocks(n, 256), 256, 0, s->st, tmp, s->pos, n);
+                CK(cudaMemcpyAsync(tmp, vel_xyz, n * 24, cudaMemcpyHostToDevice, s->st));
+                LAUNCH(k_pack_particles, blocks(n, 256), 256, 0, s->st, tmp, s->vel, n);
+                CK(cudaStreamSynchronize(s->st));
+            } catch (...) {
+                cudaFree(tmp);
+                throw;
+            }
+            cudaFree(tmp);
+        }
+        s->n = (uint32_t)n;
+        LAUNCH(k_set_u32, 1, 1, 0, s->st, s->dn(), s->n);
+        s->sorted_valid = false;
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+static int copy_dev(sdr_solver* s, const void* src, size_t bytes, void* out) {
+    CK(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int sdr_solver_copy_pressure(sdr_solver* s, double* out, size_t cap) {
+    return guard([&] {
+        require(s && out, "null argument");
+        if (cap < s->ncell) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the cell count"};
+        DeviceScope ds(s->device);
+        copy_dev(s, s->p_dense, s->ncell * 8, out);
+    });
+}
+
+int sdr_solver_copy_cells(sdr_solver* s, uint8_t* out, size_t cap) {
+    return guard([&] {
+        require(s && out, "null argument");
+        if (cap < s->ncell) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the cell count"};
+        DeviceScope ds(s->device);
+        copy_dev(s, s->cells, s->ncell, out);
+    });
+}
+
+int sdr_solver_copy_cavity_mask(sdr_solver* s, uint8_t* out, size_t cap) {
+    return guard([&] {
+        require(s && out, "null argument");
+        if (cap < s->ncell) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the cell count"};
+        DeviceScope ds(s->device);
+        copy_dev(s, s->cavity, s->ncell, out);
+    });
+}
+
+static float* face_ptr(sdr_solver* s, int which, size_t& len) {
+    switch (which) {
+        case 0: len = s->nu; return s->u;
+        case 1: len = s->nv; return s->v;
+        case 2: len = s->nw; return s->w;
+        case 3: len = s->nu; return s->su;
+        case 4: len = s->nv; return s->sv;
+        case 5: len = s->nw; return s->sw;
+    }
+    throw Fail{SDR_ERR_INVALID, "face index must be 0..5"};
+}
+
+int sdr_solver_copy_face(sdr_solver* s, int which, double* out, size_t cap) {
+    return guard([&] {
+        require(s && out, "null argument");
+        size_t len = 0;
+        float* f = face_ptr(s, which, len);
+        if (cap < len) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the face count"};
+        DeviceScope ds(s->device);
+        std::vector<float> tmp(len);
+        copy_dev(s, f, len * 4, tmp.data());
+        for (size_t i = 0; i < len; ++i) out[i] = tmp[i];
+    });
+}
+
+int sdr_solver_set_face(sdr_solver* s, int which, const double* in, size_t n) {
+    return guard([&] {
+        require(s && in, "null argument");
+        size_t len = 0;
+        float* f = face_ptr(s, which, len);
+        require(n == len, "face length mismatch");
+        DeviceScope ds(s->device);
+        std::vector<float> tmp(len);
+        for (size_t i = 0; i < len; ++i) tmp[i] = (float)in[i];
+        CK(cudaMemcpyAsync(f, tmp.data(), len * 4, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int sdr_solver_copy_sort(sdr_solver* s, uint32_t* keys, uint32_t* perm, size_t cap, size_t* n_out) {
+    return guard([&] {
+        require(s, "null solver");
+        if (n_out) *n_out = s->n;
+        if (cap < s->n) throw Fail{SDR_ERR_BUFFER, "buffer smaller than the particle count"};
+        require(s->sorted_valid, "no counting sort for the current particle set (run the P2G phase)");
+        DeviceScope ds(s->device);
+        if (keys && s->n) copy_dev(s, s->key_sort, s->n * 4, keys);
+        if (perm && s->n) copy_dev(s, s->perm, s->n * 4, perm);
+    });
+}
+
+int sdr_solver_max_pressure(sdr_solver* s, double* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        std::vector<double> p(s->ncell);
+        std::vector<uint8_t> c(s->ncell);
+        copy_dev(s, s->p_dense, s->ncell * 8, p.data());
+        copy_dev(s, s->cells, s->ncell, c.data());
+        double m = 0.0;
+        for (size_t i = 0; i < s->ncell; ++i)
+            if (c[i] == FLUID) m = std::fmax(m, p[i]);
+        *out = m;
+    });
+}
+
+int sdr_solver_mean_pressure(sdr_solver* s, double* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        std::vector<double> p(s->ncell);
+        std::vector<uint8_t> c(s->ncell);
+        copy_dev(s, s->p_dense, s->ncell * 8, p.data());
+        copy_dev(s, s->cells, s->ncell, c.data());
+        double sum = 0.0;
+        uint64_t k = 0;
+        for (size_t i = 0; i < s->ncell; ++i)
+            if (c[i] == FLUID) {
+                sum += p[i];
+                ++k;
+            }
+        *out = k ? sum / (double)k : 0.0;
+    });
+}
+
+int sdr_solver_max_speed(sdr_solver* s, double* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        std::vector<float4> v(s->n);
+        if (s->n) copy_dev(s, s->vel, s->n * sizeof(float4), v.data());
+        double m = 0.0;
+        for (auto& x : v) m = std::fmax(m, std::sqrt((double)x.x * x.x + (double)x.y * x.y + (double)x.z * x.z));
+        *out = m;
+    });
+}
+
+int sdr_solver_cells_fluid_count(sdr_solver* s, uint64_t* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        CK(cudaMemsetAsync(&s->dst->fluid_count, 0, 8, s->st));
+        LAUNCH(k_count_fluid, blocks(s->ncell, kMetBS), kMetBS, 0, s->st, s->cells, s->ncell, &s->dst->fluid_count);
+        unsigned long long v = 0;
+        copy_dev(s, &s->dst->fluid_count, 8, &v);
+        *out = v;
+    });
+}
+
+int sdr_solver_max_particles_per_cell(sdr_solver* s, uint64_t* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        s->classify(false);
+        CK(cudaMemsetAsync(&s->dst->hist_max, 0, 4, s->st));
+        LAUNCH(k_hist_max, 148, 256, 0, s->st, s->hist_valid, s->ncell, &s->dst->hist_max);
+        uint32_t v = 0;
+        copy_dev(s, &s->dst->hist_max, 4, &v);
+        *out = v;
+    });
+}
+
+// ---------------------------------------------------------------- metrics
+int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        DeviceScope ds(s->device);
+        sdr_metrics* m = new sdr_metrics();
+        try {
+            m->owner = s;
+            m->cavity_volume = cavity_volume;
+            dalloc(m->is_wall, s->ncell);
+            dalloc(m->washed, s->ncell);
+            dalloc(m->wet, s->ncell);
+            CK(cudaMemsetAsync(m->washed, 0, s->ncell, s->st));
+            CK(cudaMemsetAsync(m->wet, 0, s->ncell, s->st));
+            CK(cudaMemsetAsync(&s->dst->wall_count, 0, 8, s->st));
+            LAUNCH(k_wall_mask, blocks(s->ncell, kMetBS), kMetBS, 0, s->st, s->g, s->cavity, m->is_wall,
+                   &s->dst->wall_count);
+            unsigned long long wc = 0;
+            copy_dev(s, &s->dst->wall_count, 8, &wc);
+            m->wall_count = wc;
+        } catch (...) {
+            dfree(m->is_wall);
+            dfree(m->washed);
+            dfree(m->wet);
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int sdr_metrics_destroy(sdr_metrics* m) {
+    return guard([&] {
+        if (!m) return;
+        dfree(m->is_wall);
+        dfree(m->washed);
+        dfree(m->wet);
+        delete m;
+    });
+}
+
+int sdr_metrics_record(sdr_metrics* m, sdr_solver* s, uint64_t frame, sdr_frame_metrics* out) {
+    return guard([&] {
+        require(m && s, "null argument");
+        require(m->owner == s, "metrics collector belongs to another solver");
+        DeviceScope ds(s->device);
+        const double M3_TO_ML = 1.0e6, PA_TO_MMHG = 1.0 / 133.322, CAP_FACTOR = 3.0;
+        unsigned npb = blocks(std::max<uint32_t>(s->n, 1), kMetBS);
+        if (npb * 2 > s->mpart_cap) {
+            dalloc(s->mpart, (size_t)npb * 2);
+            s->mpart_cap = (size_t)npb * 2;
+        }
+        if (s->n)
+            LAUNCH(k_metrics_particles, npb, kMetBS, 0, s->st, s->g, s->pos, s->vel, s->n, m->is_wall, m->washed,
+                   m->wet, s->mpart);
+        else
+            npb = 0;
+        double v_jet = s->jet_speed();
+        double stagnation = 0.5 * s->fluid.density * v_jet * v_jet;
+        double gl = std::sqrt(s->fluid.gravity.x * s->fluid.gravity.x + s->fluid.gravity.y * s->fluid.gravity.y +
+                              s->fluid.gravity.z * s->fluid.gravity.z);
+        double hydrostatic = s->fluid.density * gl * ((double)s->g.ny * s->g.dx);
+        double p_cap = CAP_FACTOR * stagnation + hydrostatic + 500.0;  // metrics.rs:232-236
+        unsigned ncb = blocks(s->ncell, kMetBS);
+        LAUNCH(k_metrics_cells, ncb, kMetBS, 0, s->st, s->ncell, s->cells, s->p_dense, m->washed, m->wet, p_cap,
+               s->mcell);
+        LAUNCH(k_metrics_final, 1, 32, 0, s->st, s->mcell, (int)ncb, s->mpart, (int)npb, s->mout);
+        copy_dev(s, s->mout, sizeof(MetricsOut), s->h_mout);
+        const MetricsOut& o = *s->h_mout;
+        double pv = s->particle_volume();
+        double fluid_volume = (double)s->n * pv;
+        double drained_volume = (double)s->drained * pv;
+        double fill = m->cavity_volume > 0.0 ? fluid_volume / m->cavity_volume : 0.0;
+        m->injected_ml = (fluid_volume + drained_volume) * M3_TO_ML;
+        sdr_frame_metrics f{};
+        f.frame = frame;
+        f.time_s = s->time;
+        f.particles = s->n;
+        f.fluid_volume_ml = fluid_volume * M3_TO_ML;
+        f.drained_volume_ml = drained_volume * M3_TO_ML;
+        f.fill_fraction = fill;
+        f.wall_coverage = m->wall_count > 0 ? (double)o.washed / (double)m->wall_count : 0.0;
+        f.mean_pressure_pa = o.fl_n ? o.fl_sum / (double)o.fl_n : 0.0;
+        f.max_pressure_pa = o.fl_max;
+        f.max_pressure_mmhg = o.fl_max * PA_TO_MMHG;
+        f.wall_pressure_pa = o.ww_n ? o.ww_sum / (double)o.ww_n : 0.0;
+        f.peak_wall_pressure_pa = o.ww_n ? o.ww_peak : 0.0;
+        f.peak_wall_pressure_mmhg = f.peak_wall_pressure_pa * PA_TO_MMHG;
+        f.membrane_artifacts = o.ww_art;
+        f.max_speed_m_s = o.max_speed;
+        f.kinetic_energy = 0.5 * o.ke_sum;
+        f.pcg_iters = s->last_pcg_iters;
+        m->history.push_back(f);
+        if (out) *out = f;
+    });
+}
+
+int sdr_metrics_summary(const sdr_metrics* m, sdr_summary* out) {  // metrics.rs:324-382
+    return guard([&] {
+        require(m && out, "null argument");
+        const double PA_TO_MMHG = 1.0 / 133.322;
+        double peak_fill = 0, peak_cov = 0, peak_p = 0, peak_mem = 0, mean_mem = 0;
+        uint64_t art = 0;
+        for (auto& f : m->history) {
+            peak_fill = std::fmax(peak_fill, f.fill_fraction);
+            peak_cov = std::fmax(peak_cov, f.wall_coverage);
+            peak_p = std::fmax(peak_p, f.max_pressure_pa);
+            peak_mem = std::fmax(peak_mem, f.peak_wall_pressure_pa);
+            art += f.membrane_artifacts;
+        }
+        if (!m->history.empty()) {
+            double sum = -0.0;
+            for (auto& f : m->history) sum += f.wall_pressure_pa;
+            mean_mem = sum / (double)m->history.size();
+        }
+        const sdr_frame_metrics* last = m->history.empty() ? nullptr : &m->history.back();
+        sdr_summary s{};
+        s.frames = m->history.size();
+        s.final_time_s = last ? last->time_s : 0.0;
+        s.peak_fill_fraction = peak_fill;
+        s.final_fill_fraction = last ? last->fill_fraction : 0.0;
+        s.peak_wall_coverage = peak_cov;
+        s.final_wall_coverage = last ? last->wall_coverage : 0.0;
+        s.peak_membrane_pressure_pa = peak_mem;
+        s.peak_membrane_pressure_mmhg = peak_mem * PA_TO_MMHG;
+        s.mean_membrane_pressure_pa = mean_mem;
+        s.mean_membrane_pressure_mmhg = mean_mem * PA_TO_MMHG;
+        s.peak_pressure_pa = peak_p;
+        s.peak_pressure_mmhg = peak_p * PA_TO_MMHG;
+        s.membrane_artifacts_total = art;
+        double resident = last ? last->fluid_volume_ml : 0.0, drained = last ? last->drained_volume_ml : 0.0;
+        s.total_drained_ml = drained;
+        s.injected_ml = resident + drained;
+        s.mass_balance = m->injected_ml > 0.0 ? s.injected_ml / m->injected_ml : 1.0;
+        *out = s;
+    });
+}
+
+int sdr_metrics_wall_count(const sdr_metrics* m, uint64_t* out) {
+    return guard([&] {
+        require(m && out, "null argument");
+        *out = m->wall_count;
+    });
+}
+
+// ---------------------------------------------------------------- geometry
+int sdr_sdf_mesh_grid(const double* tris, size_t ntri, double dx, double padding, sdr_vec3* origin,
+                      uint64_t dims[3]) {
+    return guard([&] {
+        require(tris && ntri && origin && dims && dx > 0, "bad argument");
+        double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (size_t v = 0; v < 3 * ntri; ++v)
+            for (int c = 0; c < 3; ++c) {
+                mn[c] = std::fmin(mn[c], tris[3 * v + c]);
+                mx[c] = std::fmax(mx[c], tris[3 * v + c]);
+            }
+        for (int c = 0; c < 3; ++c) {
+            mn[c] -= padding;
+            mx[c] += padding;
+            dims[c] = (uint64_t)std::ceil((mx[c] - mn[c]) / dx) + 1;
+        }
+        *origin = sdr_vec3{mn[0], mn[1], mn[2]};
+    });
+}
+
+int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double dx, const uint64_t dims[3],
+                      double* out) {
+    return guard([&] {
+        require(tris && ntri && dims && out && dx > 0, "bad argument");
+        check_device();
+        size_t nn = dims[0] * dims[1] * dims[2];
+        uint32_t ntiles = (uint32_t)((ntri + kSdfTile - 1) / kSdfTile);
+        size_t padded = (size_t)ntiles * kSdfTile * 9;
+        double *dt = nullptr, *dout = nullptr;
+        uint32_t* derr = nullptr;
+        cudaStream_t st = nullptr;
+        auto cleanup = [&] {
+            if (dt) cudaFree(dt);
+            if (dout) cudaFree(dout);
+            if (derr) cudaFree(derr);
+            if (st) cudaStreamDestroy(st);
+        };
+        try {
+            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            CK(cudaMalloc((void**)&dt, padded * 8));
+            CK(cudaMalloc((void**)&dout, nn * 8));
+            CK(cudaMalloc((void**)&derr, 4));
+            CK(cudaMemsetAsync(dt, 0, padded * 8, st));
+            CK(cudaMemsetAsync(derr, 0, 4, st));
+            CK(cudaMemcpyAsync(dt, tris, ntri * 72, cudaMemcpyHostToDevice, st));
+            LAUNCH(k_sdf_mesh, blocks(nn, kSdfBS), kSdfBS, 0, st, dt, (uint32_t)ntri, ntiles, origin.x, origin.y,
+                   origin.z, dx, (int)dims[0], (int)dims[1], (int)dims[2], dout, derr);
+            CK(cudaMemcpyAsync(out, dout, nn * 8, cudaMemcpyDeviceToHost, st));
+            uint32_t e = 0;
+            CK(cudaMemcpyAsync(&e, derr, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (e) throw Fail{SDR_ERR_DEVICE_TIMEOUT, "triangle staging wait gave up"};
+        } catch (...) {
+            cleanup();
+            throw;
+        }
+        cleanup();
+    });
+}
+
+int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx, const uint64_t dims[3],
+                       double* out) {
+    return guard([&] {
+        require(p && dims && out && dx > 0, "bad argument");
+        check_device();
+        size_t nn = dims[0] * dims[1] * dims[2];
+        double* dout = nullptr;
+        cudaStream_t st = nullptr;
+        try {
+            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            CK(cudaMalloc((void**)&dout, nn * 8));
+            SinusD sd{p->semi_axes.x, p->semi_axes.y, p->semi_axes.z, p->center.x, p->center.y, p->center.z,
+                      p->taper, p->bumpiness, p->socket_x, p->socket_z, p->socket_radius, p->socket_depth};
+            LAUNCH(k_sdf_sinus, blocks(nn, 256), 256, 0, st, sd, origin.x, origin.y, origin.z, dx, (int)dims[0],
+                   (int)dims[1], (int)dims[2], dout);
+            CK(cudaMemcpyAsync(out, dout, nn * 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        } catch (...) {
+            if (dout) cudaFree(dout);
+            if (st) cudaStreamDestroy(st);
+            throw;
+        }
+        cudaFree(dout);
+        cudaStreamDestroy(st);
+    });
+}
+
+}  // extern "C"

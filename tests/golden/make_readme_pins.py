@@ -1,0 +1,78 @@
+"""Regenerate readme_pins.json: the oracle run on the reference's two README scenes.
+
+Reads the reference checkout (default /root/reference, or $SDR_REFERENCE) at
+generation time only; the committed JSON is what the tests read. The pinned
+README figures (uselessgoddess/sdr README.md:58-61 and 146-151):
+  examples/scene.toml          peak fill 19.9 %, peak coverage 59.1 %,
+                               peak membrane 1099.3 mmHg (146558 Pa),
+                               mean membrane 3.3 mmHg (436 Pa), drained 8.11 ml of 10.0
+  examples/maxillary_real.toml fill 44.9 %, 92 % of fluid in the lower half (along gravity)
+Usage: python tests/golden/make_readme_pins.py [scene|maxillary] [threads]
+"""
+import json
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import numpy as np  # noqa: E402
+
+import oracle  # noqa: E402
+from sdr_b200 import scene as sc  # noqa: E402
+from tests.helpers import cavity_volume, oracle_sdf, oracle_solver  # noqa: E402
+
+REF = os.environ.get("SDR_REFERENCE", "/root/reference")
+
+
+def run(name: str, threads: int):
+    oracle.set_threads(threads)
+    path = os.path.join(REF, "examples", f"{name}.toml")
+    cfg = sc.SceneConfig.from_toml_file(path)
+    if cfg.sinus["mesh"] is not None:
+        cfg.sinus["mesh"] = os.path.join(REF, cfg.sinus["mesh"])
+    res = cfg.resolve()
+    tris = None if res.sinus is not None else sc.load_mesh(res.mesh_path) * sc.MM
+    t0 = time.time()
+    sdf = oracle_sdf(res, tris)
+    s = oracle_solver(res, sdf)
+    vol = cavity_volume(res, tris)
+    m = oracle.Metrics(s, vol)
+    frames = []
+    for f in range(res.frames):
+        s.step(res.frame_dt)
+        r = m.record(s, f)
+        r["substeps"] = s.scalars()["last_substeps"]
+        frames.append(r)
+        print(name, f, r["time_s"], r["particles"], r["fill_fraction"], r["pcg_iters"], r["substeps"],
+              f"{time.time() - t0:.0f}s", flush=True)
+    out = {"scene": f"examples/{name}.toml", "summary": m.summary(), "frames": frames,
+           "cavity_volume_m3": vol, "grid": list(s.grid[0]), "wall_seconds": time.time() - t0,
+           "threads": threads}
+    pos, _ = s.particles()
+    if len(pos):
+        g = np.asarray(res.fluid.gravity, dtype=np.float64)
+        gd = g / np.linalg.norm(g)
+        depth = pos @ gd  # larger = lower along gravity
+        mn, mx = sdf.bounds()
+        # cavity extent along gravity from the SDF's interior nodes
+        nz, ny, nx = sdf.data.shape
+        kk, jj, ii = np.nonzero(sdf.data < 0)
+        pts = np.stack([sdf.origin[0] + ii * sdf.dx, sdf.origin[1] + jj * sdf.dx, sdf.origin[2] + kk * sdf.dx], 1)
+        d = pts @ gd
+        mid = 0.5 * (d.min() + d.max())
+        out["fraction_lower_half"] = float(np.mean(depth > mid))
+    return out
+
+
+if __name__ == "__main__":
+    which = sys.argv[1] if len(sys.argv) > 1 else "scene"
+    threads = int(sys.argv[2]) if len(sys.argv) > 2 else 4
+    res = run(which, threads)
+    dst = os.path.join(HERE, "readme_pins.json")
+    data = json.load(open(dst)) if os.path.exists(dst) else {}
+    data[which] = res
+    with open(dst, "w") as f:
+        json.dump(data, f, indent=1)
+    print(json.dumps(res["summary"], indent=1))

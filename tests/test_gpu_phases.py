@@ -1,0 +1,209 @@
+"""Per-phase parity of the CUDA substep against the CPU oracle (shadow stepping).
+
+Before each phase both solvers hold identical state (the device's f32 values,
+widened to f64 for the oracle); after it the outputs are compared:
+  * integer work (labels, cell keys, the counting-sort permutation, the
+    bounds/compaction map, redistribution moves) — bit-exact;
+  * the pressure solve — bit-exact pressure and iteration count, because the
+    device repeats the reference's f64 arithmetic and dot order;
+  * f32 transfers (P2G, extrapolation, G2P, advection) — relative tolerances
+    stated per assertion, against the oracle's f64 arithmetic.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from sdr_b200 import _lib
+from tests.gpu_common import f32, make_pair, record, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FACE_TOL = 2e-6      # f32 face values vs f64 (relative to the field's max)
+P2G_TOL = 1e-6       # P2G faces, absolute error relative to the particles' max speed: f32
+                     # weights of faces whose weighted velocities cancel carry ~1e-7 of
+                     # the particle speed, not of the (small) face value
+VEL_TOL = 2e-5       # particle velocities (relative to max speed)
+POS_TOL = 1e-7       # particle positions, metres (f32 spacing at 2 cm is ~1.9e-9 m)
+
+
+@pytest.fixture(scope="module")
+def pair():
+    gpu, orc, res = make_pair(warm_frames=3)
+    assert len(gpu) > 100
+    return gpu, orc, res
+
+
+def sync_faces(gpu, orc, which=(0, 1, 2, 3, 4, 5)):
+    for w in which:
+        orc.set_face(w, gpu.face(w))
+
+
+def test_classify_labels_bit_exact(pair):
+    gpu, orc, res = pair
+    gpu.run_phase(_lib.PHASE_CLASSIFY)
+    orc.phase(oracle.PHASE_CLASSIFY)
+    g, o = gpu.cells(), orc.cells()
+    record("classify", {"cells": int(g.size), "fluid": int((o == 1).sum()), "mismatch": int((g != o).sum())})
+    assert np.array_equal(g, o)
+    assert np.array_equal(gpu.cavity_mask(), orc.cavity_mask())
+
+
+def test_p2g_sort_is_stable_counting_sort(pair):
+    gpu, orc, res = pair
+    gpu.run_phase(_lib.PHASE_P2G)
+    keys, perm = gpu.sort()
+    # CPU stable counting sort of the same keys
+    ref = np.argsort(keys, kind="stable").astype(np.uint32)
+    record("sort", {"n": int(keys.size), "perm_mismatch": int((perm != ref).sum())})
+    assert np.array_equal(perm, ref)
+    # the keys are the f32 cell of each particle (clamped to the grid)
+    pos, _ = gpu.particles_f32()
+    (nx, ny, nz) = gpu.grid_dims
+    st = gpu.stats()
+    o = np.array([st.origin.x, st.origin.y, st.origin.z], dtype=np.float32)
+    l = (pos - o) / np.float32(st.dx)
+    ijk = np.where(l > 0, np.floor(l), 0).astype(np.int64)
+    ijk = np.minimum(ijk, np.array([nx - 1, ny - 1, nz - 1]))
+    k2 = (ijk[:, 2] * ny + ijk[:, 1]) * nx + ijk[:, 0]
+    assert np.array_equal(keys.astype(np.int64), k2)
+
+
+def test_p2g_faces(pair):
+    gpu, orc, res = pair
+    gpu.run_phase(_lib.PHASE_P2G)
+    orc.phase(oracle.PHASE_P2G)
+    orc.phase(oracle.PHASE_SAVE_GRID)
+    _, vel = gpu.particles()
+    vscale = float(np.max(np.abs(vel)))
+    errs = {w: float(np.max(np.abs(gpu.face(w) - orc.face(w)))) / vscale for w in range(6)}
+    record("p2g", {"err_over_vmax": errs, "vmax": vscale})
+    for w in range(6):
+        assert errs[w] < P2G_TOL, errs
+
+
+def test_add_forces(pair):
+    gpu, orc, res = pair
+    dt = 1e-4
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_ADD_FORCES, dt)
+    orc.phase(oracle.PHASE_ADD_FORCES, dt)
+    for w in range(3):
+        assert rel_err(gpu.face(w), orc.face(w)) < FACE_TOL
+
+
+def test_project_bit_exact_pressure(pair):
+    gpu, orc, res = pair
+    dt = 1e-4
+    gpu.run_phase(_lib.PHASE_CLASSIFY)
+    orc.phase(oracle.PHASE_CLASSIFY)
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_PROJECT, dt)
+    orc.phase(oracle.PHASE_PROJECT, dt)
+    pg, po = gpu.pressure(), orc.pressure()
+    it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
+    diff = int(np.sum(pg.view(np.uint64) != po.view(np.uint64)))
+    errs = {w: rel_err(gpu.face(w), orc.face(w)) for w in range(3)}
+    record("project", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_bit_mismatch": diff,
+                       "pressure_rel_err": rel_err(pg, po), "max_p": float(po.max()), "face_rel_err": errs})
+    assert it_g == it_o
+    assert diff == 0
+    for w in range(3):
+        assert errs[w] < FACE_TOL
+
+
+def test_extrapolate(pair):
+    gpu, orc, res = pair
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_EXTRAPOLATE)
+    orc.phase(oracle.PHASE_EXTRAPOLATE)
+    errs = {w: rel_err(gpu.face(w), orc.face(w)) for w in range(3)}
+    record("extrapolate", {"rel_err": errs})
+    for w in range(3):
+        assert errs[w] < FACE_TOL
+
+
+def test_g2p(pair):
+    gpu, orc, res = pair
+    sync_faces(gpu, orc)
+    pos, vel = gpu.particles()
+    orc.set_particles(pos, vel)
+    gpu.run_phase(_lib.PHASE_G2P)
+    orc.phase(oracle.PHASE_G2P)
+    _, vg = gpu.particles()
+    _, vo = orc.particles()
+    e = rel_err(vg, vo)
+    record("g2p", {"n": int(len(vg)), "vel_rel_err": e})
+    assert e < VEL_TOL
+
+
+def test_advect(pair):
+    gpu, orc, res = pair
+    dt = 1e-4
+    sync_faces(gpu, orc)
+    pos, vel = gpu.particles()
+    orc.set_particles(pos, vel)
+    gpu.run_phase(_lib.PHASE_ADVECT, dt)
+    orc.phase(oracle.PHASE_ADVECT, dt)
+    pg, _ = gpu.particles()
+    po, _ = orc.particles()
+    d = np.max(np.abs(pg - po), axis=1)
+    record("advect", {"n": int(len(d)), "max_abs": float(d.max()), "p99": float(np.quantile(d, 0.99)),
+                      "n_over_tol": int((d > POS_TOL).sum())})
+    assert np.quantile(d, 0.999) < POS_TOL
+    assert (d > 0.5 * res.sim_dx).sum() == 0
+
+
+def test_bounds_compaction_exact(pair):
+    gpu, orc, res = pair
+    pos, vel = gpu.particles()
+    orc.set_particles(pos, vel)
+    d0g, d0o = gpu.drained, orc.scalars()["drained"]
+    gpu.run_phase(_lib.PHASE_BOUNDS)
+    orc.phase(oracle.PHASE_BOUNDS)
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    record("bounds", {"n_gpu": int(len(pg)), "n_orc": int(len(po)), "drained_gpu": gpu.drained - d0g,
+                      "drained_orc": orc.scalars()["drained"] - d0o})
+    assert len(pg) == len(po)
+    assert np.array_equal(pg, po)  # same survivors, same order, same (f32) values
+    assert np.array_equal(vg, vo)
+
+
+def test_redistribute_moves_exact(pair):
+    gpu, orc, res = pair
+    sync_faces(gpu, orc)
+    pos, vel = gpu.particles()
+    orc.set_particles(pos, vel)
+    gpu.run_phase(_lib.PHASE_REDISTRIBUTE)
+    orc.phase(oracle.PHASE_REDISTRIBUTE)
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    moved_g = np.any(pg != pos, axis=1)
+    moved_o = np.any(po != pos, axis=1)
+    d = np.max(np.abs(pg - po), axis=1)
+    record("redistribute", {"moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
+                            "max_abs_pos": float(d.max()) if len(d) else 0.0,
+                            "vel_rel_err": rel_err(vg, vo)})
+    assert np.array_equal(moved_g, moved_o)
+    assert d.max() < POS_TOL
+
+
+def test_full_substep_shadow():
+    """One full substep from identical state: counts, labels and particle state."""
+    gpu, orc, res = make_pair(warm_frames=4)
+    dt = orc.cfl_dt()
+    gpu.substep(dt)
+    orc.substep(dt)
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    rec = {"n_gpu": int(len(pg)), "n_orc": int(len(po)), "iters_gpu": gpu.last_pcg_iters,
+           "iters_orc": orc.scalars()["last_pcg_iters"], "dt": dt}
+    if len(pg) == len(po):
+        d = np.max(np.abs(pg - po), axis=1)
+        rec.update(pos_max=float(d.max()), pos_p999=float(np.quantile(d, 0.999)), vel_rel=rel_err(vg, vo),
+                   pressure_rel=rel_err(gpu.pressure(), orc.pressure()))
+    record("full_substep", rec)
+    assert len(pg) == len(po)
+    assert np.array_equal(gpu.cells(), orc.cells())
+    assert np.quantile(d, 0.99) < 1e-6
+    assert rec["pressure_rel"] < 1e-3
