@@ -1,0 +1,266 @@
+#!/usr/bin/env python
+"""Benchmark: particle-substeps/s of the FLIP/PIC substep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sdr|reference] [--workload real_cavity]
+
+A step is one output frame (Solver::step(frame_dt), all its CFL substeps) of
+the workload. W frames warm up, K frames are timed. ``value`` is device time
+(CUDA events on the solver stream, summed over the timed frames, max over
+ranks); ``e2e`` is the same frames timed on the host around the public call
+plus the per-frame read-back of particle positions (host buffers). Between
+timed frames a 256 MiB buffer is written to flush L2.
+
+Multi-GPU runs are independent scene replicas (one per rank, different cavity
+seeds): no collective on the data path; a barrier and a max-reduce of the
+timings use torch.distributed.
+
+``--impl reference`` times the CPU restatement of the reference solver
+(oracle/, the reference Rust cannot be built here) on the host cores: W
+frames from t = 0 to reach the timed window, then K bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes of the pressure solve (the dominant kernel, k_pcg), f64
+# vectors in wavefront order: per fluid cell and PCG iteration, and per fluid
+# cell once per solve (factorisation, first preconditioner application, setup).
+PCG_BYTES_PER_CELL_ITER = 233
+PCG_BYTES_PER_CELL_SOLVE = 190
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def oracle_for(w, sdf):
+    import oracle
+    from tests.helpers import oracle_solver
+    osdf = oracle.SdfGrid(tuple(sdf.origin), sdf.dx, sdf.data)
+    return oracle_solver(w.res, osdf)
+
+
+def cpu_sample(orc, budget_s: float, max_substeps: int):
+    """Run the oracle for a bounded sample; returns (particle_substeps, seconds, substeps)."""
+    t0 = time.perf_counter()
+    ps = sub = 0
+    while sub < max_substeps and time.perf_counter() - t0 < budget_s:
+        dt = orc.cfl_dt()
+        ps += len(orc) + 0
+        orc.substep(dt)
+        sub += 1
+    return ps, time.perf_counter() - t0, sub
+
+
+def run_reference(args):
+    """CPU restatement of the reference (all host threads), same workload and metric."""
+    import oracle
+    from sdr_b200 import workloads
+    from sdr_b200.solver import Sdf
+    w = workloads.WORKLOADS[args.workload]()
+    # The reference arm builds its SDF with the oracle's own winding-number/implicit code.
+    if w.res.sinus is not None:
+        osdf = oracle.sdf_from_sinus(w.res.sinus, w.res.sdf_origin, w.res.sdf_dx, w.res.sdf_dims)
+    else:
+        osdf = oracle.sdf_from_mesh(w.tris, w.res.sdf_dx, w.res.mesh_padding)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    from tests.helpers import oracle_solver
+    orc = oracle_solver(w.res, osdf)
+    for _ in range(args.warmup):
+        orc.step(w.res.frame_dt)
+    ps_tot = 0
+    t_tot = 0.0
+    subs = 0
+    for _ in range(args.steps):
+        ps, t, sub = cpu_sample(orc, budget_s=args.ref_budget, max_substeps=args.ref_substeps)
+        ps_tot += ps
+        t_tot += t
+        subs += sub
+    v = ps_tot / t_tot if t_tot > 0 else 0.0
+    sample = (f"{args.warmup} frames from t=0 (untimed), then {args.steps} samples of up to "
+              f"{args.ref_substeps} substeps ({subs} substeps, {ps_tot} particle-substeps)")
+    line = {"metric": "particle-substeps/s", "value": v, "unit": "particle-substeps/s", "impl": "reference",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": w.name, **(w.describe or {})},
+            "cpu_baseline": {"value": v, "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+                             "sample": sample + "; C++ restatement of the reference solver (Rust not buildable)"},
+            "e2e": {"value": v, "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sdr", choices=["sdr", "reference"])
+    ap.add_argument("--workload", default="real_cavity")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of oracle time for cpu_baseline")
+    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--ref-substeps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from sdr_b200 import _lib, workloads
+
+    w = workloads.WORKLOADS[args.workload]() if args.workload != "real_cavity" else workloads.real_cavity(seed=2 + rank)
+    solver, sdf, vol = workloads.build_gpu(w)
+    solver.set_profiling(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        solver.step(w.res.frame_dt)
+    solver.reset_profile()
+    launches0 = _lib.load().sdr_kernel_launch_count()
+    clk = Clocks(local)
+    dev_ms = 0.0
+    wall = 0.0
+    ps = 0
+    h2d = 0
+    d2h = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        st0 = solver.stats()
+        t0 = time.perf_counter()
+        solver.step(w.res.frame_dt)          # public API: host emission uploads inside
+        pos, _ = solver.particles_f32()      # per-frame result read-back (positions)
+        t1 = time.perf_counter()
+        st1 = solver.stats()
+        dev_ms += st1.device_ms - st0.device_ms
+        wall += t1 - t0
+        ps += st1.particle_substeps - st0.particle_substeps
+        h2d += (st1.emitted - st0.emitted) * 32 + (st1.substeps_total - st0.substeps_total) * 4
+        d2h += pos.nbytes * 2 + (st1.substeps_total - st0.substeps_total) * 96
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = _lib.load().sdr_kernel_launch_count() - launches0
+    prof = solver.profile()
+    if world > 1:
+        t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, wall = float(t[0]), float(t[1])
+        c = torch.tensor([ps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        ps = int(c[0])
+    value = ps / (dev_ms / 1e3)
+    e2e = ps / wall
+    hbm, peak_kind = peaks()
+    pcg_launch_ms = prof["pcg_ms"] / max(prof["pcg_launches"], 1)
+    pcg_bytes = (PCG_BYTES_PER_CELL_ITER * prof["pcg_cell_iters"] + PCG_BYTES_PER_CELL_SOLVE * prof["fluid_cells"]) / max(prof["pcg_launches"], 1)
+    achieved = pcg_bytes / (pcg_launch_ms / 1e3) / 1e9 if pcg_launch_ms > 0 else 0.0
+    st = solver.stats()
+    line = {"metric": "particle-substeps/s", "value": value, "unit": "particle-substeps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": w.name, **(w.describe or {}), "grid": [st.nx, st.ny, st.nz],
+                       "particles_end": int(st.particles), "substeps": int(prof["substeps"]),
+                       "l2": "256 MiB buffer written between timed frames", "replicas": world},
+            "e2e": {"value": e2e, "unit": "particle-substeps/s", "h2d_bytes_per_step": int(h2d / args.steps),
+                    "d2h_bytes_per_step": int(d2h / args.steps)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": {"bound": "hbm", "kernel": "k_pcg", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                         "bytes_per_launch": pcg_bytes, "ms_per_launch": pcg_launch_ms},
+            "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
+            "pcg_section_cycles": dict(zip(["mic_build", "sweeps", "unused", "matvec", "dots", "axpy_norm",
+                                            "direction", "setup_exit", "lvl_stage_wait", "lvl_compute",
+                                            "lvl_barrier", "lvl_count", "sum_sweep_width", "sum_level_range",
+                                            "solves"], prof["pcg_section_cycles"])),
+            "pcg": {"launches": prof["pcg_launches"], "mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
+                    "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1)}}
+    if rank == 0 and not args.no_cpu:
+        orc = oracle_for(w, sdf)
+        pos, vel = solver.particles()
+        orc.set_particles(pos, vel)
+        s = solver.stats()
+        orc.set_scalars(s.time, s.emit_accum, s.steps, s.drained, s.rng_state)
+        import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        cps, ct, csub = cpu_sample(orc, budget_s=args.cpu_budget, max_substeps=10 ** 9)
+        line["cpu_baseline"] = {"value": cps / ct, "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+                                "sample": f"{csub} substeps from the GPU state after the timed frames "
+                                          f"({cps} particle-substeps, {ct:.1f} s); C++ restatement of the "
+                                          "reference solver, f64, rayon-parallel parts on all host threads"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

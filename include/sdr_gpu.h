@@ -106,7 +106,35 @@ typedef struct {
     uint64_t nx, ny, nz;     /* MAC grid cells */
     double dx;
     sdr_vec3 origin;
+    uint64_t particle_substeps; /* sum over substeps of the particles each one advanced */
+    double device_ms;           /* device time of all substeps (CUDA events on the solver stream) */
+    uint64_t substeps_total;    /* substeps run since creation */
 } sdr_solver_stats;
+
+/* Device time per phase group, accumulated while profiling is on (CUDA events
+ * on the solver stream; milliseconds). pcg_cell_iters = sum over solves of
+ * fluid cells x PCG iterations (the unit of the solve's algorithmic bytes). */
+typedef struct {
+    double emit_classify_sort_ms;
+    double p2g_ms;
+    double pressure_setup_ms;
+    double pcg_ms;
+    double gradient_extrapolate_ms;
+    double g2p_advect_ms;
+    double compact_ms;
+    double redistribute_ms;
+    uint64_t substeps;
+    uint64_t pcg_launches;
+    uint64_t pcg_cell_iters;
+    uint64_t fluid_cells;       /* sum over solves of fluid cells */
+    uint64_t particles;         /* sum over substeps of particles advanced */
+    /* SM cycles inside the pressure-solve kernel by section: MIC(0) build,
+     * forward+backward preconditioner sweeps, (unused), matvec, dot products,
+     * update of p and r with the residual norm, search direction, setup/exit;
+     * then per forward-sweep level: staging wait, compute, barrier, level
+     * count; then the sum of sweep widths, of non-empty level ranges, and solves. */
+    uint64_t pcg_section_cycles[16];
+} sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */
 typedef struct {
@@ -162,6 +190,17 @@ int sdr_solver_step(sdr_solver* s, double dt);
 int sdr_solver_substep(sdr_solver* s, double dt);
 /* Public fields time/steps/last_pcg_iters/last_substeps/drained (solver.rs:155-166). */
 int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
+/* Dot-product order inside the pressure solve. 1: the reference's order
+ * (fixed 4096-cell chunks summed sequentially, partials in chunk order,
+ * src/pressure.rs:588-603) — pressure and iteration counts then equal the
+ * reference's bit for bit given the same right-hand side. 0 (default): a fixed
+ * block-tree order — deterministic run to run, faster, differing from the
+ * reference in the last bits of each dot. */
+int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
+/* Phase-group timing with CUDA events (adds one event record per group). */
+int sdr_solver_set_profiling(sdr_solver* s, int on);
+int sdr_solver_get_profile(const sdr_solver* s, sdr_profile* out);
+int sdr_solver_reset_profile(sdr_solver* s);
 /* Restore the solver's scalar state (checkpoint / shadow stepping). */
 int sdr_solver_set_scalars(sdr_solver* s, double time, double emit_accum, uint64_t steps,
                            uint64_t drained, uint64_t rng_state);

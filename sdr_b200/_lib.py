@@ -64,7 +64,21 @@ class SolverStats(C.Structure):
                 ("last_residual", C.c_double), ("emit_accum", C.c_double), ("rng_state", C.c_uint64),
                 ("emitted", C.c_uint64), ("culled", C.c_uint64), ("redistributed", C.c_uint64),
                 ("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64), ("dx", C.c_double),
-                ("origin", Vec3)]
+                ("origin", Vec3), ("particle_substeps", C.c_uint64), ("device_ms", C.c_double),
+                ("substeps_total", C.c_uint64)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("emit_classify_sort_ms", C.c_double), ("p2g_ms", C.c_double), ("pressure_setup_ms", C.c_double),
+                ("pcg_ms", C.c_double), ("gradient_extrapolate_ms", C.c_double), ("g2p_advect_ms", C.c_double),
+                ("compact_ms", C.c_double), ("redistribute_ms", C.c_double), ("substeps", C.c_uint64),
+                ("pcg_launches", C.c_uint64), ("pcg_cell_iters", C.c_uint64), ("fluid_cells", C.c_uint64),
+                ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16)]
+
+    def to_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["pcg_section_cycles"] = list(self.pcg_section_cycles)
+        return d
 
 
 _FM = ["frame:u", "time_s", "particles:u", "fluid_volume_ml", "drained_volume_ml", "fill_fraction",
@@ -119,6 +133,10 @@ SIGNATURES = {
     "sdr_solver_substep": (i32, [vp, d]),
     "sdr_solver_get_stats": (i32, [vp, P(SolverStats)]),
     "sdr_solver_set_scalars": (i32, [vp, d, d, u64, u64, u64]),
+    "sdr_solver_set_dot_order": (i32, [vp, i32]),
+    "sdr_solver_set_profiling": (i32, [vp, i32]),
+    "sdr_solver_get_profile": (i32, [vp, P(Profile)]),
+    "sdr_solver_reset_profile": (i32, [vp]),
     "sdr_solver_copy_particles": (i32, [vp, P(d), P(d), sz, P(sz)]),
     "sdr_solver_copy_particles_f32": (i32, [vp, P(C.c_float), P(C.c_float), sz, P(sz)]),
     "sdr_solver_set_particles": (i32, [vp, P(d), P(d), sz]),

@@ -3,6 +3,7 @@
 // face max-reduction behind cfl_dt (grid.rs:202-206).
 #pragma once
 #include "common.cuh"
+#include "particles.cuh"
 
 namespace sdr {
 
@@ -72,8 +73,8 @@ __global__ void k_cavity_and_base(Grid g, SdfD s, int has_outlet, Aabb outlet,
 // Validity for extrapolation: the face borders a Fluid cell (solver.rs:612-642).
 __global__ void k_extrap_valid(Grid g, const uint8_t* __restrict__ cells, uint8_t* __restrict__ ku,
                                uint8_t* __restrict__ kv, uint8_t* __restrict__ kw) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx) return;
+    int i, j, k;
+    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     auto fl = [&](int a, int b, int c) {
         return cells[((size_t)c * g.ny + b) * g.nx + a] == FLUID;
     };
@@ -134,9 +135,9 @@ struct ExtrapArgs {
 
 __global__ void __launch_bounds__(256) k_extrap(ExtrapArgs a) {
     const Grid& g = a.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    int i, j, k;
     float mu = 0.f, mv = 0.f, mw = 0.f;
-    if (i <= g.nx) {
+    if (node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) {
         if (j < g.ny && k < g.nz) {
             extrap_one(a.u, a.ku, a.u2, a.ku2, g.nx + 1, g.ny, g.nz, i, j, k);
             mu = fabsf(a.u2[((size_t)k * g.ny + j) * (g.nx + 1) + i]);

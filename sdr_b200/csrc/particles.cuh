@@ -18,8 +18,8 @@ __global__ void k_base_labels(const uint8_t* __restrict__ base, uint8_t* __restr
 }
 
 // Per particle: the f64 cell key of Solver::cell_of (labels, histograms) and
-// the f32 clamped cell the P2G gather bins by (the same f32 arithmetic the
-// gather's weights use, so every contribution lands in the gathered stencil).
+// the clamped cell the P2G gather bins by (from the same f64 grid coordinate
+// the gather's weights use, so every contribution lands in the gathered stencil).
 // With mark_fluid, also the second half of classify: Air cells holding a
 // particle that is not in the outlet become Fluid (solver.rs:362-370).
 __global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t n,
@@ -38,10 +38,11 @@ __global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t
             !(has_outlet && aabb_contains(outlet, q.x, q.y, q.z)))
             cells[c] = FLUID;  // benign race: every writer stores FLUID
     }
-    float lx = (q.x - g.oxf) / g.dxf, ly = (q.y - g.oyf) / g.dxf, lz = (q.z - g.ozf) / g.dxf;
-    int i = (lx > 0.f) ? min((int)floorf(lx), g.nx - 1) : 0;
-    int j = (ly > 0.f) ? min((int)floorf(ly), g.ny - 1) : 0;
-    int k = (lz > 0.f) ? min((int)floorf(lz), g.nz - 1) : 0;
+    double lx = ddiv(dsub((double)q.x, g.ox), g.dx), ly = ddiv(dsub((double)q.y, g.oy), g.dx),
+           lz = ddiv(dsub((double)q.z, g.oz), g.dx);
+    int i = (lx > 0.0) ? (int)fmin(floor(lx), (double)(g.nx - 1)) : 0;
+    int j = (ly > 0.0) ? (int)fmin(floor(ly), (double)(g.ny - 1)) : 0;
+    int k = (lz > 0.0) ? (int)fmin(floor(lz), (double)(g.nz - 1)) : 0;
     uint32_t ks = ((uint32_t)k * g.ny + j) * g.nx + i;
     key_sort[p] = ks;
     atomicAdd(&hist_sort[ks], 1u);
@@ -106,12 +107,25 @@ __global__ void k_sort_long(const uint32_t* __restrict__ start, const uint32_t* 
 }
 
 // ------------------------------------------------------------------ P2G gather
+// Sorted particle records for the gather: the f64 grid coordinate
+// (p - origin)/dx of Solver's u/v/w_coords (grid.rs:161-175) and the f32 velocity.
+__global__ void k_sorted_records(Grid g, const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                 const uint32_t* __restrict__ perm, uint32_t n, double4* __restrict__ lrec,
+                                 float4* __restrict__ vrec) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t p = perm[s];
+    float4 q = pos[p];
+    lrec[s] = make_double4(ddiv(dsub((double)q.x, g.ox), g.dx), ddiv(dsub((double)q.y, g.oy), g.dx),
+                           ddiv(dsub((double)q.z, g.oz), g.dx), 0.0);
+    vrec[s] = vel[p];
+}
+
 struct P2GArgs {
     Grid g;
-    const float4* pos;
-    const float4* vel;
+    const double4* lrec;
+    const float4* vrec;
     const uint32_t* start;  // ncell + 1
-    const uint32_t* perm;
     float* u;
     float* v;
     float* w;
@@ -131,70 +145,85 @@ __device__ __forceinline__ bool solid_at(const Grid& g, const uint8_t* cells, in
     return cells[((size_t)k * g.ny + j) * g.nx + i] == SOLID;
 }
 
+// Flat node index -> (i, j, k) over (nx+1) x (ny+1) x (nz+1).
+__device__ __forceinline__ bool node_of(const Grid& g, size_t t, int& i, int& j, int& k) {
+    size_t nxp = (size_t)g.nx + 1, nyp = (size_t)g.ny + 1;
+    if (t >= nxp * nyp * ((size_t)g.nz + 1)) return false;
+    i = (int)(t % nxp);
+    j = (int)((t / nxp) % nyp);
+    k = (int)(t / (nxp * nyp));
+    return true;
+}
+
+// clamp_base (grid.rs:25-34) in f64 and the weight of node `i` (0 if not a corner).
+__device__ __forceinline__ double corner_w(double gcoord, int n, int node) {
+    int i0;
+    double f;
+    if (!(gcoord > 0.0)) {
+        i0 = 0;
+        f = 0.0;
+    } else if (gcoord >= (double)(n - 1)) {
+        i0 = n - 2;
+        f = 1.0;
+    } else {
+        double fl = floor(gcoord);
+        i0 = (int)fl;
+        f = dsub(gcoord, fl);
+    }
+    int d = node - i0;
+    return d == 0 ? dsub(1.0, f) : (d == 1 ? f : -1.0);
+}
+
 // One thread per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]; it owns the u, v
 // and w faces with that index. It visits the 27 cells around the node in
-// fixed (k, j, i) order and, within a cell, particles in ascending index,
-// accumulating the trilinear_scatter weights (grid.rs:52-88) in f64, then
-// normalises (solver.rs:944-952), saves the FLIP copy (save_grid), and
-// optionally adds gravity (add_forces) and zeroes solid faces.
+// fixed (k, j, i) order — for each (k, j) the three cells i-1..i+1 are one
+// contiguous run of the sorted records — and, within a cell, particles in
+// ascending index, accumulating the trilinear_scatter weights (grid.rs:52-88,
+// w = wx*wy*wz) in f64. Then it normalises (solver.rs:944-952), saves the FLIP
+// copy (save_grid), and optionally adds gravity and zeroes solid faces.
 __global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
     const Grid& g = a.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx) return;
+    int i, j, k;
+    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     const bool hu = j < g.ny && k < g.nz, hv = i < g.nx && k < g.nz, hw = i < g.nx && j < g.ny;
     double su = 0, wu = 0, sv = 0, wv = 0, sw = 0, ww = 0;
+    const int ci0 = max(i - 1, 0), ci1 = min(i + 1, g.nx - 1);
     for (int ck = max(k - 1, 0); ck <= min(k + 1, g.nz - 1); ++ck)
-        for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj)
-            for (int ci = max(i - 1, 0); ci <= min(i + 1, g.nx - 1); ++ci) {
-                uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx + ci;
-                uint32_t s0 = a.start[c], s1 = a.start[c + 1];
-                for (uint32_t s = s0; s < s1; ++s) {
-                    uint32_t p = a.perm[s];
-                    float4 q = a.pos[p];
-                    float4 vel = a.vel[p];
-                    float lx = (q.x - g.oxf) / g.dxf, ly = (q.y - g.oyf) / g.dxf,
-                          lz = (q.z - g.ozf) / g.dxf;
-                    int i0, j0, k0;
-                    float fx, fy, fz;
-                    if (hu) {
-                        clamp_base(lx, g.nx + 1, i0, fx);
-                        clamp_base(ly - 0.5f, g.ny, j0, fy);
-                        clamp_base(lz - 0.5f, g.nz, k0, fz);
-                        int di = i - i0, dj = j - j0, dk = k - k0;
-                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
-                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
-                                        (dk ? fz : 1.0f - fz);
-                            su = dadd(su, (double)wgt * (double)vel.x);
-                            wu = dadd(wu, (double)wgt);
-                        }
+        for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj) {
+            uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx;
+            uint32_t s0 = a.start[c + ci0], s1 = a.start[c + ci1 + 1];
+            for (uint32_t s = s0; s < s1; ++s) {
+                double4 l = a.lrec[s];
+                float4 vel = a.vrec[s];
+                if (hu) {
+                    double wx = corner_w(l.x, g.nx + 1, i), wy = corner_w(l.y - 0.5, g.ny, j),
+                           wz = corner_w(l.z - 0.5, g.nz, k);
+                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                        double wgt = dmul(dmul(wx, wy), wz);
+                        su = dadd(su, dmul(wgt, (double)vel.x));
+                        wu = dadd(wu, wgt);
                     }
-                    if (hv) {
-                        clamp_base(lx - 0.5f, g.nx, i0, fx);
-                        clamp_base(ly, g.ny + 1, j0, fy);
-                        clamp_base(lz - 0.5f, g.nz, k0, fz);
-                        int di = i - i0, dj = j - j0, dk = k - k0;
-                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
-                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
-                                        (dk ? fz : 1.0f - fz);
-                            sv = dadd(sv, (double)wgt * (double)vel.y);
-                            wv = dadd(wv, (double)wgt);
-                        }
+                }
+                if (hv) {
+                    double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y, g.ny + 1, j),
+                           wz = corner_w(l.z - 0.5, g.nz, k);
+                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                        double wgt = dmul(dmul(wx, wy), wz);
+                        sv = dadd(sv, dmul(wgt, (double)vel.y));
+                        wv = dadd(wv, wgt);
                     }
-                    if (hw) {
-                        clamp_base(lx - 0.5f, g.nx, i0, fx);
-                        clamp_base(ly - 0.5f, g.ny, j0, fy);
-                        clamp_base(lz, g.nz + 1, k0, fz);
-                        int di = i - i0, dj = j - j0, dk = k - k0;
-                        if ((unsigned)di < 2u && (unsigned)dj < 2u && (unsigned)dk < 2u) {
-                            float wgt = (di ? fx : 1.0f - fx) * (dj ? fy : 1.0f - fy) *
-                                        (dk ? fz : 1.0f - fz);
-                            sw = dadd(sw, (double)wgt * (double)vel.z);
-                            ww = dadd(ww, (double)wgt);
-                        }
+                }
+                if (hw) {
+                    double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y - 0.5, g.ny, j),
+                           wz = corner_w(l.z, g.nz + 1, k);
+                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                        double wgt = dmul(dmul(wx, wy), wz);
+                        sw = dadd(sw, dmul(wgt, (double)vel.z));
+                        ww = dadd(ww, wgt);
                     }
                 }
             }
+        }
     if (hu) {
         size_t f = ((size_t)k * g.ny + j) * (g.nx + 1) + i;
         float val = wu > 1e-12 ? (float)ddiv(su, wu) : 0.0f;
@@ -231,8 +260,8 @@ __global__ void k_add_forces(float* __restrict__ f, size_t n, double gdt) {
 // thread per node, owning the u/v/w faces with that index.
 __global__ void k_enforce_solid(Grid g, const uint8_t* __restrict__ cells, float* __restrict__ u,
                                 float* __restrict__ v, float* __restrict__ w) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx) return;
+    int i, j, k;
+    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     if (j < g.ny && k < g.nz && (solid_at(g, cells, i - 1, j, k) || solid_at(g, cells, i, j, k)))
         u[((size_t)k * g.ny + j) * (g.nx + 1) + i] = 0.0f;
     if (i < g.nx && k < g.nz && (solid_at(g, cells, i, j - 1, k) || solid_at(g, cells, i, j, k)))

@@ -15,11 +15,12 @@
 // count equal the CPU reference's bit for bit.
 #pragma once
 #include "common.cuh"
+#include "particles.cuh"
 
 namespace sdr {
 
 constexpr int kDotChunk = 4096;
-constexpr int kPcgBS = 1024;
+constexpr int kPcgBS = 768;
 constexpr int kPcgWin = 6144;  // smem window (doubles) per level buffer
 
 // Neighbour directions in the reference's visit order.
@@ -139,10 +140,13 @@ __global__ void k_fluid_flags(const uint8_t* __restrict__ cells, size_t n, uint3
 }
 
 __global__ void k_corder(const uint8_t* __restrict__ cells, size_t n, const uint32_t* __restrict__ off,
-                         const int* __restrict__ pos_of_cell, int* __restrict__ corder,
+                         const int* __restrict__ pos_of_cell, int* __restrict__ corder, int* __restrict__ cinv,
                          int* __restrict__ chunk_start, int nchunks, const uint32_t* __restrict__ nf) {
     size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n && cells[c] == FLUID) corder[off[c]] = pos_of_cell[c];
+    if (c < n && cells[c] == FLUID) {
+        corder[off[c]] = pos_of_cell[c];
+        cinv[pos_of_cell[c]] = (int)off[c];
+    }
     if (c < n && c % kDotChunk == 0) chunk_start[c / kDotChunk] = (int)off[c];
     if (c == 0) chunk_start[nchunks] = (int)*nf;
 }
@@ -151,11 +155,13 @@ struct PcgArgs {
     const uint32_t* nf;  // device fluid count
     int nlevels;
     int nchunks;
+    int nx, ny;
     const int* level_start;
     const int* nbr;
     const uint8_t* diag;
     const uint8_t* nmask;
     const int* corder;
+    const int* cinv;        // wavefront position -> cell-order index
     const int* chunk_start;
     const double* b;
     double* precon;
@@ -166,33 +172,118 @@ struct PcgArgs {
     double* as;
     double* q;
     double* pq;
-    double* partials;  // nchunks
+    double* prod;       // per-cell products in cell order (reference dot order)
+    double* partials;   // nchunks (global fallback when they do not fit in shared memory)
+    int4* frec;         // per cell: forward sweep record (precon + window slots of -x,-y,-z)
+    int4* brec;         // per cell: backward sweep record (precon + window slots of +x,+y,+z)
     double tol;
     int max_iters;
     const uint32_t* lv_cell;
-    double* p_dense;   // pre-zeroed; fluid cells written at exit
+    double* p_dense;    // pre-zeroed; fluid cells written at exit
     int* out_iters;
     double* out_residual;
+    unsigned long long* timing;  // optional: cycles per section
+    int exact_dots;              // 1: the reference's chunked sequential dot order (bit-exact); 0: fixed block tree
 };
 
-// Exact reference dot (pressure.rs:588-603): chunk partials in parallel, each
-// a sequential sum over its fluid cells in cell order, then the partials in
-// chunk order. Empty chunks contribute +0.0.
-__device__ __forceinline__ double pcg_dot(const PcgArgs& a, const double* x, const double* y,
-                                          double* sh) {
-    for (int ch = threadIdx.x; ch < a.nchunks; ch += blockDim.x) {
-        int e = a.chunk_start[ch + 1];
-        double acc = 0.0;
-        for (int t = a.chunk_start[ch]; t < e; ++t) {
-            int ps = a.corder[t];
-            acc = dadd(acc, dmul(x[ps], y[ps]));
+// Sweep record: the cell's MIC factor and the shared-window slots (index
+// within the neighbouring level, -1 = not fluid) of its three neighbours.
+struct SweepRec {
+    double pc;
+    short s0, s1, s2, pad;
+};
+
+// Shared-memory plan of k_pcg (dynamic): a ring of kStages staged levels
+// (two f64 operands and one record per cell), two level windows of f64 and of
+// neighbour masks, the level starts and the dot partials.
+constexpr int kStages = 4;          // levels in flight ahead of the sweep
+constexpr int kMaxLevelsSmem = 2048;
+constexpr int kMaxChunksSmem = 2048;
+constexpr int kSweepMax = kPcgBS - 32;  // compute threads; one producer warp stages ahead
+constexpr size_t kPcgSmem = (size_t)kStages * kPcgBS * (8 + 8 + 16) + 2 * kPcgBS * 8 + 2 * kPcgBS * 4 +
+                            (kMaxLevelsSmem + 1) * 4 + kMaxChunksSmem * 8;
+
+struct PcgSmem {
+    double* sa;     // [kStages][BS]
+    double* sb;     // [kStages][BS]
+    SweepRec* sr;   // [kStages][BS]
+    double* w0;     // [BS] level window
+    double* w1;
+    int* m0;        // [BS] neighbour-mask window (MIC build)
+    int* m1;
+    int* lvs;       // level starts (smem copy or global)
+    double* part;   // dot partials
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// The producer keeps two levels complete ahead of the one being computed, so
+// compute threads can read level L+1's staged data into registers while level
+// L is in flight.
+__device__ __forceinline__ void cp_wait_ahead() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kStages - 3) : "memory");
+}
+
+// Barrier over the first `n` threads (named barrier 1): the sweeps run on the
+// compute warps plus one producer warp, sized to the widest level, so the
+// per-level barrier carries only working warps.
+__device__ __forceinline__ void sweep_bar(int n) { asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory"); }
+
+// Producer warp: stage every cell of level L (if the level fits the ring)
+// into slot L % kStages: operand A, optional operand B, and the record.
+__device__ __forceinline__ void produce_level(const PcgSmem& m, int L, int lo, int hi, const double* va,
+                                              const double* vb, const int4* rec, int lane) {
+    if (L >= lo && L < hi) {
+        int ls = m.lvs[L], le = m.lvs[L + 1];
+        if (le - ls <= kSweepMax) {
+            int base = (L % kStages) * kPcgBS;
+            for (int t = lane; t < le - ls; t += 32) {
+                cp_async8(&m.sa[base + t], &va[ls + t]);
+                if (vb) cp_async8(&m.sb[base + t], &vb[ls + t]);
+                cp_async16(&m.sr[base + t], &rec[ls + t]);
+            }
         }
-        a.partials[ch] = acc;
+    }
+    cp_commit();
+}
+
+// Exact reference dot (pressure.rs:588-603) over `prod` (cell order): one
+// warp per 4096-cell chunk folds its products in cell order from registers
+// through shuffles, then one thread sums the partials in chunk order.
+__device__ __forceinline__ double pcg_chunk_sums(const PcgArgs& a, const PcgSmem& m, double* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int ch = warp; ch < a.nchunks; ch += nw) {
+        int t = a.chunk_start[ch], e = a.chunk_start[ch + 1];
+        double acc = 0.0;
+        for (; t < e; t += 512) {
+            double v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                int idx = t + u * 32 + lane;
+                v[u] = idx < e ? a.prod[idx] : 0.0;
+            }
+            int cnt = min(512, e - t);
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+#pragma unroll 8
+                for (int src = 0; src < 32; ++src) {
+                    double x = __shfl_sync(0xffffffffu, v[u], src);
+                    if (u * 32 + src < cnt) acc = dadd(acc, x);
+                }
+            }
+        }
+        if (lane == 0) m.part[ch] = acc;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = -0.0;
-        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, a.partials[ch]);
+        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, m.part[ch]);
         sh[0] = s;
     }
     __syncthreads();
@@ -201,43 +292,49 @@ __device__ __forceinline__ double pcg_dot(const PcgArgs& a, const double* x, con
     return r;
 }
 
-// build_mic0 (pressure.rs:442-513) as a forward level sweep; precon values of
-// level L-1 are read from the shared window (or global when the level is wider).
-__device__ void pcg_build_mic0(const PcgArgs& a, double* win0, double* win1) {
+// build_mic0 (pressure.rs:442-513) as a forward level sweep. precon and the
+// neighbour mask of level L-1 come from the shared windows.
+__device__ void pcg_build_mic0(const PcgArgs& a, const PcgSmem& m, int sw, int l0, int l1) {
     const double TAU = 0.97, SIGMA = 0.25;
-    double* prev = win0;
-    double* cur = win1;
-    for (int L = 0; L < a.nlevels; ++L) {
-        int ls = a.level_start[L], le = a.level_start[L + 1];
-        int lsp = L > 0 ? a.level_start[L - 1] : 0;
-        bool prev_in = L > 0 && (ls - lsp) <= kPcgWin;
-        bool cur_in = (le - ls) <= kPcgWin;
-        for (int ps = ls + threadIdx.x; ps < le; ps += blockDim.x) {
+    if ((int)threadIdx.x >= sw) {
+        __syncthreads();
+        return;
+    }
+    double* prev = m.w0;
+    double* cur = m.w1;
+    int* mprev = m.m0;
+    int* mcur = m.m1;
+    for (int L = l0; L < l1; ++L) {
+        int ls = m.lvs[L], le = m.lvs[L + 1];
+        int lsp = L > 0 ? m.lvs[L - 1] : 0;
+        bool prev_in = L > l0 && (ls - lsp) <= kPcgBS;
+        bool cur_in = (le - ls) <= kPcgBS;
+        for (int ps = ls + threadIdx.x; ps < le; ps += sw) {
             const int* nb = a.nbr + (size_t)ps * 6;
             double axi = 0, pxi = 0, axi_y = 0, axi_z = 0;
             double ayj = 0, pyj = 0, ayj_x = 0, ayj_z = 0;
             double azk = 0, pzk = 0, azk_x = 0, azk_y = 0;
-            int m = nb[NB_MX];
-            if (m >= 0) {
-                uint8_t mk = a.nmask[m];
+            int mm = nb[NB_MX];
+            if (mm >= 0) {
+                int mk = prev_in ? mprev[mm - lsp] : a.nmask[mm];
                 axi = -1.0;
-                pxi = prev_in ? prev[m - lsp] : a.precon[m];
+                pxi = prev_in ? prev[mm - lsp] : a.precon[mm];
                 axi_y = (mk >> NB_PY & 1) ? -1.0 : 0.0;
                 axi_z = (mk >> NB_PZ & 1) ? -1.0 : 0.0;
             }
-            m = nb[NB_MY];
-            if (m >= 0) {
-                uint8_t mk = a.nmask[m];
+            mm = nb[NB_MY];
+            if (mm >= 0) {
+                int mk = prev_in ? mprev[mm - lsp] : a.nmask[mm];
                 ayj = -1.0;
-                pyj = prev_in ? prev[m - lsp] : a.precon[m];
+                pyj = prev_in ? prev[mm - lsp] : a.precon[mm];
                 ayj_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
                 ayj_z = (mk >> NB_PZ & 1) ? -1.0 : 0.0;
             }
-            m = nb[NB_MZ];
-            if (m >= 0) {
-                uint8_t mk = a.nmask[m];
+            mm = nb[NB_MZ];
+            if (mm >= 0) {
+                int mk = prev_in ? mprev[mm - lsp] : a.nmask[mm];
                 azk = -1.0;
-                pzk = prev_in ? prev[m - lsp] : a.precon[m];
+                pzk = prev_in ? prev[mm - lsp] : a.precon[mm];
                 azk_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
                 azk_y = (mk >> NB_PY & 1) ? -1.0 : 0.0;
             }
@@ -251,122 +348,381 @@ __device__ void pcg_build_mic0(const PcgArgs& a, double* win0, double* win1) {
             if (e < dmul(SIGMA, diag)) e = diag;
             double pc = e > 0.0 ? ddiv(1.0, __dsqrt_rn(e)) : 0.0;
             a.precon[ps] = pc;
-            if (cur_in) cur[ps - ls] = pc;
+            if (cur_in) {
+                cur[ps - ls] = pc;
+                mcur[ps - ls] = a.nmask[ps];
+            }
         }
-        __syncthreads();
+        sweep_bar(sw);
         double* t = prev;
         prev = cur;
         cur = t;
+        int* tm = mprev;
+        mprev = mcur;
+        mcur = tm;
     }
+    __syncthreads();
+}
+
+// Per-solve sweep records from the neighbour table and the factor.
+__device__ void pcg_build_records(const PcgArgs& a, const PcgSmem& m, uint32_t nf) {
+    for (uint32_t ps = threadIdx.x; ps < nf; ps += blockDim.x) {
+        uint32_t c = a.lv_cell[ps];
+        int i = c % a.nx, j = (c / a.nx) % a.ny, k = c / (a.nx * a.ny);
+        int L = i + j + k;
+        const int* nb = a.nbr + (size_t)ps * 6;
+        int lsp = L > 0 ? m.lvs[L - 1] : 0, lsn = m.lvs[L + 1];
+        SweepRec f, g;
+        f.pc = g.pc = a.precon[ps];
+        int mm;
+        f.s0 = (short)((mm = nb[NB_MX]) >= 0 ? mm - lsp : -1);
+        f.s1 = (short)((mm = nb[NB_MY]) >= 0 ? mm - lsp : -1);
+        f.s2 = (short)((mm = nb[NB_MZ]) >= 0 ? mm - lsp : -1);
+        g.s0 = (short)((mm = nb[NB_PX]) >= 0 ? mm - lsn : -1);
+        g.s1 = (short)((mm = nb[NB_PY]) >= 0 ? mm - lsn : -1);
+        g.s2 = (short)((mm = nb[NB_PZ]) >= 0 ? mm - lsn : -1);
+        f.pad = g.pad = 0;
+        a.frec[ps] = *reinterpret_cast<int4*>(&f);
+        a.brec[ps] = *reinterpret_cast<int4*>(&g);
+    }
+    __syncthreads();
 }
 
 // apply_mic0 (pressure.rs:517-570): forward L q = r then backward L^T z = q.
 // Forward:  t = r + pq[-x] + pq[-y] + pq[-z]  (pq = precon*q of the predecessor,
 //           which is what `t -= plus*precon*q` with plus = -1 adds), q = t*pc.
-// Backward: t = q + pc*z[+x] + pc*z[+y] + pc*z[+z], z = t*pc.
-__device__ void pcg_apply_mic0(const PcgArgs& a, const double* r, double* z, double* win0,
-                               double* win1) {
-    double* prev = win0;
-    double* cur = win1;
-    for (int L = 0; L < a.nlevels; ++L) {
-        int ls = a.level_start[L], le = a.level_start[L + 1];
-        int lsp = L > 0 ? a.level_start[L - 1] : 0;
-        bool prev_in = L > 0 && (ls - lsp) <= kPcgWin;
-        bool cur_in = (le - ls) <= kPcgWin;
-        for (int ps = ls + threadIdx.x; ps < le; ps += blockDim.x) {
-            const int* nb = a.nbr + (size_t)ps * 6;
-            double t = r[ps];
-            int m = nb[NB_MX];
-            if (m >= 0) t = dadd(t, prev_in ? prev[m - lsp] : a.pq[m]);
-            m = nb[NB_MY];
-            if (m >= 0) t = dadd(t, prev_in ? prev[m - lsp] : a.pq[m]);
-            m = nb[NB_MZ];
-            if (m >= 0) t = dadd(t, prev_in ? prev[m - lsp] : a.pq[m]);
-            double pc = a.precon[ps];
-            double qv = dmul(t, pc);
-            double pqv = dmul(pc, qv);
-            a.q[ps] = qv;
-            a.pq[ps] = pqv;
-            if (cur_in) cur[ps - ls] = pqv;
-        }
+// Backward: t = q + pc*z[+x] + pc*z[+y] + pc*z[+z], z = t*pc, plus the z*r
+//           products of the following dot.
+// Compute threads [0, sw) take one cell each per level from the staged ring;
+// the producer warp [sw, sw+32) stages level L + kStages - 1 while level L is
+// computed. Levels wider than the ring use global memory (uniform branch).
+__device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const double* r, double* z, int sw, int l0,
+                                 int l1, unsigned long long* lt = nullptr) {
+    const int tid = threadIdx.x;
+    const int nbar = sw + 32;
+    double zr = 0.0;
+    if (tid >= nbar) {
         __syncthreads();
-        double* t = prev;
-        prev = cur;
-        cur = t;
+        return zr;
     }
-    double* next = win0;
-    cur = win1;
-    for (int L = a.nlevels - 1; L >= 0; --L) {
-        int ls = a.level_start[L], le = a.level_start[L + 1];
-        int lsn = a.level_start[L + 1];
-        int len_next = L + 1 < a.nlevels ? a.level_start[L + 2] - lsn : 0;
-        bool next_in = L + 1 < a.nlevels && len_next <= kPcgWin;
-        bool cur_in = (le - ls) <= kPcgWin;
-        for (int ps = ls + threadIdx.x; ps < le; ps += blockDim.x) {
-            const int* nb = a.nbr + (size_t)ps * 6;
-            double pc = a.precon[ps];
-            double t = a.q[ps];
-            int m = nb[NB_PX];
-            if (m >= 0) t = dadd(t, dmul(pc, next_in ? next[m - lsn] : z[m]));
-            m = nb[NB_PY];
-            if (m >= 0) t = dadd(t, dmul(pc, next_in ? next[m - lsn] : z[m]));
-            m = nb[NB_PZ];
-            if (m >= 0) t = dadd(t, dmul(pc, next_in ? next[m - lsn] : z[m]));
-            double zv = dmul(t, pc);
-            z[ps] = zv;
-            if (cur_in) cur[ps - ls] = zv;
+    const bool producer = tid >= sw;
+    const int lane = tid - sw;
+    // ---------------- forward
+    if (producer) {
+        for (int d = 0; d < kStages - 1; ++d) produce_level(m, l0 + d, l0, l1, r, nullptr, a.frec, lane);
+        cp_wait_ahead();
+    }
+    sweep_bar(nbar);
+    double* prev = m.w0;
+    double* cur = m.w1;
+    int lsP = l0 > 0 ? m.lvs[l0 - 1] : 0, lsA = m.lvs[l0], lsB = m.lvs[l0 + 1];
+    // staged operands of this thread's cell in the current level (registers)
+    double ct = 0.0;
+    SweepRec crc{};
+    if (!producer && tid < lsB - lsA && lsB - lsA <= kSweepMax) {
+        int slot = (l0 % kStages) * kPcgBS + tid;
+        ct = m.sa[slot];
+        crc = m.sr[slot];
+    }
+    for (int L = l0; L < l1; ++L) {
+        int lsC = m.lvs[min(L + 2, a.nlevels)];
+        unsigned long long c0 = lt ? clock64() : 0;
+        const int wprev = lsA - lsP, wcur = lsB - lsA, wnext = lsC - lsB;
+        double nt_ = 0.0;
+        SweepRec nrc{};
+        if (producer) {
+            produce_level(m, L + kStages - 1, l0, l1, r, nullptr, a.frec, lane);
+            cp_wait_ahead();
+        } else {
+            if (L + 1 < l1 && tid < wnext && wnext <= kSweepMax) {  // prefetch level L+1
+                int slot = ((L + 1) % kStages) * kPcgBS + tid;
+                nt_ = m.sa[slot];
+                nrc = m.sr[slot];
+            }
+            if (wcur <= kSweepMax) {
+                if (tid < wcur) {
+                    double t = ct;
+                    if (wprev <= kPcgBS) {
+                        if (crc.s0 >= 0) t = dadd(t, prev[crc.s0]);
+                        if (crc.s1 >= 0) t = dadd(t, prev[crc.s1]);
+                        if (crc.s2 >= 0) t = dadd(t, prev[crc.s2]);
+                    } else {
+                        const int* nb = a.nbr + (size_t)(lsA + tid) * 6;
+                        int mm;
+                        if ((mm = nb[NB_MX]) >= 0) t = dadd(t, a.pq[mm]);
+                        if ((mm = nb[NB_MY]) >= 0) t = dadd(t, a.pq[mm]);
+                        if ((mm = nb[NB_MZ]) >= 0) t = dadd(t, a.pq[mm]);
+                    }
+                    double qv = dmul(t, crc.pc);
+                    double pqv = dmul(crc.pc, qv);
+                    cur[tid] = pqv;
+                    a.q[lsA + tid] = qv;
+                }
+            } else {
+                for (int ps = lsA + tid; ps < lsB; ps += sw) {
+                    const int* nb = a.nbr + (size_t)ps * 6;
+                    double t = r[ps];
+                    int mm;
+                    if (wprev <= kPcgBS) {
+                        if ((mm = nb[NB_MX]) >= 0) t = dadd(t, prev[mm - lsP]);
+                        if ((mm = nb[NB_MY]) >= 0) t = dadd(t, prev[mm - lsP]);
+                        if ((mm = nb[NB_MZ]) >= 0) t = dadd(t, prev[mm - lsP]);
+                    } else {
+                        if ((mm = nb[NB_MX]) >= 0) t = dadd(t, a.pq[mm]);
+                        if ((mm = nb[NB_MY]) >= 0) t = dadd(t, a.pq[mm]);
+                        if ((mm = nb[NB_MZ]) >= 0) t = dadd(t, a.pq[mm]);
+                    }
+                    double pc = a.precon[ps];
+                    double qv = dmul(t, pc);
+                    a.q[ps] = qv;
+                    a.pq[ps] = dmul(pc, qv);
+                }
+            }
         }
-        __syncthreads();
-        double* t = next;
-        next = cur;
-        cur = t;
+        unsigned long long c1 = lt ? clock64() : 0;
+        sweep_bar(nbar);
+        if (lt) {
+            unsigned long long c2 = clock64();
+            lt[1] += c1 - c0;
+            lt[2] += c2 - c1;
+            lt[3] += 1;
+        }
+        if (wcur <= kPcgBS) {
+            double* tt = prev;
+            prev = cur;
+            cur = tt;
+        }
+        ct = nt_;
+        crc = nrc;
+        lsP = lsA;
+        lsA = lsB;
+        lsB = lsC;
     }
+    if (producer) asm volatile("cp.async.wait_all;" ::: "memory");
+    sweep_bar(nbar);
+    // ---------------- backward
+    if (producer) {
+        for (int d = 0; d < kStages - 1; ++d) produce_level(m, l1 - 1 - d, l0, l1, a.q, r, a.brec, lane);
+        cp_wait_ahead();
+    }
+    sweep_bar(nbar);
+    double* next = m.w0;
+    cur = m.w1;
+    int lsN = m.lvs[l1], lsH = m.lvs[min(l1 + 1, a.nlevels)];  // starts of levels L+1, L+2
+    lsA = m.lvs[l1 - 1];
+    double cq = 0.0, cr = 0.0;
+    crc = SweepRec{};
+    if (!producer && tid < lsN - lsA && lsN - lsA <= kSweepMax) {
+        int slot = ((l1 - 1) % kStages) * kPcgBS + tid;
+        cq = m.sa[slot];
+        cr = m.sb[slot];
+        crc = m.sr[slot];
+    }
+    for (int L = l1 - 1; L >= l0; --L) {
+        int lsQ = L > 0 ? m.lvs[L - 1] : 0;
+        const int wnext = lsH - lsN, wcur = lsN - lsA, wlow = lsA - lsQ;
+        double nq = 0.0, nr = 0.0;
+        SweepRec nrc{};
+        if (producer) {
+            produce_level(m, L - (kStages - 1), l0, l1, a.q, r, a.brec, lane);
+            cp_wait_ahead();
+        } else {
+            if (L - 1 >= l0 && tid < wlow && wlow <= kSweepMax) {  // prefetch level L-1
+                int slot = ((L - 1) % kStages) * kPcgBS + tid;
+                nq = m.sa[slot];
+                nr = m.sb[slot];
+                nrc = m.sr[slot];
+            }
+            if (wcur <= kSweepMax) {
+                if (tid < wcur) {
+                    double t = cq, pc = crc.pc;
+                    if (L + 1 < l1 && wnext <= kPcgBS) {
+                        if (crc.s0 >= 0) t = dadd(t, dmul(pc, next[crc.s0]));
+                        if (crc.s1 >= 0) t = dadd(t, dmul(pc, next[crc.s1]));
+                        if (crc.s2 >= 0) t = dadd(t, dmul(pc, next[crc.s2]));
+                    } else {
+                        const int* nb = a.nbr + (size_t)(lsA + tid) * 6;
+                        int mm;
+                        if ((mm = nb[NB_PX]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                        if ((mm = nb[NB_PY]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                        if ((mm = nb[NB_PZ]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                    }
+                    double zv = dmul(t, pc);
+                    cur[tid] = zv;
+                    z[lsA + tid] = zv;
+                    double pr = dmul(zv, cr);
+                    if (a.exact_dots) a.prod[a.cinv[lsA + tid]] = pr;
+                    else zr = dadd(zr, pr);
+                }
+            } else {
+                for (int ps = lsA + tid; ps < lsN; ps += sw) {
+                    const int* nb = a.nbr + (size_t)ps * 6;
+                    double pc = a.precon[ps];
+                    double t = a.q[ps];
+                    int mm;
+                    if (L + 1 < l1 && wnext <= kPcgBS) {
+                        if ((mm = nb[NB_PX]) >= 0) t = dadd(t, dmul(pc, next[mm - lsN]));
+                        if ((mm = nb[NB_PY]) >= 0) t = dadd(t, dmul(pc, next[mm - lsN]));
+                        if ((mm = nb[NB_PZ]) >= 0) t = dadd(t, dmul(pc, next[mm - lsN]));
+                    } else {
+                        if ((mm = nb[NB_PX]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                        if ((mm = nb[NB_PY]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                        if ((mm = nb[NB_PZ]) >= 0) t = dadd(t, dmul(pc, z[mm]));
+                    }
+                    double zv = dmul(t, pc);
+                    z[ps] = zv;
+                    double pr = dmul(zv, r[ps]);
+                    if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
+                    else zr = dadd(zr, pr);
+                }
+            }
+        }
+        sweep_bar(nbar);
+        if (wcur <= kPcgBS) {
+            double* tt = next;
+            next = cur;
+            cur = tt;
+        }
+        cq = nq;
+        cr = nr;
+        crc = nrc;
+        lsH = lsN;
+        lsN = lsA;
+        lsA = lsQ;
+    }
+    if (producer) asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    return zr;
 }
 
 // pcg (pressure.rs:341-397) in one persistent block.
 __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
-    extern __shared__ double win[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[40];
-    double* win0 = win;
-    double* win1 = win + kPcgWin;
+    PcgSmem m;
+    {
+        unsigned char* q = smem_raw;
+        m.sr = (SweepRec*)q; q += (size_t)kStages * kPcgBS * 16;
+        m.sa = (double*)q; q += (size_t)kStages * kPcgBS * 8;
+        m.sb = (double*)q; q += (size_t)kStages * kPcgBS * 8;
+        m.w0 = (double*)q; q += (size_t)kPcgBS * 8;
+        m.w1 = (double*)q; q += (size_t)kPcgBS * 8;
+        m.part = (double*)q; q += (size_t)kMaxChunksSmem * 8;
+        m.m0 = (int*)q; q += (size_t)kPcgBS * 4;
+        m.m1 = (int*)q; q += (size_t)kPcgBS * 4;
+        m.lvs = (int*)q;
+    }
+    if (a.nlevels > kMaxLevelsSmem) m.lvs = const_cast<int*>(a.level_start);
+    else
+        for (int L = threadIdx.x; L <= a.nlevels; L += blockDim.x) m.lvs[L] = a.level_start[L];
+    if (a.nchunks > kMaxChunksSmem) m.part = a.partials;
+    __syncthreads();
     const uint32_t nf = *a.nf;
     const int tid = threadIdx.x, nt = blockDim.x;
+    // Non-empty level range and the widest level -> sweep width (warps).
+    __shared__ int s_l0, s_l1, s_wmax;
+    if (tid == 0) {
+        s_l0 = a.nlevels;
+        s_l1 = 0;
+        s_wmax = 0;
+    }
+    __syncthreads();
+    for (int L = tid; L < a.nlevels; L += nt) {
+        int w = m.lvs[L + 1] - m.lvs[L];
+        if (w > 0) {
+            atomicMin(&s_l0, L);
+            atomicMax(&s_l1, L + 1);
+            atomicMax(&s_wmax, w);
+        }
+    }
+    __syncthreads();
+    const int l0 = s_l0, l1 = s_l1;
+    const int sw = min(kSweepMax, max(32, (s_wmax + 31) & ~31));
 
-    double m = 0.0;
-    for (uint32_t i = tid; i < nf; i += nt) m = fmax(m, fabs(a.b[i]));
-    double residual = block_max<kPcgBS>(m, sh);
+    // Section timers (thread 0 only, kept in shared memory to spare registers).
+    __shared__ unsigned long long tsec[8], ltim[4], tck;
+    const bool timed = a.timing != nullptr;
+    if (tid == 0) {
+        for (int q = 0; q < 8; ++q) tsec[q] = 0;
+        for (int q = 0; q < 4; ++q) ltim[q] = 0;
+        tck = clock64();
+    }
+    unsigned long long* lt = (timed && tid == 0) ? ltim : nullptr;
+#define SECTION(idx)                                   \
+    do {                                               \
+        if (timed && tid == 0) {                       \
+            unsigned long long now_ = clock64();       \
+            tsec[idx] += now_ - tck;                   \
+            tck = now_;                                \
+        }                                              \
+    } while (0)
+    double mx = 0.0;
+    for (uint32_t i = tid; i < nf; i += nt) mx = fmax(mx, fabs(a.b[i]));
+    double residual = block_max<kPcgBS>(mx, sh);
     int iters = 0;
     if (residual > a.tol) {
-        pcg_build_mic0(a, win0, win1);
+        SECTION(7);
+        pcg_build_mic0(a, m, sw, l0, l1);
+        pcg_build_records(a, m, nf);
+        SECTION(0);
         for (uint32_t i = tid; i < nf; i += nt) {
             a.r[i] = a.b[i];
             a.p[i] = 0.0;
         }
         __syncthreads();
-        pcg_apply_mic0(a, a.r, a.z, win0, win1);
+        double zr = pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1);
+        SECTION(1);
         for (uint32_t i = tid; i < nf; i += nt) a.s[i] = a.z[i];
         __syncthreads();
-        double sigma = pcg_dot(a, a.z, a.r, sh);
+        double sigma = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(zr, sh);  // dot(z, r)
+        SECTION(4);
         for (int it = 0; it < a.max_iters; ++it) {
             iters = it + 1;
-            // apply_a (pressure.rs:400-439): diag*x, then +x,-x,+y,-y,+z,-z
-            for (uint32_t i = tid; i < nf; i += nt) {
-                const int* nb = a.nbr + (size_t)i * 6;
-                double v = dmul((double)a.diag[i], a.s[i]);
-                int o;
-                if ((o = nb[NB_PX]) >= 0) v = dsub(v, a.s[o]);
-                if ((o = nb[NB_MX]) >= 0) v = dsub(v, a.s[o]);
-                if ((o = nb[NB_PY]) >= 0) v = dsub(v, a.s[o]);
-                if ((o = nb[NB_MY]) >= 0) v = dsub(v, a.s[o]);
-                if ((o = nb[NB_PZ]) >= 0) v = dsub(v, a.s[o]);
-                if ((o = nb[NB_MZ]) >= 0) v = dsub(v, a.s[o]);
-                a.as[i] = v;
+            // apply_a (pressure.rs:400-439): diag*x, then +x,-x,+y,-y,+z,-z; and s*As.
+            // Two cells per thread per round, index loads first for memory parallelism.
+            double sas = 0.0;
+            for (uint32_t i0 = tid; i0 < nf; i0 += 2 * nt) {
+                int nbv[2][6];
+                double sv[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    uint32_t i = i0 + u * nt;
+                    if (i < nf) {
+                        const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
+                        int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
+                        nbv[u][0] = x0.x; nbv[u][1] = x0.y; nbv[u][2] = x1.x;
+                        nbv[u][3] = x1.y; nbv[u][4] = x2.x; nbv[u][5] = x2.y;
+                        sv[u] = a.s[i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    uint32_t i = i0 + u * nt;
+                    if (i < nf) {
+                        double nsv[6];
+#pragma unroll
+                        for (int d = 0; d < 6; ++d) nsv[d] = nbv[u][d] >= 0 ? a.s[nbv[u][d]] : 0.0;
+                        double v = dmul((double)a.diag[i], sv[u]);
+                        if (nbv[u][NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
+                        if (nbv[u][NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
+                        if (nbv[u][NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
+                        if (nbv[u][NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
+                        if (nbv[u][NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
+                        if (nbv[u][NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
+                        a.as[i] = v;
+                        if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv[u], v);
+                        else sas = dadd(sas, dmul(sv[u], v));
+                    }
+                }
             }
             __syncthreads();
-            double denom = pcg_dot(a, a.s, a.as, sh);
+            SECTION(3);
+            double denom = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(sas, sh);  // dot(s, As)
+            SECTION(4);
             if (fabs(denom) < 1e-30) break;
             double alpha = ddiv(sigma, denom);
             double mr = 0.0;
+#pragma unroll 4
             for (uint32_t i = tid; i < nf; i += nt) {
                 a.p[i] = dadd(a.p[i], dmul(alpha, a.s[i]));
                 double rv = dsub(a.r[i], dmul(alpha, a.as[i]));
@@ -374,19 +730,33 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
                 mr = fmax(mr, fabs(rv));
             }
             residual = block_max<kPcgBS>(mr, sh);
+            SECTION(5);
             if (residual <= a.tol) break;
-            pcg_apply_mic0(a, a.r, a.z, win0, win1);
-            double sigma_new = pcg_dot(a, a.z, a.r, sh);
+            zr = pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1, lt);
+            SECTION(1);
+            double sigma_new = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(zr, sh);  // dot(z, r)
+            SECTION(4);
             double beta = ddiv(sigma_new, sigma);
+#pragma unroll 4
             for (uint32_t i = tid; i < nf; i += nt) a.s[i] = dadd(a.z[i], dmul(beta, a.s[i]));
             __syncthreads();
+            SECTION(6);
             sigma = sigma_new;
         }
         for (uint32_t i = tid; i < nf; i += nt) a.p_dense[a.lv_cell[i]] = a.p[i];
     }
+    SECTION(7);
+#undef SECTION
     if (tid == 0) {
         *a.out_iters = iters;
         *a.out_residual = residual;
+        if (a.timing) {
+            for (int q = 0; q < 8; ++q) a.timing[q] += tsec[q];
+            for (int q = 0; q < 4; ++q) a.timing[8 + q] += ltim[q];
+            a.timing[12] += (unsigned long long)sw;
+            a.timing[13] += (unsigned long long)(l1 - l0);
+            a.timing[14] += 1;
+        }
     }
 }
 
@@ -395,8 +765,8 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
 __global__ void k_gradient(Grid g, const uint8_t* __restrict__ cells, const double* __restrict__ p,
                            double coef, float* __restrict__ u, float* __restrict__ v,
                            float* __restrict__ w) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx) return;
+    int i, j, k;
+    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
     size_t c = ((size_t)k * g.ny + j) * g.nx + i;
     if (j < g.ny && k < g.nz && i >= 1 && i < g.nx) {
         uint8_t l = cells[c - 1], r = cells[c];

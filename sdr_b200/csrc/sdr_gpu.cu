@@ -18,7 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sdr_gpu.h"
+#include "sdr_gpu.h"
 #include "common.cuh"
 #include "grid.cuh"
 #include "metrics.cuh"
@@ -85,6 +85,7 @@ struct DevStatus {
     uint32_t hist_max;
     unsigned long long fluid_count;
     unsigned long long wall_count;
+    unsigned long long pcg_cycles[16];
 };
 
 __global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
@@ -159,6 +160,8 @@ struct sdr_solver {
     uint32_t *drn = nullptr;
     uint32_t *hist_valid = nullptr, *hist_sort = nullptr, *start = nullptr, *fill = nullptr;
     uint32_t* long_list = nullptr;
+    double4* lrec = nullptr;
+    float4* vrec = nullptr;
     uint32_t* tsum = nullptr;
     size_t tsum_cap = 0;
     DevStatus* dst = nullptr;
@@ -167,10 +170,11 @@ struct sdr_solver {
     int nlevels = 0, nchunks = 0;
     uint32_t *lines_cnt = nullptr, *lv_cell = nullptr, *cflag = nullptr, *coff = nullptr;
     int *level_start = nullptr, *pos_of_cell = nullptr, *nbr = nullptr, *corder = nullptr,
-        *chunk_start = nullptr;
+        *chunk_start = nullptr, *cinv = nullptr;
     uint8_t *diag = nullptr, *nmask = nullptr;
     double *b = nullptr, *precon = nullptr, *p = nullptr, *r = nullptr, *z = nullptr, *s = nullptr,
-           *as = nullptr, *q = nullptr, *pq = nullptr, *partials = nullptr, *p_dense = nullptr;
+           *as = nullptr, *q = nullptr, *pq = nullptr, *partials = nullptr, *p_dense = nullptr, *prod = nullptr;
+    int4 *frec = nullptr, *brec = nullptr;
     // redistribution
     uint32_t* cand = nullptr;
     int* slots = nullptr;
@@ -186,6 +190,25 @@ struct sdr_solver {
     MetricsOut* mout = nullptr;
     MetricsOut* h_mout = nullptr;
     bool sorted_valid = false;  // perm/start describe the current particle set
+    // timing
+    cudaEvent_t ev[10] = {};
+    bool profiling = false;
+    bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
+    sdr_profile prof{};
+    uint64_t particle_substeps = 0, substeps_total = 0;
+    double device_ms = 0.0;
+
+    void create_events() {
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+    }
+    void mark(int i) {
+        if (profiling || i == 0 || i == 9) CK(cudaEventRecord(ev[i], st));
+    }
+    float elapsed(int a, int b) const {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[a], ev[b]);
+        return ms;
+    }
 
     double particle_volume() const {  // solver.rs:225-228
         double cell = g.dx * g.dx * g.dx;
@@ -198,6 +221,7 @@ struct sdr_solver {
     Sdf sdf_f() const { return Sdf{snx, sny, snz, (float)sdx, (float)sox, (float)soy, (float)soz, sdf32}; }
     SdfD sdf_d() const { return SdfD{snx, sny, snz, sdx, sox, soy, soz, sdf64}; }
     Faces faces() const { return Faces{u, v, w}; }
+    size_t nnodes() const { return ((size_t)g.nx + 1) * ((size_t)g.ny + 1) * ((size_t)g.nz + 1); }
     Faces saved() const { return Faces{su, sv, sw}; }
     uint32_t* dn() { return &dst->n; }
 
@@ -245,6 +269,8 @@ struct sdr_solver {
         dalloc(cand, ncap);
         dalloc(slots, ncap * 7);
         dalloc(moves, ncap * 2);
+        dalloc(lrec, ncap);
+        dalloc(vrec, ncap);
         cap = ncap;
         sorted_valid = false;
     }
@@ -282,6 +308,10 @@ struct sdr_solver {
         dalloc(s, nc); dalloc(as, nc); dalloc(q, nc); dalloc(pq, nc);
         dalloc(partials, nchunks + 1);
         dalloc(corder, nc);
+        dalloc(cinv, nc);
+        dalloc(prod, nc);
+        dalloc(frec, nc);
+        dalloc(brec, nc);
         dalloc(chunk_start, nchunks + 1);
         dalloc(cflag, nc);
         dalloc(coff, nc);
@@ -301,16 +331,18 @@ struct sdr_solver {
         dfree(hist_valid); dfree(hist_sort); dfree(start); dfree(fill); dfree(long_list); dfree(tsum);
         dfree(dst);
         dfree(lines_cnt); dfree(lv_cell); dfree(cflag); dfree(coff); dfree(level_start); dfree(pos_of_cell);
-        dfree(nbr); dfree(corder); dfree(chunk_start); dfree(diag); dfree(nmask);
+        dfree(nbr); dfree(corder); dfree(cinv); dfree(prod); dfree(frec); dfree(brec); dfree(chunk_start); dfree(diag); dfree(nmask);
         dfree(b); dfree(precon); dfree(p); dfree(r); dfree(z); dfree(s); dfree(as); dfree(q); dfree(pq);
         dfree(partials); dfree(p_dense);
-        dfree(cand); dfree(slots); dfree(moves);
+        dfree(cand); dfree(slots); dfree(moves); dfree(lrec); dfree(vrec);
         dfree(mcell); dfree(mpart); dfree(mout);
         if (hst) cudaFreeHost(hst);
         if (h_epos) cudaFreeHost(h_epos);
         if (h_evel) cudaFreeHost(h_evel);
         if (h_mout) cudaFreeHost(h_mout);
         hst = nullptr; h_epos = nullptr; h_evel = nullptr; h_mout = nullptr;
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
         if (st) cudaStreamDestroy(st);
         st = nullptr;
     }
@@ -382,16 +414,16 @@ struct sdr_solver {
         LAUNCH(k_sort_segments, blocks(ncell, 256), 256, 0, st, start, (uint32_t)ncell, perm, long_list,
                &dst->long_count);
         LAUNCH(k_sort_long, 148, 256, 0, st, start, long_list, &dst->long_count, perm, ptmp);
+        if (n) LAUNCH(k_sorted_records, blocks(n, kBS), kBS, 0, st, g, pos, vel, perm, n, lrec, vrec);
         sorted_valid = true;
     }
 
     void p2g(double dt, bool fused) {
         P2GArgs a{};
         a.g = g;
-        a.pos = pos;
-        a.vel = vel;
+        a.lrec = lrec;
+        a.vrec = vrec;
         a.start = start;
-        a.perm = perm;
         a.u = u; a.v = v; a.w = w;
         a.su = su; a.sv = sv; a.sw = sw;
         a.cells = cells;
@@ -400,8 +432,7 @@ struct sdr_solver {
         a.gdt[2] = fluid.gravity.z * dt;
         a.add_forces = fused;
         a.enforce = fused;
-        dim3 grid(blocks(g.nx + 1, kBS), g.ny + 1, g.nz + 1);
-        LAUNCH(k_p2g, grid, kBS, 0, st, a);
+        LAUNCH(k_p2g, blocks(nnodes(), kBS), kBS, 0, st, a);
     }
 
     void add_forces(double dt) {  // solver.rs:593-604
@@ -411,7 +442,14 @@ struct sdr_solver {
     }
 
     void project(double dt, bool enforce) {  // pressure.rs:123-239 + solver.rs:290-300
-        dim3 ngrid(blocks(g.nx + 1, 256), g.ny + 1, g.nz + 1);
+        project_setup(dt, enforce);
+        project_solve(dt);
+        project_gradient(dt);
+    }
+
+    // enforce_solid_faces, wavefront numbering, neighbour tables, RHS, dot chunks.
+    void project_setup(double dt, bool enforce) {
+        unsigned ngrid = blocks(nnodes(), 256);
         if (enforce) LAUNCH(k_enforce_solid, ngrid, 256, 0, st, g, cells, u, v, w);
         size_t nl = (size_t)nlevels * g.nz;
         LAUNCH(k_lines_count, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt);
@@ -442,18 +480,28 @@ struct sdr_solver {
         LAUNCH(k_tables, blocks(ncell, 256), 256, 0, st, t);
         LAUNCH(k_fluid_flags, blocks(ncell, 256), 256, 0, st, cells, ncell, cflag);
         scan(cflag, coff, ncell, nullptr);
-        LAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, chunk_start,
+        LAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, cinv, chunk_start,
                nchunks, &dst->nf);
         CK(cudaMemsetAsync(p_dense, 0, ncell * 8, st));
+    }
+
+    void project_solve(double dt) {
+        (void)dt;
         PcgArgs a{};
         a.nf = &dst->nf;
         a.nlevels = nlevels;
         a.nchunks = nchunks;
+        a.nx = g.nx;
+        a.ny = g.ny;
+        a.frec = frec;
+        a.brec = brec;
         a.level_start = level_start;
         a.nbr = nbr;
         a.diag = diag;
         a.nmask = nmask;
         a.corder = corder;
+        a.cinv = cinv;
+        a.prod = prod;
         a.chunk_start = chunk_start;
         a.b = b;
         a.precon = precon; a.p = p; a.r = r; a.z = z; a.s = s; a.as = as; a.q = q; a.pq = pq;
@@ -464,13 +512,19 @@ struct sdr_solver {
         a.p_dense = p_dense;
         a.out_iters = &dst->iters;
         a.out_residual = &dst->residual;
-        LAUNCH(k_pcg, 1, kPcgBS, 2 * kPcgWin * sizeof(double), st, a);
+        a.timing = profiling ? dst->pcg_cycles : nullptr;
+        a.exact_dots = exact_dots ? 1 : 0;
+        LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+    }
+
+    void project_gradient(double dt) {
+        unsigned ngrid = blocks(nnodes(), 256);
         double coef = dt / (fluid.density * g.dx);
         LAUNCH(k_gradient, ngrid, 256, 0, st, g, cells, p_dense, coef, u, v, w);
     }
 
     void extrapolate() {  // solver.rs:608-647
-        dim3 ngrid(blocks(g.nx + 1, 256), g.ny + 1, g.nz + 1);
+        unsigned ngrid = blocks(nnodes(), 256);
         LAUNCH(k_extrap_valid, ngrid, 256, 0, st, g, cells, ku, kv, kw);
         CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
         float *a_u = u, *a_v = v, *a_w = w, *b_u = u2, *b_v = v2, *b_w = w2;
@@ -591,20 +645,51 @@ struct sdr_solver {
     }
 
     void substep(double dt) {  // solver.rs:284-310
+        mark(0);
         emit(dt);
         classify(true);
         sort();
+        mark(1);
         p2g(dt, true);
-        project(dt, false);
+        mark(2);
+        project_setup(dt, false);
+        mark(3);
+        project_solve(dt);
+        mark(4);
+        project_gradient(dt);
         extrapolate();
+        mark(5);
         g2p_advect(dt, true, true, true, true);
+        mark(6);
         uint32_t n_before = n;
         compact(true);
+        mark(7);
         if (fluid.redistribute) redistribute(n_before);
+        mark(8);
+        mark(9);
         sync_status();
         last_pcg_iters = (uint64_t)hst->iters;
         last_residual = hst->residual;
         read_grid_speed();
+        device_ms += elapsed(0, 9);
+        particle_substeps += n_before;
+        substeps_total += 1;
+        if (profiling) {
+            prof.emit_classify_sort_ms += elapsed(0, 1);
+            prof.p2g_ms += elapsed(1, 2);
+            prof.pressure_setup_ms += elapsed(2, 3);
+            prof.pcg_ms += elapsed(3, 4);
+            prof.gradient_extrapolate_ms += elapsed(4, 5);
+            prof.g2p_advect_ms += elapsed(5, 6);
+            prof.compact_ms += elapsed(6, 7);
+            prof.redistribute_ms += elapsed(7, 8);
+            prof.substeps += 1;
+            prof.pcg_launches += 1;
+            prof.pcg_cell_iters += (uint64_t)hst->nf * (uint64_t)std::max(hst->iters, 0);
+            prof.fluid_cells += hst->nf;
+            prof.particles += n_before;
+            for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
+        }
         time += dt;
         steps += 1;
     }
@@ -664,6 +749,8 @@ struct sdr_solver {
             if (ph == SDR_PHASE_PROJECT) {
                 last_pcg_iters = (uint64_t)hst->iters;
                 last_residual = hst->residual;
+                if (profiling)
+                    for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
             }
             if (ph == SDR_PHASE_EXTRAPOLATE) read_grid_speed();
         }
@@ -752,8 +839,8 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
                 throw Fail{SDR_ERR_NO_DEVICE, "this library is built for sm_100a (B200); device is sm_" +
                                                   std::to_string(prop.major) + std::to_string(prop.minor)};
             CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
-            CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(2 * kPcgWin * sizeof(double))));
+            s->create_events();
+            CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmem));
             s->fluid = *fluid;
             s->needle = *needle;
             s->snx = (int)sdf->nx; s->sny = (int)sdf->ny; s->snz = (int)sdf->nz;
@@ -882,6 +969,40 @@ int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* o) {
         o->nx = s->g.nx; o->ny = s->g.ny; o->nz = s->g.nz;
         o->dx = s->g.dx;
         o->origin = sdr_vec3{s->g.ox, s->g.oy, s->g.oz};
+        o->particle_substeps = s->particle_substeps;
+        o->device_ms = s->device_ms;
+        o->substeps_total = s->substeps_total;
+    });
+}
+
+int sdr_solver_set_dot_order(sdr_solver* s, int reference_order) {
+    return guard([&] {
+        require(s, "null solver");
+        s->exact_dots = reference_order != 0;
+    });
+}
+
+int sdr_solver_set_profiling(sdr_solver* s, int on) {
+    return guard([&] {
+        require(s, "null solver");
+        s->profiling = on != 0;
+    });
+}
+
+int sdr_solver_get_profile(const sdr_solver* s, sdr_profile* out) {
+    return guard([&] {
+        require(s && out, "null argument");
+        *out = s->prof;
+    });
+}
+
+int sdr_solver_reset_profile(sdr_solver* s) {
+    return guard([&] {
+        require(s, "null solver");
+        DeviceScope ds(s->device);
+        s->prof = sdr_profile{};
+        CK(cudaMemsetAsync(s->dst->pcg_cycles, 0, sizeof(s->dst->pcg_cycles), s->st));
+        CK(cudaStreamSynchronize(s->st));
     });
 }
 

@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sdr_gpu.h"
+#include "sdr_gpu.h"
 
 namespace {
 

@@ -160,6 +160,21 @@ class Solver:
         check(_lib.load().sdr_solver_get_stats(self._h, C.byref(st)))
         return st
 
+    def set_dot_order(self, reference_order: bool) -> None:
+        """Reference dot order in the PCG (bit-exact pressure) or the faster block tree."""
+        check(_lib.load().sdr_solver_set_dot_order(self._h, 1 if reference_order else 0))
+
+    def set_profiling(self, on: bool) -> None:
+        check(_lib.load().sdr_solver_set_profiling(self._h, 1 if on else 0))
+
+    def profile(self) -> dict:
+        pr = _lib.Profile()
+        check(_lib.load().sdr_solver_get_profile(self._h, C.byref(pr)))
+        return pr.to_dict()
+
+    def reset_profile(self) -> None:
+        check(_lib.load().sdr_solver_reset_profile(self._h))
+
     @property
     def time(self) -> float:
         return self.stats().time

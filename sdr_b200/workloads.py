@@ -1,0 +1,78 @@
+"""Named workloads: the scenes the benchmark and scaling runs are quoted on.
+
+plain_parametric  the `sdr init` parametric sinus at 0.8 mm, 4 ml/s for 0.5 s (52x55x41 cells)
+real_cavity       seeded perturbed-ellipsoid cavity (2.2 ml, ~20k triangles, SH noise 15 %),
+                  winding-number SDF at 0.5 mm; a 1 ml dose (4 ml/s for 0.25 s) then 0.35 s of
+                  settling, 18 frames (the real-cavity shape stood in for by synthetic input)
+large_parametric  the parametric sinus at 0.2 mm (207x217x161 cells), 6 ml/s for 0.3 s then
+                  0.3 s settling, PCG capped at 400 iterations
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import scene as sc
+from .cavity import perturbed_ellipsoid
+
+
+@dataclass
+class Workload:
+    name: str
+    res: sc.ResolvedScene
+    tris: Optional[np.ndarray] = None   # mesh cavities
+    cavity_volume: Optional[float] = None
+    describe: Optional[dict] = None
+
+
+def plain_parametric() -> Workload:
+    cfg = sc.SceneConfig.from_toml_str(
+        "[sim]\nresolution_mm = 0.8\nduration_s = 0.5\nframes = 15\npcg_tol = 1e-6\n"
+        "[needle]\nflow_rate_ml_s = 4.0\n")
+    return Workload("plain_parametric", cfg.resolve(),
+                    describe={"cavity": "parametric sinus (sdr init defaults)", "dx_mm": 0.8,
+                              "flow_ml_s": 4.0, "duration_s": 0.5})
+
+
+def large_parametric() -> Workload:
+    cfg = sc.SceneConfig.from_toml_str(
+        "[sim]\nresolution_mm = 0.2\nduration_s = 0.6\nframes = 18\npcg_iters = 400\npcg_tol = 1e-6\n"
+        "[needle]\nflow_rate_ml_s = 6.0\ninject_s = 0.3\n")
+    return Workload("large_parametric", cfg.resolve(),
+                    describe={"cavity": "parametric sinus", "dx_mm": 0.2, "flow_ml_s": 6.0,
+                              "inject_s": 0.3, "duration_s": 0.6, "pcg_iters": 400})
+
+
+def real_cavity(seed: int = 2, tilt_deg: float = 0.0, flow_ml_s: float = 4.0, dose_ml: float = 1.0,
+                volume_ml: float = 2.2, dx_mm: float = 0.5, duration_s: float = 0.6, frames: int = 18) -> Workload:
+    cav = perturbed_ellipsoid(seed, volume_ml=volume_ml, tilt_deg=tilt_deg)
+    sim_dx = dx_mm * sc.MM
+    fluid = sc.FluidParams(density=1000.0, gravity=(0.0, -9.81, 0.0), flip_ratio=0.7, particles_per_cell=8,
+                           volume_stiffness=1.0, redistribute=True, redist_cap_factor=1.0)
+    needle = sc.Needle(tip=cav.tip, axis=cav.axis, radius=0.5 * 0.8 * sc.MM, flow_rate=flow_ml_s * sc.ML_PER_S,
+                       inject_until=dose_ml / flow_ml_s)
+    res = sc.ResolvedScene(sim_dx=sim_dx, fluid=fluid, needle=needle, outlet=None,
+                           solve=sc.SolveParams(200, 1e-6), frames=frames, frame_dt=duration_s / frames,
+                           sinus=None, mesh_path=None, sdf_dx=sim_dx, mesh_padding=3.0 * sim_dx)
+    return Workload("real_cavity", res, tris=cav.tris, cavity_volume=abs(cav.volume),
+                    describe={"cavity": f"perturbed ellipsoid seed {seed}, {len(cav.tris)} triangles, "
+                                        f"{volume_ml} ml, SH degree 1-4 noise 15%",
+                              "dx_mm": dx_mm, "flow_ml_s": flow_ml_s, "dose_ml": dose_ml,
+                              "duration_s": duration_s, "tilt_deg": tilt_deg})
+
+
+WORKLOADS = {"plain_parametric": plain_parametric, "real_cavity": real_cavity, "large_parametric": large_parametric}
+
+
+def build_gpu(w: Workload, max_particles: int = 0):
+    """Device SDF + solver for a workload; returns (solver, sdf, cavity_volume)."""
+    from .solver import Solver, build_sdf, cavity_volume
+    sdf = build_sdf(w.res, w.tris)
+    vol = w.cavity_volume if w.cavity_volume is not None else cavity_volume(w.res, sdf, w.tris)
+    s = Solver(sdf, w.res.sim_dx, w.res.fluid, w.res.needle, max_particles=max_particles)
+    s.solve = w.res.solve
+    s.outlet = w.res.outlet
+    return s, sdf, vol

@@ -92,8 +92,10 @@ def test_add_forces(pair):
 
 
 def test_project_bit_exact_pressure(pair):
+    """With the reference dot order the solve is bit-exact: same iterations, same pressure bits."""
     gpu, orc, res = pair
     dt = 1e-4
+    gpu.set_dot_order(True)
     gpu.run_phase(_lib.PHASE_CLASSIFY)
     orc.phase(oracle.PHASE_CLASSIFY)
     sync_faces(gpu, orc)
@@ -105,10 +107,31 @@ def test_project_bit_exact_pressure(pair):
     errs = {w: rel_err(gpu.face(w), orc.face(w)) for w in range(3)}
     record("project", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_bit_mismatch": diff,
                        "pressure_rel_err": rel_err(pg, po), "max_p": float(po.max()), "face_rel_err": errs})
+    gpu.set_dot_order(False)
     assert it_g == it_o
     assert diff == 0
     for w in range(3):
         assert errs[w] < FACE_TOL
+
+
+PRESSURE_TOL = 1e-8  # block-tree dots: pressure relative to its max, f64
+
+
+def test_project_tree_dots(pair):
+    """The default block-tree dot order: pressure within 1e-8 relative, iterations within one."""
+    gpu, orc, res = pair
+    dt = 1e-4
+    gpu.run_phase(_lib.PHASE_CLASSIFY)
+    orc.phase(oracle.PHASE_CLASSIFY)
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_PROJECT, dt)
+    orc.phase(oracle.PHASE_PROJECT, dt)
+    pg, po = gpu.pressure(), orc.pressure()
+    it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
+    e = rel_err(pg, po)
+    record("project_tree", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_rel_err": e})
+    assert abs(it_g - it_o) <= 1
+    assert e < PRESSURE_TOL
 
 
 def test_extrapolate(pair):

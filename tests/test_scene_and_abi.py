@@ -1,0 +1,88 @@
+"""Host logic without a GPU: scene configuration (scene.rs tests), the C-ABI
+library's exported symbols, and the README pins of the oracle."""
+import ctypes
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from sdr_b200 import scene as sc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_unknown_keys_are_rejected():  # scene.rs:507-511
+    with pytest.raises(sc.SceneError):
+        sc.SceneConfig.from_toml_str("[needle]\nflowrate_ml_s = 3.0\n")
+
+
+def test_minimal_config_uses_defaults():  # scene.rs:495-504
+    cfg = sc.SceneConfig.from_toml_str("[sim]\nframes = 4\n")
+    assert cfg.sim["frames"] == 4
+    res = cfg.resolve()
+    assert res.frame_dt > 0
+    assert res.outlet is not None and res.sinus is not None
+
+
+def test_millimetre_conversion_is_correct():  # scene.rs:514-531
+    cfg = sc.SceneConfig.from_toml_str("[sinus]\nsemi_axes_mm = [20, 18, 15]\n[needle]\nauto = true\n"
+                                       "diameter_mm = 1.0\nflow_rate_ml_s = 6.0\n")
+    p = cfg.sinus_params()
+    assert abs(p.semi_axes[0] - 0.020) < 1e-12
+    n = cfg.resolve_needle(((0.0, 0.0, 0.0), (0.0, 1.0, 0.0)))
+    assert abs(n.radius - 0.0005) < 1e-12 and abs(n.flow_rate - 6.0e-6) < 1e-18
+
+
+def test_scene_validation_errors():  # scene.rs:267-272, 336-373
+    with pytest.raises(sc.SceneError):
+        sc.SceneConfig.from_toml_str("[sim]\nresolution_mm = 0\n").resolve()
+    with pytest.raises(sc.SceneError):
+        sc.SceneConfig.from_toml_str("[fluid]\nflip_ratio = 1.5\n").resolve()
+    with pytest.raises(sc.SceneError):
+        sc.SceneConfig.from_toml_str("[needle]\nauto = false\n").resolve()
+    with pytest.raises(sc.SceneError):
+        sc.SceneConfig.from_toml_str("[needle]\ntip_mm = [0, 0, 0]\naxis = [0, 0, 0]\n").resolve()
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "sdr_gpu.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|uint64_t|const char\*)\s+(sdr_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from sdr_b200 import _lib
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+    assert lib.sdr_abi_version() == 1
+
+
+def test_library_reports_errors_without_a_device():
+    """No compute call runs here; argument checks fail before touching CUDA."""
+    from sdr_b200 import _lib
+    lib = _lib.load()
+    assert lib.sdr_solver_step(None, 0.01) == 1
+    assert b"null" in lib.sdr_last_error()
+
+
+def test_readme_pins():
+    """Oracle runs of the reference's README scenes (tests/golden/make_readme_pins.py).
+
+    examples/maxillary_real.toml: fill 44.9 % (README.md:58-61) and the 2.228 ml cavity
+    (assets/README.md). examples/scene.toml (README.md:146-151): the injected dose
+    (10.0 ml) and the mean membrane load (436 Pa) agree; the peak fill, coverage,
+    drained volume and focal peak differ by 2-15 %."""
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "readme_pins.json")))
+    mx = d["maxillary_real"]["summary"]
+    assert round(mx["peak_fill_fraction"] * 100, 1) == 44.9
+    assert abs(d["maxillary_real"]["cavity_volume_m3"] * 1e6 - 2.228) < 5e-4
+    assert mx["mass_balance"] == 1.0
+    s = d["scene"]["summary"]
+    assert abs(s["injected_ml"] - 10.0) < 1e-9
+    assert abs(s["mean_membrane_pressure_pa"] - 436) / 436 < 0.01
+    assert abs(s["total_drained_ml"] - 8.11) / 8.11 < 0.03
