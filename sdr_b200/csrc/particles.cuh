@@ -400,13 +400,24 @@ __global__ void k_compact(const float4* __restrict__ pos, const float4* __restri
 //    the cap at the start of a sweep can ever exceed it (receivers stop at the
 //    cap), so only particles in those cells can move;
 //  * decisions read counts only; positions/velocities of moved particles are
-//    functions of (index, destination cell) and can be written afterwards.
-// So: histogram -> index-ordered candidate list -> sequential decision replay
-// over the candidates in shared memory -> parallel move application.
+//    functions of (index, destination cell) and can be written afterwards;
+//  * a sweep that moves nothing leaves the state unchanged, so every later
+//    sweep of the substep moves nothing either.
+// Per sweep: histogram -> append candidates -> one block sorts them by index,
+// replays the sequential decisions in shared memory, and applies the moves.
 
-// n is read from the device (the count after this substep's compaction).
+struct RedistState {
+    uint32_t ncand;   // candidates appended this sweep
+    uint32_t active;  // 0 once a sweep made no move (later sweeps are no-ops)
+    uint32_t nmoves;  // moves of the last sweep
+    uint32_t err;
+    unsigned long long moves_total;
+};
+
 __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
-                                int* __restrict__ key_cell, uint32_t* __restrict__ count) {
+                                const RedistState* __restrict__ rs, int* __restrict__ key_cell,
+                                uint32_t* __restrict__ count) {
+    if (!rs->active) return;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= *n_dev) return;
     float4 q = pos[p];
@@ -415,170 +426,218 @@ __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const ui
     if (c >= 0) atomicAdd(&count[c], 1u);
 }
 
-// Flags over [0, n_upper): zero past the live count so the scan sees exact flags.
-__global__ void k_redist_flag_n(const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
-                                const uint32_t* __restrict__ n_dev, uint32_t n_upper, uint32_t cap,
-                                uint32_t* __restrict__ flag) {
+// Particles in over-cap cells, appended in arbitrary order (sorted later).
+__global__ void k_redist_append(const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
+                                const uint32_t* __restrict__ n_dev, uint32_t cap, RedistState* __restrict__ rs,
+                                uint32_t* __restrict__ cand, uint32_t cand_cap) {
+    if (!rs->active) return;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n_upper) return;
-    if (p >= *n_dev) {
-        flag[p] = 0;
-        return;
-    }
+    if (p >= *n_dev) return;
     int c = key_cell[p];
-    flag[p] = (c >= 0 && count[c] > cap) ? 1u : 0u;
+    if (c >= 0 && count[c] > cap) {
+        uint32_t s = atomicAdd(&rs->ncand, 1u);
+        if (s < cand_cap) cand[s] = p;
+    }
 }
 
-__global__ void k_redist_gather(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
-                                uint32_t n, uint32_t* __restrict__ cand) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < n && flag[p]) cand[off[p]] = p;
-}
-
-constexpr int kRedistTable = 4096;  // shared-memory hash slots (power of two)
+constexpr int kRedistTable = 4096;   // shared-memory hash slots (power of two)
 constexpr int kRedistBS = 1024;
+constexpr int kRedistSmemCand = 8192;  // candidates sorted and replayed in shared memory
 
 struct RedistArgs {
     Grid g;
+    Sdf sdf;
+    Faces f;
+    float4* pos;
+    float4* vel;
     const int* key_cell;
     uint32_t* count;         // histogram at sweep start (the fallback path mutates it)
     const uint8_t* cavity;
-    const uint32_t* cand;    // candidate particles, ascending index
-    const uint32_t* ncand;   // device count
+    uint32_t* cand;          // candidate particles (sorted in place when long)
     uint32_t cand_cap;
-    int* slots;              // 7 per candidate: own cell + 6 neighbours (-1 = none)
     uint32_t cap;
     double down[6];          // dir . gdir for -x,+x,-y,+y,-z,+z (f64, solver.rs:490-511)
     uint32_t* moves;         // pairs (particle, destination cell)
-    uint32_t* nmoves;
-    uint32_t* err;
+    RedistState* rs;
 };
 
 __device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761u) & (kRedistTable - 1); }
 
-// One block. Phase 1: all threads insert every referenced cell into a shared
-// hash table and record slots. Phase 2: thread 0 replays the reference's
-// sequential loop over the candidates (index order), mutating counts, exactly
-// as solver.rs:476-555 does. If the table overflows, thread 0 replays against
-// the global counts instead (same result, slower).
+// One block per sweep: sort the candidates by particle index, insert every
+// referenced cell into a shared hash table, replay the reference's sequential
+// loop (solver.rs:476-555) on thread 0, then apply the moves (solver.rs:545-554)
+// with all threads. If the table overflows or the list is too long for shared
+// memory, thread 0 replays against the global counts (same result, slower).
 __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
-    __shared__ int tkey[kRedistTable];
-    __shared__ uint32_t tcnt[kRedistTable];
-    __shared__ uint8_t tcav[kRedistTable];
+    extern __shared__ __align__(16) unsigned char rsm[];
+    int* tkey = (int*)rsm;                                  // kRedistTable
+    uint32_t* tcnt = (uint32_t*)(tkey + kRedistTable);      // kRedistTable
+    uint32_t* scand = tcnt + kRedistTable;                  // kRedistSmemCand
+    short* slots = (short*)(scand + kRedistSmemCand);       // 7 per candidate
+    uint8_t* tcav = (uint8_t*)(slots + 7 * kRedistSmemCand);  // kRedistTable
     __shared__ int overflow;
-    const uint32_t nc = min(*a.ncand, a.cand_cap);
-    if (threadIdx.x == 0 && *a.ncand > a.cand_cap) atomicOr(a.err, 1u);
+    __shared__ uint32_t s_nm;
+    RedistState* rs = a.rs;
+    if (!rs->active) return;
+    const uint32_t nc_all = rs->ncand;
+    if (nc_all > a.cand_cap) {
+        if (threadIdx.x == 0) atomicOr(&rs->err, 1u);
+        return;
+    }
+    const uint32_t nc = nc_all;
     const Grid& g = a.g;
-    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) tkey[s] = -1;
-    if (threadIdx.x == 0) overflow = 0;
-    __syncthreads();
-    for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
-        int c = a.key_cell[a.cand[m]];
-        int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
-        int nb[7] = {c, i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
-                     j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
-                     k + 1 < g.nz ? c + g.nx * g.ny : -1};
-        for (int q = 0; q < 7; ++q) {
-            int slot = -1;
-            if (nb[q] >= 0) {
-                uint32_t h = rd_hash((uint32_t)nb[q]);
-                for (int probe = 0; probe < kRedistTable; ++probe) {
-                    int prev = atomicCAS(&tkey[h], -1, nb[q]);
-                    if (prev == -1 || prev == nb[q]) {
-                        slot = (int)h;
-                        break;
+    const bool in_smem = nc <= (uint32_t)kRedistSmemCand;
+    // ---- sort candidates ascending (indices are distinct)
+    if (in_smem) {
+        uint32_t np2 = 1;
+        while (np2 < nc) np2 <<= 1;
+        for (uint32_t t = threadIdx.x; t < np2; t += blockDim.x) scand[t] = t < nc ? a.cand[t] : 0xffffffffu;
+        __syncthreads();
+        for (uint32_t k = 2; k <= np2; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = threadIdx.x; t < np2; t += blockDim.x) {
+                    uint32_t o = t ^ j;
+                    if (o > t) {
+                        uint32_t x = scand[t], y = scand[o];
+                        bool up = (t & k) == 0;
+                        if ((x > y) == up) {
+                            scand[t] = y;
+                            scand[o] = x;
+                        }
                     }
-                    h = (h + 1) & (kRedistTable - 1);
                 }
-                if (slot < 0) overflow = 1;
+                __syncthreads();
             }
-            a.slots[(size_t)m * 7 + q] = slot;
-        }
-    }
-    __syncthreads();
-    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) {
-        int c = tkey[s];
-        if (c >= 0) {
-            tcnt[s] = a.count[c];
-            tcav[s] = a.cavity[c];
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    const uint32_t cap = a.cap;
-    uint32_t nm = 0;
-    if (!overflow) {
-        for (uint32_t m = 0; m < nc; ++m) {
-            const int* sl = a.slots + (size_t)m * 7;
-            int s0 = sl[0];
-            if (tcnt[s0] <= cap) continue;
-            int best = -1;
-            double best_down = -INFINITY;
-            uint32_t best_room = 0;
-            for (int q = 1; q < 7; ++q) {
-                int s = sl[q];
-                if (s < 0) continue;
-                if (!tcav[s] || tcnt[s] >= cap) continue;
-                uint32_t room = cap - tcnt[s];
-                double dn = a.down[q - 1];
-                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                    best = s;
-                    best_down = dn;
-                    best_room = room;
-                }
-            }
-            if (best >= 0) {
-                tcnt[s0] -= 1;
-                tcnt[best] += 1;
-                a.moves[2 * nm] = a.cand[m];
-                a.moves[2 * nm + 1] = (uint32_t)tkey[best];
-                ++nm;
-            }
-        }
     } else {
-        uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
-        for (uint32_t m = 0; m < nc; ++m) {
-            int c = a.key_cell[a.cand[m]];
-            if (cnt[c] <= cap) continue;
+        // rank sort in global memory through the moves buffer as scratch
+        for (uint32_t t = threadIdx.x; t < nc; t += blockDim.x) {
+            uint32_t v = a.cand[t], r = 0;
+            for (uint32_t u = 0; u < nc; ++u) r += a.cand[u] < v;
+            a.moves[r] = v;
+        }
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < nc; t += blockDim.x) a.cand[t] = a.moves[t];
+        __syncthreads();
+    }
+    const uint32_t* cl = in_smem ? scand : a.cand;
+    // ---- hash table of referenced cells
+    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) tkey[s] = -1;
+    if (threadIdx.x == 0) {
+        overflow = in_smem ? 0 : 1;
+        s_nm = 0;
+    }
+    __syncthreads();
+    if (in_smem) {
+        for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
+            int c = a.key_cell[cl[m]];
             int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
-            int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+            int nb[7] = {c, i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
                          j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
                          k + 1 < g.nz ? c + g.nx * g.ny : -1};
-            int best = -1;
-            double best_down = -INFINITY;
-            uint32_t best_room = 0;
-            for (int q = 0; q < 6; ++q) {
-                int s = nb[q];
-                if (s < 0 || !a.cavity[s] || cnt[s] >= cap) continue;
-                uint32_t room = cap - cnt[s];
-                double dn = a.down[q];
-                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                    best = s;
-                    best_down = dn;
-                    best_room = room;
+            for (int q = 0; q < 7; ++q) {
+                int slot = -1;
+                if (nb[q] >= 0) {
+                    uint32_t h = rd_hash((uint32_t)nb[q]);
+                    for (int probe = 0; probe < kRedistTable; ++probe) {
+                        int prev = atomicCAS(&tkey[h], -1, nb[q]);
+                        if (prev == -1 || prev == nb[q]) {
+                            slot = (int)h;
+                            break;
+                        }
+                        h = (h + 1) & (kRedistTable - 1);
+                    }
+                    if (slot < 0) overflow = 1;
                 }
+                slots[(size_t)m * 7 + q] = (short)slot;
             }
-            if (best >= 0) {
-                cnt[c] -= 1;
-                cnt[best] += 1;
-                a.moves[2 * nm] = a.cand[m];
-                a.moves[2 * nm + 1] = (uint32_t)best;
-                ++nm;
+        }
+        __syncthreads();
+        for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) {
+            int c = tkey[s];
+            if (c >= 0) {
+                tcnt[s] = a.count[c];
+                tcav[s] = a.cavity[c];
             }
         }
     }
-    *a.nmoves = nm;
-}
-
-// Apply the recorded moves (solver.rs:545-554): position near the destination
-// cell centre with the index-keyed jitter, pushed inside, and the local grid
-// velocity.
-__global__ void k_redist_apply(Grid g, Sdf sdf, Faces f, const uint32_t* __restrict__ moves,
-                               const uint32_t* __restrict__ nmoves, float4* __restrict__ pos,
-                               float4* __restrict__ vel) {
-    uint32_t nm = *nmoves;
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += gridDim.x * blockDim.x) {
-        uint32_t p = moves[2 * m], c = moves[2 * m + 1];
+    __syncthreads();
+    // ---- sequential decisions
+    if (threadIdx.x == 0) {
+        const uint32_t cap = a.cap;
+        uint32_t nm = 0;
+        if (!overflow) {
+            for (uint32_t m = 0; m < nc; ++m) {
+                const short* sl = slots + (size_t)m * 7;
+                int s0 = sl[0];
+                if (tcnt[s0] <= cap) continue;
+                int best = -1;
+                double best_down = -INFINITY;
+                uint32_t best_room = 0;
+#pragma unroll
+                for (int q = 1; q < 7; ++q) {
+                    int s = sl[q];
+                    if (s < 0) continue;
+                    if (!tcav[s] || tcnt[s] >= cap) continue;
+                    uint32_t room = cap - tcnt[s];
+                    double dn = a.down[q - 1];
+                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                        best = s;
+                        best_down = dn;
+                        best_room = room;
+                    }
+                }
+                if (best >= 0) {
+                    tcnt[s0] -= 1;
+                    tcnt[best] += 1;
+                    a.moves[2 * nm] = cl[m];
+                    a.moves[2 * nm + 1] = (uint32_t)tkey[best];
+                    ++nm;
+                }
+            }
+        } else {
+            uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
+            for (uint32_t m = 0; m < nc; ++m) {
+                int c = a.key_cell[cl[m]];
+                if (cnt[c] <= cap) continue;
+                int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+                int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                             j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
+                             k + 1 < g.nz ? c + g.nx * g.ny : -1};
+                int best = -1;
+                double best_down = -INFINITY;
+                uint32_t best_room = 0;
+                for (int q = 0; q < 6; ++q) {
+                    int s = nb[q];
+                    if (s < 0 || !a.cavity[s] || cnt[s] >= cap) continue;
+                    uint32_t room = cap - cnt[s];
+                    double dn = a.down[q];
+                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                        best = s;
+                        best_down = dn;
+                        best_room = room;
+                    }
+                }
+                if (best >= 0) {
+                    cnt[c] -= 1;
+                    cnt[best] += 1;
+                    a.moves[2 * nm] = cl[m];
+                    a.moves[2 * nm + 1] = (uint32_t)best;
+                    ++nm;
+                }
+            }
+        }
+        s_nm = nm;
+        rs->nmoves = nm;
+        rs->moves_total += nm;
+        rs->ncand = 0;
+        if (nm == 0) rs->active = 0;
+    }
+    __syncthreads();
+    // ---- apply the moves: near the destination centre with the index-keyed
+    // jitter, pushed inside, with the local grid velocity.
+    const uint32_t nm = s_nm;
+    for (uint32_t mv = threadIdx.x; mv < nm; mv += blockDim.x) {
+        uint32_t p = a.moves[2 * mv], c = a.moves[2 * mv + 1];
         int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
         uint64_t key = p;
         double jx = jitter_mix(key * 3), jy = jitter_mix(key * 3 + 1), jz = jitter_mix(key * 3 + 2);
@@ -587,11 +646,14 @@ __global__ void k_redist_apply(Grid g, Sdf sdf, Faces f, const uint32_t* __restr
         double cz = dadd(g.oz, dmul((double)k + 0.5, g.dx));
         float3 q = make_float3((float)dadd(cx, dmul(jx, g.dx)), (float)dadd(cy, dmul(jy, g.dx)),
                                (float)dadd(cz, dmul(jz, g.dx)));
-        q = project_inside(sdf, 0.5f * g.dxf, q);
-        float3 v = velocity_at(g, f, q.x, q.y, q.z);
-        pos[p] = make_float4(q.x, q.y, q.z, 0.0f);
-        vel[p] = make_float4(v.x, v.y, v.z, 0.0f);
+        q = project_inside(a.sdf, 0.5f * g.dxf, q);
+        float3 v = velocity_at(g, a.f, q.x, q.y, q.z);
+        a.pos[p] = make_float4(q.x, q.y, q.z, 0.0f);
+        a.vel[p] = make_float4(v.x, v.y, v.z, 0.0f);
     }
 }
+
+constexpr size_t kRedistSmem = (size_t)kRedistTable * 4 * 2 + (size_t)kRedistSmemCand * 4 +
+                               (size_t)kRedistSmemCand * 7 * 2 + kRedistTable;
 
 }  // namespace sdr

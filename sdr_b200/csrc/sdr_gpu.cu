@@ -89,7 +89,15 @@ struct DevStatus {
 };
 
 __global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
-__global__ void k_add_moves(DevStatus* s) { s->moves += s->nmoves; }
+__global__ void k_redist_begin(RedistState* r) {
+    r->ncand = 0;
+    r->active = 1;
+    r->nmoves = 0;
+}
+__global__ void k_redist_end(const RedistState* r, DevStatus* s) {
+    s->moves = r->moves_total;
+    s->err |= r->err;
+}
 __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
     size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < n) out[q] = (float)in[q];
@@ -177,8 +185,8 @@ struct sdr_solver {
     int4 *frec = nullptr, *brec = nullptr;
     // redistribution
     uint32_t* cand = nullptr;
-    int* slots = nullptr;
     uint32_t* moves = nullptr;
+    RedistState* rds = nullptr;
     // emission staging (pinned)
     float4* h_epos = nullptr;
     float4* h_evel = nullptr;
@@ -267,7 +275,6 @@ struct sdr_solver {
         dalloc(off, ncap + 1);
         dalloc(drn, ncap);
         dalloc(cand, ncap);
-        dalloc(slots, ncap * 7);
         dalloc(moves, ncap * 2);
         dalloc(lrec, ncap);
         dalloc(vrec, ncap);
@@ -334,7 +341,7 @@ struct sdr_solver {
         dfree(nbr); dfree(corder); dfree(cinv); dfree(prod); dfree(frec); dfree(brec); dfree(chunk_start); dfree(diag); dfree(nmask);
         dfree(b); dfree(precon); dfree(p); dfree(r); dfree(z); dfree(s); dfree(as); dfree(q); dfree(pq);
         dfree(partials); dfree(p_dense);
-        dfree(cand); dfree(slots); dfree(moves); dfree(lrec); dfree(vrec);
+        dfree(cand); dfree(moves); dfree(rds); dfree(lrec); dfree(vrec);
         dfree(mcell); dfree(mpart); dfree(mout);
         if (hst) cudaFreeHost(hst);
         if (h_epos) cudaFreeHost(h_epos);
@@ -598,30 +605,29 @@ struct sdr_solver {
         V3 gd = vnorm0({fluid.gravity.x, fluid.gravity.y, fluid.gravity.z});
         RedistArgs ra{};
         ra.g = g;
+        ra.sdf = sdf_f();
+        ra.f = faces();
+        ra.pos = pos;
+        ra.vel = vel;
         ra.key_cell = key_cell;
         ra.count = hist_valid;
         ra.cavity = cavity;
         ra.cand = cand;
-        ra.ncand = &dst->ncand;
         ra.cand_cap = (uint32_t)cap;
-        ra.slots = slots;
         ra.cap = cap_;
         const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
         ra.moves = moves;
-        ra.nmoves = &dst->nmoves;
-        ra.err = &dst->err;
+        ra.rs = rds;
+        LAUNCH(k_redist_begin, 1, 1, 0, st, rds);
         for (int sweep = 0; sweep < 4; ++sweep) {
             CK(cudaMemsetAsync(hist_valid, 0, ncell * 4, st));
-            LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), key_cell, hist_valid);
-            LAUNCH(k_redist_flag_n, blocks(n_upper, kBS), kBS, 0, st, key_cell, hist_valid, dn(), n_upper, cap_,
-                   flag);
-            scan(flag, off, n_upper, &dst->ncand);
-            LAUNCH(k_redist_gather, blocks(n_upper, kBS), kBS, 0, st, flag, off, n_upper, cand);
-            LAUNCH(k_redist_replay, 1, kRedistBS, 0, st, ra);
-            LAUNCH(k_redist_apply, 148, 256, 0, st, g, sdf_f(), faces(), moves, &dst->nmoves, pos, vel);
-            LAUNCH(k_add_moves, 1, 1, 0, st, dst);
+            LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), rds, key_cell, hist_valid);
+            LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, key_cell, hist_valid, dn(), cap_, rds, cand,
+                   (uint32_t)cap);
+            LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
         }
+        LAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
         sorted_valid = false;
     }
 
@@ -841,6 +847,7 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
             CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
             s->create_events();
             CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmem));
+            CK(cudaFuncSetAttribute(k_redist_replay, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRedistSmem));
             s->fluid = *fluid;
             s->needle = *needle;
             s->snx = (int)sdf->nx; s->sny = (int)sdf->ny; s->snz = (int)sdf->nz;
@@ -870,6 +877,8 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
             LAUNCH(k_f64_to_f32, blocks(sn, 256), 256, 0, s->st, s->sdf64, s->sdf32, sn);
             dalloc(s->dst, 1);
             CK(cudaMemsetAsync(s->dst, 0, sizeof(DevStatus), s->st));
+            dalloc(s->rds, 1);
+            CK(cudaMemsetAsync(s->rds, 0, sizeof(RedistState), s->st));
             CK(cudaMallocHost((void**)&s->hst, sizeof(DevStatus)));
             CK(cudaMallocHost((void**)&s->h_mout, sizeof(MetricsOut)));
             std::memset(s->hst, 0, sizeof(DevStatus));
