@@ -269,6 +269,31 @@ int sdr_sdf_mesh_grid(const double* tris, size_t ntri, double dx, double padding
  * sign and closest-point distance per node, on the device. */
 int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double dx,
                       const uint64_t dims[3], double* out);
+/* Largest mesh sdr_sdf_from_mesh_noalloc accepts. */
+#define SDR_NOALLOC_MAX_TRIANGLES 32768
+
+/* The winding-number SDF of sdr_sdf_from_mesh for callers that cannot
+ * allocate device memory: hosts that hand out their whole GPU memory budget
+ * up front, code running while a stream is being captured (where cudaMalloc is
+ * not allowed), or latency-bound loops that cannot afford cudaMalloc's device
+ * synchronisation. No counterpart in the reference (it has no device).
+ *
+ * tris_dev and out_dev are device pointers owned by the caller: ntri triangles
+ * of 9 f64 (x0 y0 z0 x1 y1 z1 x2 y2 z2) and dims[0]*dims[1]*dims[2] f64 values
+ * (x fastest, 8-byte aligned). stream is a cudaStream_t (NULL = the default
+ * stream); the call returns after the work on it has finished.
+ *
+ * It calls no cudaMalloc/cudaFree: its scratch (the triangles padded to whole
+ * staging tiles, ~2.4 MB, plus an error word) is a static device array that
+ * every GPU loading this library holds until the process exits. Meshes with
+ * more than SDR_NOALLOC_MAX_TRIANGLES triangles return SDR_ERR_INVALID. The
+ * first call on a device looks up the scratch's device address; make that
+ * first call before any stream capture. All calls share the one scratch, so
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * must be serialised by the caller. */
+int sdr_sdf_from_mesh_noalloc(const double* tris_dev, size_t ntri, sdr_vec3 origin, double dx,
+                              const uint64_t dims[3], double* out_dev, void* stream);
+
 /* SinusParams, src/sinus.rs:26-45 (SI units). */
 typedef struct {
     sdr_vec3 semi_axes;

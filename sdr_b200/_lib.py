@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsdr_gpu.so")
 
 SDR_OK = 0
+NOALLOC_MAX_TRIANGLES = 32768
 ERRORS = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "CAPACITY", 5: "DEVICE_TIMEOUT", 6: "NO_DEVICE", 7: "BUFFER"}
 
 PHASE_EMIT, PHASE_CLASSIFY, PHASE_P2G, PHASE_ADD_FORCES = 0, 1, 2, 4
@@ -160,6 +161,7 @@ SIGNATURES = {
     "sdr_sdf_mesh_grid": (i32, [P(d), sz, d, d, P(Vec3), P(u64)]),
     "sdr_sdf_from_mesh": (i32, [P(d), sz, Vec3, d, P(u64), P(d)]),
     "sdr_sdf_from_sinus": (i32, [P(SinusParamsC), Vec3, d, P(u64), P(d)]),
+    "sdr_sdf_from_mesh_noalloc": (i32, [vp, sz, Vec3, d, P(u64), vp, vp]),
     "sdr_surface_nets_volume": (i32, [P(d), P(u64), Vec3, d, P(d), P(u64)]),
 }
 

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -819,6 +820,38 @@ void check_device() {
 
 }  // namespace
 
+// ---------------------------------------------------------------- no-allocation SDF build
+// Scratch of sdr_sdf_from_mesh_noalloc: the triangles padded to whole
+// bulk-copy tiles, followed by one error word. It is a file-scope device
+// array, so every GPU that loads this library holds it until exit, and every
+// call on a device shares it.
+namespace {
+constexpr size_t kNoAllocTris = ((size_t)SDR_NOALLOC_MAX_TRIANGLES + kSdfTile - 1) / kSdfTile * kSdfTile;
+constexpr size_t kNoAllocDoubles = kNoAllocTris * 9 + 2;
+}  // namespace
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[128] = {};
+
+// Device address of the scratch on the current device. In host code the
+// symbol is only a host-side stand-in, so the address is looked up once per
+// device with that device current, and cached.
+double* noalloc_scratch() {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) throw Fail{SDR_ERR_NO_DEVICE, "device ordinal out of range"};
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* ptr = nullptr;
+        CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    return static_cast<double*>(g_noalloc_ptr[dev]);
+}
+}  // namespace
+
 // ================================================================= C ABI
 extern "C" {
 
@@ -1455,6 +1488,35 @@ int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double d
             throw;
         }
         cleanup();
+    });
+}
+
+int sdr_sdf_from_mesh_noalloc(const double* tris_dev, size_t ntri, sdr_vec3 origin, double dx,
+                              const uint64_t dims[3], double* out_dev, void* stream) {
+    return guard([&] {
+        require(tris_dev && out_dev && dims && ntri && dx > 0, "bad argument");
+        if (ntri > (size_t)SDR_NOALLOC_MAX_TRIANGLES)
+            throw Fail{SDR_ERR_INVALID, "mesh has " + std::to_string(ntri) + " triangles; the no-allocation scratch holds " +
+                                            std::to_string(SDR_NOALLOC_MAX_TRIANGLES)};
+        require(((uintptr_t)out_dev & 7) == 0, "out_dev must be 8-byte aligned");
+        check_device();
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        double* tiles = noalloc_scratch();
+        uint32_t* err = reinterpret_cast<uint32_t*>(tiles + kNoAllocTris * 9);
+        uint32_t ntiles = (uint32_t)((ntri + kSdfTile - 1) / kSdfTile);
+        size_t used = ntri * 9, padded = (size_t)ntiles * kSdfTile * 9;
+        size_t nn = dims[0] * dims[1] * dims[2];
+        // The scratch keeps the previous call's contents: overwrite the
+        // triangles, zero the padding tail and the error word.
+        CK(cudaMemcpyAsync(tiles, tris_dev, used * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (padded > used) CK(cudaMemsetAsync(tiles + used, 0, (padded - used) * sizeof(double), st));
+        CK(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+        LAUNCH(k_sdf_mesh, blocks(nn, kSdfBS), kSdfBS, 0, st, tiles, (uint32_t)ntri, ntiles, origin.x, origin.y,
+               origin.z, dx, (int)dims[0], (int)dims[1], (int)dims[2], out_dev, err);
+        uint32_t e = 0;
+        CK(cudaMemcpyAsync(&e, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (e) throw Fail{SDR_ERR_DEVICE_TIMEOUT, "triangle staging wait gave up"};
     });
 }
 
