@@ -474,8 +474,10 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
                     }
                     double pc = a.precon[ps];
                     double qv = dmul(t, pc);
+                    double pqv = dmul(pc, qv);
                     a.q[ps] = qv;
-                    a.pq[ps] = dmul(pc, qv);
+                    a.pq[ps] = pqv;
+                    if (wcur <= kPcgBS) cur[ps - lsA] = pqv;  // the next level reads the window
                 }
             }
         }
@@ -571,6 +573,7 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
                     }
                     double zv = dmul(t, pc);
                     z[ps] = zv;
+                    if (wcur <= kPcgBS) cur[ps - lsA] = zv;  // the next level reads the window
                     double pr = dmul(zv, r[ps]);
                     if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
                     else zr = dadd(zr, pr);

@@ -114,6 +114,59 @@ def test_project_bit_exact_pressure(pair):
         assert errs[w] < FACE_TOL
 
 
+WIDE_TOML = """
+[sim]
+resolution_mm = 0.6
+duration_s = 0.5
+frames = 10
+[needle]
+auto = true
+diameter_mm = 0.8
+flow_rate_ml_s = 5.0
+"""
+
+
+def test_project_wide_levels_bit_exact():
+    """The parametric cavity filled with fluid at 0.6 mm: wavefront levels are
+    wider than the block's shared-memory window, so the sweeps take their
+    global-memory path for those levels (and the window path around them);
+    the pressure is still bit-exact with the reference dot order."""
+    gpu, orc, res = make_pair(WIDE_TOML)
+    (nx, ny, nz), origin, dx = orc.grid
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    pos = np.stack([origin[0] + (i + 0.5) * dx, origin[1] + (j + 0.5) * dx, origin[2] + (k + 0.5) * dx],
+                   axis=-1).reshape(-1, 3)
+    pos = f32(pos)
+    vel = np.zeros_like(pos)
+    gpu.set_particles(pos, vel)
+    orc.set_particles(pos, vel)
+    rng = np.random.default_rng(5)
+    for w in range(3):
+        f = f32(0.05 * rng.standard_normal(orc.face(w).shape))
+        gpu.set_face(w, f)
+        orc.set_face(w, f)
+    gpu.set_dot_order(True)
+    try:
+        gpu.run_phase(_lib.PHASE_CLASSIFY)
+        orc.phase(oracle.PHASE_CLASSIFY)
+        fluid = orc.cells().reshape(nz, ny, nx) == 1
+        widths = np.bincount((i + j + k)[fluid])
+        sync_faces(gpu, orc)
+        gpu.run_phase(_lib.PHASE_PROJECT, 1e-4)
+        orc.phase(oracle.PHASE_PROJECT, 1e-4)
+    finally:
+        gpu.set_dot_order(False)
+    pg, po = gpu.pressure(), orc.pressure()
+    it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
+    diff = int(np.sum(pg.view(np.uint64) != po.view(np.uint64)))
+    record("project_wide", {"fluid_cells": int(fluid.sum()), "max_level_width": int(widths.max()),
+                            "levels_over_736": int((widths > 736).sum()), "iters_gpu": it_g, "iters_orc": it_o,
+                            "pressure_bit_mismatch": diff})
+    assert widths.max() > 768
+    assert it_g == it_o
+    assert diff == 0
+
+
 PRESSURE_TOL = 1e-8  # block-tree dots: pressure relative to its max, f64
 
 
