@@ -86,8 +86,12 @@ typedef struct {
 typedef struct {
     uint64_t max_particles; /* device particle capacity (0 = derive from the cavity volume) */
     int32_t device;         /* CUDA device ordinal (-1 = current) */
-    int32_t reserved0;
+    int32_t flags;          /* SDR_SOLVER_* bits */
 } sdr_solver_options;
+
+/* The host thread sleeps while it waits for the solver's stream (instead of
+ * spinning): for many solvers driven by more host threads than cores. */
+#define SDR_SOLVER_BLOCKING_SYNC 1
 
 /* Solver's public scalar fields (src/solver.rs:143-167) plus GPU-side counters. */
 typedef struct {
@@ -312,6 +316,68 @@ int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx,
  * (src/surface_nets.rs:48-195, src/mesh.rs:63-70): the parametric cavity volume. */
 int sdr_surface_nets_volume(const double* values, const uint64_t dims[3], sdr_vec3 origin,
                             double dx, double* volume, uint64_t* triangles);
+
+/* ---------------------------------------------------------------- batches and serving
+ * Many independent scenes on one GPU. The reference runs one scene per
+ * process (main.rs:215-386: build the scene, Solver::step per frame,
+ * MetricsCollector::record, summary); these entry points run that same loop
+ * for many scenes at once, each scene on its own solver, CUDA stream and host
+ * thread, so the scenes' kernels (one SM per pressure solve) share the GPU.
+ * A scene's result does not depend on what runs beside it. */
+
+/* One scene: the solver set-up of Solver::new plus the run length and the
+ * cavity volume the metrics need (scene.rs:312). The SDF data is copied when
+ * the scene is handed over. */
+typedef struct {
+    sdr_sdf_desc sdf;
+    double sim_dx;
+    sdr_fluid_params fluid;
+    sdr_needle needle;
+    sdr_solve_params solve;
+    int32_t has_outlet;
+    int32_t reserved0;
+    sdr_aabb outlet;
+    double cavity_volume;   /* m^3 */
+    double frame_dt;        /* seconds per frame */
+    uint64_t frames;        /* frames to run */
+    uint64_t max_particles; /* device particle capacity (0 = derive from the dose) */
+} sdr_scene_desc;
+
+/* Device bytes a scene needs while it runs (grid, particle capacity, SDF,
+ * workspace): the admission estimate of the server. Host arithmetic only. */
+int sdr_scene_footprint(const sdr_scene_desc* scene, uint64_t* bytes);
+
+typedef struct sdr_batch sdr_batch;
+int sdr_batch_create(const sdr_scene_desc* scenes, size_t n, int32_t device, sdr_batch** out);
+/* Run every scene of the batch to its frame count with up to `concurrency`
+ * scenes in flight (0 = all; 1 = one after another, the plain path). Scene
+ * failures are reported per scene by sdr_batch_result; the call itself fails
+ * only for bad arguments. */
+int sdr_batch_run(sdr_batch* b, uint32_t concurrency);
+/* status: SDR_OK or the scene's error code (message in `error`, may be NULL). */
+int sdr_batch_result(const sdr_batch* b, size_t i, int32_t* status, sdr_summary* summary,
+                     sdr_solver_stats* stats_or_null, double* seconds_or_null, char* error, size_t error_cap);
+int sdr_batch_destroy(sdr_batch* b);
+
+/* A request loop: scenes submitted at any time are admitted in arrival order
+ * while their footprint fits the byte budget and a slot is free, run
+ * concurrently, and release their memory when their summary is ready. */
+typedef struct sdr_server sdr_server;
+enum { SDR_REQ_QUEUED = 0, SDR_REQ_RUNNING = 1, SDR_REQ_DONE = 2, SDR_REQ_FAILED = 3 };
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint32_t active, peak_active;
+    uint64_t bytes_in_use, peak_bytes;
+} sdr_server_stats;
+int sdr_server_create(int32_t device, uint64_t budget_bytes, uint32_t max_active, sdr_server** out);
+int sdr_server_submit(sdr_server* s, const sdr_scene_desc* scene, uint64_t* ticket);
+/* state: SDR_REQ_*. When done: the summary and the seconds from submission to
+ * summary (time-to-summary); when failed: the message in `error` (may be NULL). */
+int sdr_server_poll(sdr_server* s, uint64_t ticket, int32_t* state, sdr_summary* summary_or_null,
+                    double* seconds_or_null, char* error, size_t error_cap);
+int sdr_server_get_stats(sdr_server* s, sdr_server_stats* out);
+/* Waits for every admitted and queued request, then frees the server. */
+int sdr_server_destroy(sdr_server* s);
 
 #ifdef __cplusplus
 }

@@ -56,7 +56,10 @@ class SdfDesc(C.Structure):
 
 
 class SolverOptions(C.Structure):
-    _fields_ = [("max_particles", C.c_uint64), ("device", C.c_int32), ("reserved0", C.c_int32)]
+    _fields_ = [("max_particles", C.c_uint64), ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+SOLVER_BLOCKING_SYNC = 1
 
 
 class SolverStats(C.Structure):
@@ -117,6 +120,24 @@ class SinusParamsC(C.Structure):
                 ("socket_depth", C.c_double), ("model_dx", C.c_double)]
 
 
+class SceneDesc(C.Structure):
+    _fields_ = [("sdf", SdfDesc), ("sim_dx", C.c_double), ("fluid", FluidParamsC), ("needle", NeedleC),
+                ("solve", SolveParamsC), ("has_outlet", C.c_int32), ("reserved0", C.c_int32), ("outlet", Aabb),
+                ("cavity_volume", C.c_double), ("frame_dt", C.c_double), ("frames", C.c_uint64),
+                ("max_particles", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("active", C.c_uint32), ("peak_active", C.c_uint32), ("bytes_in_use", C.c_uint64),
+                ("peak_bytes", C.c_uint64)]
+
+    def to_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 P = C.POINTER
 d, u64, i32, vp, sz = C.c_double, C.c_uint64, C.c_int, C.c_void_p, C.c_size_t
 
@@ -163,6 +184,16 @@ SIGNATURES = {
     "sdr_sdf_from_sinus": (i32, [P(SinusParamsC), Vec3, d, P(u64), P(d)]),
     "sdr_sdf_from_mesh_noalloc": (i32, [vp, sz, Vec3, d, P(u64), vp, vp]),
     "sdr_surface_nets_volume": (i32, [P(d), P(u64), Vec3, d, P(d), P(u64)]),
+    "sdr_scene_footprint": (i32, [P(SceneDesc), P(u64)]),
+    "sdr_batch_create": (i32, [P(SceneDesc), sz, C.c_int32, P(vp)]),
+    "sdr_batch_run": (i32, [vp, C.c_uint32]),
+    "sdr_batch_result": (i32, [vp, sz, P(C.c_int32), P(SummaryC), P(SolverStats), P(d), C.c_char_p, sz]),
+    "sdr_batch_destroy": (i32, [vp]),
+    "sdr_server_create": (i32, [C.c_int32, u64, C.c_uint32, P(vp)]),
+    "sdr_server_submit": (i32, [vp, P(SceneDesc), P(u64)]),
+    "sdr_server_poll": (i32, [vp, u64, P(C.c_int32), P(SummaryC), P(d), C.c_char_p, sz]),
+    "sdr_server_get_stats": (i32, [vp, P(ServerStats)]),
+    "sdr_server_destroy": (i32, [vp]),
 }
 
 _lib = None

@@ -201,6 +201,7 @@ struct sdr_solver {
     bool sorted_valid = false;  // perm/start describe the current particle set
     // timing
     cudaEvent_t ev[10] = {};
+    cudaEvent_t ev_block = nullptr;  // blocking-sync event (SDR_SOLVER_BLOCKING_SYNC)
     bool profiling = false;
     bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
     sdr_profile prof{};
@@ -351,6 +352,8 @@ struct sdr_solver {
         hst = nullptr; h_epos = nullptr; h_evel = nullptr; h_mout = nullptr;
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (ev_block) cudaEventDestroy(ev_block);
+        ev_block = nullptr;
         if (st) cudaStreamDestroy(st);
         st = nullptr;
     }
@@ -634,7 +637,12 @@ struct sdr_solver {
 
     void sync_status() {
         CK(cudaMemcpyAsync(hst, dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        if (ev_block) {  // the waiting thread sleeps instead of spinning
+            CK(cudaEventRecord(ev_block, st));
+            CK(cudaEventSynchronize(ev_block));
+        } else {
+            CK(cudaStreamSynchronize(st));
+        }
         n = hst->n;
         drained = hst->drained;
         culled = hst->culled;
@@ -853,6 +861,10 @@ double* noalloc_scratch() {
 }  // namespace
 
 // ================================================================= C ABI
+// Library-internal (not part of the C ABI): lets the host-side batch and
+// serving layer report its own failures through sdr_last_error.
+void sdr_internal_set_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 int sdr_abi_version(void) { return SDR_ABI_VERSION; }
@@ -879,6 +891,8 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
                                                   std::to_string(prop.major) + std::to_string(prop.minor)};
             CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
             s->create_events();
+            if (options && (options->flags & SDR_SOLVER_BLOCKING_SYNC))
+                CK(cudaEventCreateWithFlags(&s->ev_block, cudaEventBlockingSync | cudaEventDisableTiming));
             CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmem));
             CK(cudaFuncSetAttribute(k_redist_replay, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRedistSmem));
             s->fluid = *fluid;

@@ -6,6 +6,9 @@ real_cavity       seeded perturbed-ellipsoid cavity (2.2 ml, ~20k triangles, SH 
                   settling, 18 frames (the real-cavity shape stood in for by synthetic input)
 large_parametric  the parametric sinus at 0.2 mm (207x217x161 cells), 6 ml/s for 0.3 s then
                   0.3 s settling, PCG capped at 400 iterations
+batch_scene(seed) one scene of the batched / served family: a seeded perturbed ellipsoid of
+                  U[1.5, 3] ml, grid cells log-uniform in [32^3, 96^3], needle tilt U[-30, 30] deg,
+                  flow U[1, 8] ml/s, dose U[0.5, 2] ml, 0.6 s in 18 frames
 """
 from __future__ import annotations
 
@@ -62,6 +65,46 @@ def real_cavity(seed: int = 2, tilt_deg: float = 0.0, flow_ml_s: float = 4.0, do
                                         f"{volume_ml} ml, SH degree 1-4 noise 15%",
                               "dx_mm": dx_mm, "flow_ml_s": flow_ml_s, "dose_ml": dose_ml,
                               "duration_s": duration_s, "tilt_deg": tilt_deg})
+
+
+def batch_scene(seed: int, frames: Optional[int] = None) -> Workload:
+    """One scene of the batched family, every choice drawn from SplitMix64(seed).
+
+    The cell size follows from the target cell count over the cavity's
+    bounding box: dx = (bbox volume / N)^(1/3). ``frames`` shortens the run
+    (the frame length stays 0.6 s / 18)."""
+    from .cavity import SplitMix64
+    rng = SplitMix64(0x5CE7E000 + seed)
+    volume_ml = rng.uniform(1.5, 3.0)
+    cells = math.exp(rng.uniform(math.log(32.0 ** 3), math.log(96.0 ** 3)))
+    tilt = rng.uniform(-30.0, 30.0)
+    flow = rng.uniform(1.0, 8.0)
+    dose = rng.uniform(0.5, 2.0)
+    cav = perturbed_ellipsoid(seed, volume_ml=volume_ml, tilt_deg=tilt)
+    pts = cav.tris.reshape(-1, 3)
+    ext = pts.max(axis=0) - pts.min(axis=0)
+    dx = float((ext[0] * ext[1] * ext[2] / cells) ** (1.0 / 3.0))
+    fluid = sc.FluidParams(density=1000.0, gravity=(0.0, -9.81, 0.0), flip_ratio=0.7, particles_per_cell=8,
+                           volume_stiffness=1.0, redistribute=True, redist_cap_factor=1.0)
+    needle = sc.Needle(tip=cav.tip, axis=cav.axis, radius=0.5 * 0.8 * sc.MM, flow_rate=flow * sc.ML_PER_S,
+                       inject_until=dose / flow)
+    total = 18
+    res = sc.ResolvedScene(sim_dx=dx, fluid=fluid, needle=needle, outlet=None, solve=sc.SolveParams(200, 1e-6),
+                           frames=total if frames is None else int(frames), frame_dt=0.6 / total, sinus=None,
+                           mesh_path=None, sdf_dx=dx, mesh_padding=3.0 * dx)
+    return Workload(f"batch_scene_{seed}", res, tris=cav.tris, cavity_volume=abs(cav.volume),
+                    describe={"seed": seed, "volume_ml": volume_ml, "target_cells": cells, "dx_mm": dx * 1e3,
+                              "tilt_deg": tilt, "flow_ml_s": flow, "dose_ml": dose})
+
+
+def scene_spec(w: Workload):
+    """The batched-run description of a workload (its SDF voxelised on the device)."""
+    from .serving import SceneSpec
+    from .solver import build_sdf, cavity_volume
+    sdf = build_sdf(w.res, w.tris)
+    vol = w.cavity_volume if w.cavity_volume is not None else cavity_volume(w.res, sdf, w.tris)
+    return SceneSpec(sdf=sdf, sim_dx=w.res.sim_dx, fluid=w.res.fluid, needle=w.res.needle, solve=w.res.solve,
+                     cavity_volume=vol, frame_dt=w.res.frame_dt, frames=w.res.frames, outlet=w.res.outlet)
 
 
 WORKLOADS = {"plain_parametric": plain_parametric, "real_cavity": real_cavity, "large_parametric": large_parametric}

@@ -1,0 +1,89 @@
+"""Many scenes on one GPU: every scene's result is the same alone, one after
+another, and in a concurrent mix (batch or server), and equals the plain
+single-solver path. Scenes are small (the smoke sinus at 2 mm, 2 frames)."""
+import numpy as np
+import pytest
+
+from sdr_b200 import _lib, scene as sc
+from sdr_b200.serving import SceneSpec, Server, footprint, run_batch
+from tests.gpu_common import SMOKE_TOML, record
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("frames", "final_time_s", "peak_fill_fraction", "final_fill_fraction", "peak_wall_coverage",
+          "final_wall_coverage", "peak_membrane_pressure_pa", "mean_membrane_pressure_pa", "peak_pressure_pa",
+          "membrane_artifacts_total", "total_drained_ml", "injected_ml", "mass_balance")
+
+
+def _specs(flows=(3.0, 5.0, 7.0), frames=2):
+    from sdr_b200.solver import build_sdf, cavity_volume
+    base = sc.SceneConfig.from_toml_str(SMOKE_TOML).resolve()
+    sdf = build_sdf(base)
+    vol = cavity_volume(base, sdf)
+    out = []
+    for f in flows:
+        n = base.needle
+        needle = sc.Needle(tip=n.tip, axis=n.axis, radius=n.radius, flow_rate=f * sc.ML_PER_S,
+                           inject_until=n.inject_until)
+        out.append(SceneSpec(sdf=sdf, sim_dx=base.sim_dx, fluid=base.fluid, needle=needle, solve=base.solve,
+                             cavity_volume=vol, frame_dt=base.frame_dt, frames=frames, outlet=base.outlet))
+    return out
+
+
+def _same(a: dict, b: dict):
+    for k in FIELDS:
+        assert a[k] == b[k], (k, a[k], b[k])
+
+
+def _plain(spec: SceneSpec) -> dict:
+    """The single-scene API path: Solver + MetricsCollector, frame by frame."""
+    from sdr_b200.solver import MetricsCollector, Solver
+    s = Solver(spec.sdf, spec.sim_dx, spec.fluid, spec.needle)
+    s.solve = spec.solve
+    s.outlet = spec.outlet
+    m = MetricsCollector(s, spec.cavity_volume)
+    for f in range(spec.frames):
+        s.step(spec.frame_dt)
+        m.record(s, f)
+    return m.summary()
+
+
+def test_batch_same_alone_sequential_and_concurrent():
+    specs = _specs()
+    seq = run_batch(specs, concurrency=1)
+    mix = run_batch(specs, concurrency=0)
+    assert all(r.status == _lib.SDR_OK for r in seq + mix), [r.error for r in seq + mix]
+    for a, b in zip(seq, mix):
+        _same(a.summary, b.summary)
+        assert a.stats["particles"] == b.stats["particles"] and a.stats["steps"] == b.stats["steps"]
+    alone = _plain(specs[1])
+    _same(alone, mix[1].summary)
+    record("batch", {"seconds_sequential": sum(r.seconds for r in seq), "seconds_each_in_mix": [r.seconds for r in mix],
+                     "fill": [r.summary["final_fill_fraction"] for r in mix]})
+
+
+def test_server_continuous_batching_matches_batch():
+    specs = _specs(flows=(2.0, 3.0, 4.0, 5.0, 6.0))
+    ref = run_batch(specs, concurrency=1)
+    with Server(budget_bytes=64 << 30, max_active=2) as srv:
+        tickets = [srv.submit(s) for s in specs[:3]]
+        more = [srv.submit(s) for s in specs[3:]]  # arrive while the first ones run
+        res = srv.wait(tickets + more, timeout=600)
+        st = srv.stats()
+    assert all(r.status == _lib.REQ_DONE for r in res), [r.error for r in res]
+    for a, b in zip(ref, res):
+        _same(a.summary, b.summary)
+        assert b.seconds > 0.0
+    assert st["completed"] == 5 and st["failed"] == 0 and 1 <= st["peak_active"] <= 2
+    assert st["active"] == 0 and st["bytes_in_use"] == 0
+    record("server", {"stats": st, "time_to_summary": [r.seconds for r in res]})
+
+
+def test_server_budget_admits_one_at_a_time():
+    specs = _specs(flows=(3.0, 6.0))
+    fp = max(footprint(s) for s in specs)
+    with Server(budget_bytes=int(fp * 1.5), max_active=4) as srv:
+        res = srv.wait([srv.submit(s) for s in specs], timeout=600)
+        st = srv.stats()
+    assert all(r.status == _lib.REQ_DONE for r in res)
+    assert st["peak_active"] == 1 and st["peak_bytes"] <= int(fp * 1.5)
