@@ -37,7 +37,8 @@ enum {
     SDR_ERR_CAPACITY = 4,       /* particle or work-list capacity exceeded */
     SDR_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
     SDR_ERR_NO_DEVICE = 6,      /* no CUDA device or the library was built for another arch */
-    SDR_ERR_BUFFER = 7          /* caller buffer too small; required size reported */
+    SDR_ERR_BUFFER = 7,         /* caller buffer too small; required size reported */
+    SDR_ERR_IO = 8              /* a file could not be created or written */
 };
 
 /* Cell labels (src/pressure.rs:24-32). */
@@ -201,7 +202,9 @@ int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
  * block-tree order — deterministic run to run, faster, differing from the
  * reference in the last bits of each dot. */
 int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
-/* Phase-group timing with CUDA events (adds one event record per group). */
+/* Phase-group timing with CUDA events (adds one event record per group):
+ * on = 1. on = 2 also turns on the section timers inside the pressure-solve
+ * kernel (pcg_section_cycles), which cost a little on its critical path. */
 int sdr_solver_set_profiling(sdr_solver* s, int on);
 int sdr_solver_get_profile(const sdr_solver* s, sdr_profile* out);
 int sdr_solver_reset_profile(sdr_solver* s);
@@ -316,6 +319,31 @@ int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx,
  * (src/surface_nets.rs:48-195, src/mesh.rs:63-70): the parametric cavity volume. */
 int sdr_surface_nets_volume(const double* values, const uint64_t dims[3], sdr_vec3 origin,
                             double dx, double* volume, uint64_t* triangles);
+
+/* ---------------------------------------------------------------- frame output */
+/* Particle files of src/output.rs: SDR_FORMAT_VTK is write_points_vtk
+ * (output.rs:23-48, ASCII legacy VTK, numbers as Rust prints f64),
+ * SDR_FORMAT_XYZ is write_points_xyz (output.rs:98-110, raw little-endian f32
+ * triples). */
+enum { SDR_FORMAT_VTK = 0, SDR_FORMAT_XYZ = 1 };
+/* n points from host memory, xyz interleaved. */
+int sdr_write_points(const char* path, int32_t format, const float* xyz, size_t n);
+/* frame_path (output.rs:114-122): "<dir>/<prefix>_<frame, 6 digits>.<vtk|xyz>". */
+int sdr_frame_path(const char* dir, const char* prefix, uint64_t frame, int32_t format, char* out, size_t cap);
+
+/* The per-frame output of cmd_simulate (main.rs:255-266) without stopping the
+ * solver: submit copies the current positions to one of two pinned host
+ * buffers on the solver's stream and returns; a writer thread waits for that
+ * copy and writes frame_path(dir, prefix, frame, format) while the next frames
+ * run. A third submit waits for the older buffer's file to be written. The
+ * directory must exist. Write errors are reported by the next submit, flush
+ * or destroy. */
+typedef struct sdr_frame_writer sdr_frame_writer;
+int sdr_frame_writer_create(const char* dir, const char* prefix, int32_t format, sdr_frame_writer** out);
+int sdr_frame_writer_submit(sdr_frame_writer* w, sdr_solver* s, uint64_t frame);
+/* Waits until every submitted frame is on disk. */
+int sdr_frame_writer_flush(sdr_frame_writer* w);
+int sdr_frame_writer_destroy(sdr_frame_writer* w);
 
 /* ---------------------------------------------------------------- batches and serving
  * Many independent scenes on one GPU. The reference runs one scene per

@@ -137,6 +137,7 @@ class ServerStats(C.Structure):
 
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+FORMAT_VTK, FORMAT_XYZ = 0, 1
 
 P = C.POINTER
 d, u64, i32, vp, sz = C.c_double, C.c_uint64, C.c_int, C.c_void_p, C.c_size_t
@@ -184,6 +185,12 @@ SIGNATURES = {
     "sdr_sdf_from_sinus": (i32, [P(SinusParamsC), Vec3, d, P(u64), P(d)]),
     "sdr_sdf_from_mesh_noalloc": (i32, [vp, sz, Vec3, d, P(u64), vp, vp]),
     "sdr_surface_nets_volume": (i32, [P(d), P(u64), Vec3, d, P(d), P(u64)]),
+    "sdr_write_points": (i32, [C.c_char_p, C.c_int32, P(C.c_float), sz]),
+    "sdr_frame_path": (i32, [C.c_char_p, C.c_char_p, u64, C.c_int32, C.c_char_p, sz]),
+    "sdr_frame_writer_create": (i32, [C.c_char_p, C.c_char_p, C.c_int32, P(vp)]),
+    "sdr_frame_writer_submit": (i32, [vp, vp, u64]),
+    "sdr_frame_writer_flush": (i32, [vp]),
+    "sdr_frame_writer_destroy": (i32, [vp]),
     "sdr_scene_footprint": (i32, [P(SceneDesc), P(u64)]),
     "sdr_batch_create": (i32, [P(SceneDesc), sz, C.c_int32, P(vp)]),
     "sdr_batch_run": (i32, [vp, C.c_uint32]),

@@ -14,7 +14,11 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <condition_variable>
+#include <deque>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <string>
 #include <vector>
@@ -203,6 +207,7 @@ struct sdr_solver {
     cudaEvent_t ev[10] = {};
     cudaEvent_t ev_block = nullptr;  // blocking-sync event (SDR_SOLVER_BLOCKING_SYNC)
     bool profiling = false;
+    bool kernel_timers = false;  // profiling level 2: section timers inside k_pcg
     bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
     sdr_profile prof{};
     uint64_t particle_substeps = 0, substeps_total = 0;
@@ -523,7 +528,7 @@ struct sdr_solver {
         a.p_dense = p_dense;
         a.out_iters = &dst->iters;
         a.out_residual = &dst->residual;
-        a.timing = profiling ? dst->pcg_cycles : nullptr;
+        a.timing = kernel_timers ? dst->pcg_cycles : nullptr;
         a.exact_dots = exact_dots ? 1 : 0;
         LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
     }
@@ -1042,6 +1047,7 @@ int sdr_solver_set_profiling(sdr_solver* s, int on) {
     return guard([&] {
         require(s, "null solver");
         s->profiling = on != 0;
+        s->kernel_timers = on >= 2;
     });
 }
 
@@ -1559,6 +1565,154 @@ int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx, co
         cudaFree(dout);
         cudaStreamDestroy(st);
     });
+}
+
+}  // extern "C"
+
+// ================================================================= frame writer
+// Double-buffered per-frame particle output (see sdr_frame_writer_* in the
+// header): the D2H copy is queued on the solver's stream, the file is written
+// by a thread once the copy's event fires.
+int sdr_internal_write_points(const char* path, int32_t format, const float* xyz, size_t stride, size_t n,
+                              std::string& err);
+std::string sdr_internal_frame_path(const char* dir, const char* prefix, uint64_t frame, int32_t format);
+
+struct sdr_frame_writer {
+    std::string dir, prefix;
+    int32_t format = SDR_FORMAT_VTK;
+    float4* host[2] = {nullptr, nullptr};  // pinned
+    size_t cap[2] = {0, 0};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int ev_device[2] = {-1, -1};
+    size_t count[2] = {0, 0};
+    uint64_t frame[2] = {0, 0};
+    bool busy[2] = {false, false};  // submitted and not yet written
+    int next = 0;
+    std::deque<int> ready;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread th;
+    bool stop = false;
+    int err_code = SDR_OK;
+    std::string err;
+
+    void loop() {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv.wait(lk, [&] { return stop || !ready.empty(); });
+            if (ready.empty()) return;  // stopping and drained
+            const int slot = ready.front();
+            ready.pop_front();
+            lk.unlock();
+            int rc = SDR_OK;
+            std::string msg;
+            if (ev_device[slot] >= 0) cudaSetDevice(ev_device[slot]);
+            cudaError_t e = cudaEventSynchronize(ev[slot]);
+            if (e != cudaSuccess) {
+                rc = SDR_ERR_CUDA;
+                msg = std::string("frame copy: ") + cudaGetErrorString(e);
+            } else {
+                std::string path = sdr_internal_frame_path(dir.c_str(), prefix.c_str(), frame[slot], format);
+                rc = sdr_internal_write_points(path.c_str(), format, reinterpret_cast<const float*>(host[slot]), 4,
+                                               count[slot], msg);
+            }
+            lk.lock();
+            if (rc != SDR_OK && err_code == SDR_OK) {
+                err_code = rc;
+                err = msg;
+            }
+            busy[slot] = false;
+            cv.notify_all();
+        }
+    }
+};
+
+extern "C" {
+
+int sdr_frame_writer_create(const char* dir, const char* prefix, int32_t format, sdr_frame_writer** out) {
+    return guard([&] {
+        require(dir && prefix && out, "null argument");
+        require(format == SDR_FORMAT_VTK || format == SDR_FORMAT_XYZ, "unknown output format");
+        *out = nullptr;
+        auto w = std::make_unique<sdr_frame_writer>();
+        w->dir = dir;
+        w->prefix = prefix;
+        w->format = format;
+        w->th = std::thread([p = w.get()] { p->loop(); });
+        *out = w.release();
+    });
+}
+
+int sdr_frame_writer_submit(sdr_frame_writer* w, sdr_solver* s, uint64_t frame) {
+    return guard([&] {
+        require(w && s, "null argument");
+        DeviceScope ds(s->device);
+        std::unique_lock<std::mutex> lk(w->mu);
+        if (w->err_code != SDR_OK) throw Fail{w->err_code, w->err};
+        const int slot = w->next;
+        w->cv.wait(lk, [&] { return !w->busy[slot]; });  // its previous file is written
+        if (w->err_code != SDR_OK) throw Fail{w->err_code, w->err};
+        w->busy[slot] = true;
+        lk.unlock();
+        try {
+            const size_t n = s->n;
+            if (n > w->cap[slot]) {
+                if (w->host[slot]) cudaFreeHost(w->host[slot]);
+                w->host[slot] = nullptr;
+                w->cap[slot] = 0;
+                size_t c = std::max<size_t>(n + n / 2, 4096);
+                CK(cudaMallocHost((void**)&w->host[slot], c * sizeof(float4)));
+                w->cap[slot] = c;
+            }
+            if (!w->ev[slot] || w->ev_device[slot] != s->device) {
+                if (w->ev[slot]) cudaEventDestroy(w->ev[slot]);
+                w->ev[slot] = nullptr;
+                CK(cudaEventCreateWithFlags(&w->ev[slot], cudaEventDisableTiming));
+                w->ev_device[slot] = s->device;
+            }
+            if (n) CK(cudaMemcpyAsync(w->host[slot], s->pos, n * sizeof(float4), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaEventRecord(w->ev[slot], s->st));
+        } catch (...) {
+            lk.lock();
+            w->busy[slot] = false;
+            w->cv.notify_all();
+            throw;
+        }
+        lk.lock();
+        w->count[slot] = s->n;
+        w->frame[slot] = frame;
+        w->ready.push_back(slot);
+        w->next ^= 1;
+        w->cv.notify_all();
+    });
+}
+
+int sdr_frame_writer_flush(sdr_frame_writer* w) {
+    return guard([&] {
+        require(w, "null writer");
+        std::unique_lock<std::mutex> lk(w->mu);
+        w->cv.wait(lk, [&] { return !w->busy[0] && !w->busy[1]; });
+        if (w->err_code != SDR_OK) throw Fail{w->err_code, w->err};
+    });
+}
+
+int sdr_frame_writer_destroy(sdr_frame_writer* w) {
+    if (!w) return SDR_OK;
+    {
+        std::lock_guard<std::mutex> lk(w->mu);
+        w->stop = true;
+    }
+    w->cv.notify_all();
+    if (w->th.joinable()) w->th.join();
+    const int rc = w->err_code;
+    const std::string msg = w->err;
+    for (int i = 0; i < 2; ++i) {
+        if (w->host[i]) cudaFreeHost(w->host[i]);
+        if (w->ev[i]) cudaEventDestroy(w->ev[i]);
+    }
+    delete w;
+    if (rc != SDR_OK) g_err = msg;
+    return rc;
 }
 
 }  // extern "C"
