@@ -61,16 +61,116 @@ struct Fail {
 
 inline unsigned blocks(size_t n, unsigned bs) { return (unsigned)std::max<size_t>(1, (n + bs - 1) / bs); }
 
+// Solver-owned device buffers come from one library memory pool per device,
+// allocated and released in the order of the owning solver's stream
+// (cudaMallocFromPoolAsync / cudaFreeAsync). Unlike cudaMalloc/cudaFree this
+// neither synchronises the device nor takes the driver's allocation lock for
+// long, so one scene's set-up, growth or teardown does not stall the scenes
+// running beside it; a freed block is reused by the next scene without a
+// round trip to the driver. The pool keeps up to a quarter of device memory
+// cached between scenes and returns the rest at synchronisation points.
+cudaMemPool_t device_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Fail{SDR_ERR_CUDA, "device index out of range"};
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        CK(cudaMemPoolCreate(&pool, &props));
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        uint64_t keep = total_b / 4;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
+// Without a stream (one-shot entry points) these are plain cudaMalloc/cudaFree.
 template <class T>
-void dalloc(T*& p, size_t n) {
-    if (p) cudaFree(p);
+void dalloc(T*& p, size_t n, cudaStream_t s = nullptr) {
+    if (p) {
+        if (s) cudaFreeAsync(p, s);
+        else cudaFree(p);
+    }
     p = nullptr;
-    CK(cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)));
+    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    if (s) CK(cudaMallocFromPoolAsync((void**)&p, bytes, device_pool(), s));
+    else CK(cudaMalloc((void**)&p, bytes));
 }
 
 template <class T>
-void dfree(T*& p) {
-    if (p) cudaFree(p);
+void dfree(T*& p, cudaStream_t s = nullptr) {
+    if (p) {
+        if (s) cudaFreeAsync(p, s);
+        else cudaFree(p);
+    }
+    p = nullptr;
+}
+
+// Pinned host blocks (status words, emission staging, frame buffers) come
+// from a process-wide cache of power-of-two blocks: cudaFreeHost synchronises
+// the device, so a block is never handed back to the driver, only to the
+// cache, which is bounded by the peak number of blocks in use at once.
+class PinnedCache {
+   public:
+    static void* get(size_t bytes, size_t* granted = nullptr) {
+        int cls = size_class(bytes);
+        size_t size = (size_t)1 << cls;
+        if (granted) *granted = size;
+        {
+            std::lock_guard<std::mutex> lk(mu());
+            auto& fl = lists()[cls];
+            if (!fl.empty()) {
+                void* p = fl.back();
+                fl.pop_back();
+                return p;
+            }
+        }
+        void* p = nullptr;
+        CK(cudaMallocHost(&p, size));
+        return p;
+    }
+    static void put(void* p, size_t bytes) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu());
+        lists()[size_class(bytes)].push_back(p);
+    }
+
+   private:
+    static int size_class(size_t bytes) {
+        int c = 8;  // 256-byte minimum
+        while (((size_t)1 << c) < bytes) ++c;
+        return c;
+    }
+    static std::mutex& mu() {
+        static std::mutex m;
+        return m;
+    }
+    static std::vector<void*>* lists() {
+        static std::vector<void*> l[64];
+        return l;
+    }
+};
+
+template <class T>
+void hget(T*& p, size_t n, size_t* granted_elems = nullptr) {
+    size_t g = 0;
+    p = static_cast<T*>(PinnedCache::get(std::max<size_t>(n, 1) * sizeof(T), &g));
+    if (granted_elems) *granted_elems = g / sizeof(T);
+}
+
+// `n` must be the element count the block was requested (or granted) with.
+template <class T>
+void hput(T*& p, size_t n) {
+    PinnedCache::put(p, std::max<size_t>(n, 1) * sizeof(T));
     p = nullptr;
 }
 
@@ -141,6 +241,7 @@ inline V3 vnorm0(V3 a) {  // math.rs:73-80
 struct sdr_solver {
     int device = 0;
     cudaStream_t st = nullptr;
+    std::vector<sdr_metrics*> collectors;  // live metrics collectors of this solver
     Grid g{};
     size_t ncell = 0, nu = 0, nv = 0, nw = 0;
     int snx = 0, sny = 0, snz = 0;
@@ -247,7 +348,7 @@ struct sdr_solver {
         }
         uint32_t nt = (uint32_t)((n_ + kScanTile - 1) / kScanTile);
         if (nt > tsum_cap) {
-            dalloc(tsum, nt);
+            dalloc(tsum, nt, st);
             tsum_cap = nt;
         }
         LAUNCH(k_scan_tiles, nt, kScanBS, 0, st, in, (uint32_t)n_, tsum);
@@ -258,103 +359,103 @@ struct sdr_solver {
     void ensure_capacity(size_t need) {
         if (need <= cap) return;
         size_t ncap = std::max(need + need / 2, cap + cap / 2);
-        ncap = std::max<size_t>(ncap, 1 << 16);
-        CK(cudaStreamSynchronize(st));
+        ncap = std::max<size_t>(ncap, 256);
+        // Stream-ordered: the copies run after every queued use of the old
+        // arrays and the old arrays are released after the copies.
         float4 *np = nullptr, *nv_ = nullptr;
-        CK(cudaMalloc((void**)&np, ncap * sizeof(float4)));
-        CK(cudaMalloc((void**)&nv_, ncap * sizeof(float4)));
+        dalloc(np, ncap, st);
+        dalloc(nv_, ncap, st);
         if (n) {
             CK(cudaMemcpyAsync(np, pos, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(nv_, vel, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
-            CK(cudaStreamSynchronize(st));
         }
-        dfree(pos);
-        dfree(vel);
+        dfree(pos, st);
+        dfree(vel, st);
         pos = np;
         vel = nv_;
-        dalloc(pos2, ncap);
-        dalloc(vel2, ncap);
-        dalloc(key_cell, ncap);
-        dalloc(key_sort, ncap);
-        dalloc(perm, ncap);
-        dalloc(ptmp, ncap);
-        dalloc(flag, ncap + 1);
-        dalloc(off, ncap + 1);
-        dalloc(drn, ncap);
-        dalloc(cand, ncap);
-        dalloc(moves, ncap * 2);
-        dalloc(lrec, ncap);
-        dalloc(vrec, ncap);
+        dalloc(pos2, ncap, st);
+        dalloc(vel2, ncap, st);
+        dalloc(key_cell, ncap, st);
+        dalloc(key_sort, ncap, st);
+        dalloc(perm, ncap, st);
+        dalloc(ptmp, ncap, st);
+        dalloc(flag, ncap + 1, st);
+        dalloc(off, ncap + 1, st);
+        dalloc(drn, ncap, st);
+        dalloc(cand, ncap, st);
+        dalloc(moves, ncap * 2, st);
+        dalloc(lrec, ncap, st);
+        dalloc(vrec, ncap, st);
         cap = ncap;
         sorted_valid = false;
     }
 
     void alloc_grid() {
         size_t nc = ncell;
-        dalloc(u, nu); dalloc(v, nv); dalloc(w, nw);
-        dalloc(su, nu); dalloc(sv, nv); dalloc(sw, nw);
-        dalloc(u2, nu); dalloc(v2, nv); dalloc(w2, nw);
-        dalloc(ku, nu); dalloc(kv, nv); dalloc(kw, nw);
-        dalloc(ku2, nu); dalloc(kv2, nv); dalloc(kw2, nw);
+        dalloc(u, nu, st); dalloc(v, nv, st); dalloc(w, nw, st);
+        dalloc(su, nu, st); dalloc(sv, nv, st); dalloc(sw, nw, st);
+        dalloc(u2, nu, st); dalloc(v2, nv, st); dalloc(w2, nw, st);
+        dalloc(ku, nu, st); dalloc(kv, nv, st); dalloc(kw, nw, st);
+        dalloc(ku2, nu, st); dalloc(kv2, nv, st); dalloc(kw2, nw, st);
         CK(cudaMemsetAsync(u, 0, nu * 4, st));
         CK(cudaMemsetAsync(v, 0, nv * 4, st));
         CK(cudaMemsetAsync(w, 0, nw * 4, st));
         CK(cudaMemsetAsync(su, 0, nu * 4, st));
         CK(cudaMemsetAsync(sv, 0, nv * 4, st));
         CK(cudaMemsetAsync(sw, 0, nw * 4, st));
-        dalloc(cells, nc); dalloc(base, nc); dalloc(cavity, nc);
+        dalloc(cells, nc, st); dalloc(base, nc, st); dalloc(cavity, nc, st);
         CK(cudaMemsetAsync(cells, AIR, nc, st));
-        dalloc(hist_valid, nc + 1);
-        dalloc(hist_sort, nc + 1);
-        dalloc(start, nc + 1);
-        dalloc(fill, nc + 1);
-        dalloc(long_list, nc);
+        dalloc(hist_valid, nc + 1, st);
+        dalloc(hist_sort, nc + 1, st);
+        dalloc(start, nc + 1, st);
+        dalloc(fill, nc + 1, st);
+        dalloc(long_list, nc, st);
         nlevels = g.nx + g.ny + g.nz - 2;
         nchunks = (int)((nc + kDotChunk - 1) / kDotChunk);
-        dalloc(lines_cnt, (size_t)nlevels * g.nz + 1);
-        dalloc(level_start, nlevels + 1);
-        dalloc(pos_of_cell, nc);
-        dalloc(lv_cell, nc);
-        dalloc(nbr, nc * 6);
-        dalloc(diag, nc);
-        dalloc(nmask, nc);
-        dalloc(b, nc); dalloc(precon, nc); dalloc(p, nc); dalloc(r, nc); dalloc(z, nc);
-        dalloc(s, nc); dalloc(as, nc); dalloc(q, nc); dalloc(pq, nc);
-        dalloc(partials, nchunks + 1);
-        dalloc(corder, nc);
-        dalloc(cinv, nc);
-        dalloc(prod, nc);
-        dalloc(frec, nc);
-        dalloc(brec, nc);
-        dalloc(chunk_start, nchunks + 1);
-        dalloc(cflag, nc);
-        dalloc(coff, nc);
-        dalloc(p_dense, nc);
+        dalloc(lines_cnt, (size_t)nlevels * g.nz + 1, st);
+        dalloc(level_start, nlevels + 1, st);
+        dalloc(pos_of_cell, nc, st);
+        dalloc(lv_cell, nc, st);
+        dalloc(nbr, nc * 6, st);
+        dalloc(diag, nc, st);
+        dalloc(nmask, nc, st);
+        dalloc(b, nc, st); dalloc(precon, nc, st); dalloc(p, nc, st); dalloc(r, nc, st); dalloc(z, nc, st);
+        dalloc(s, nc, st); dalloc(as, nc, st); dalloc(q, nc, st); dalloc(pq, nc, st);
+        dalloc(partials, nchunks + 1, st);
+        dalloc(corder, nc, st);
+        dalloc(cinv, nc, st);
+        dalloc(prod, nc, st);
+        dalloc(frec, nc, st);
+        dalloc(brec, nc, st);
+        dalloc(chunk_start, nchunks + 1, st);
+        dalloc(cflag, nc, st);
+        dalloc(coff, nc, st);
+        dalloc(p_dense, nc, st);
         CK(cudaMemsetAsync(p_dense, 0, nc * 8, st));
-        dalloc(mcell, blocks(nc, kMetBS));
-        dalloc(mout, 1);
+        dalloc(mcell, blocks(nc, kMetBS), st);
+        dalloc(mout, 1, st);
     }
 
     void free_all() {
-        dfree(sdf64); dfree(sdf32);
-        dfree(u); dfree(v); dfree(w); dfree(su); dfree(sv); dfree(sw); dfree(u2); dfree(v2); dfree(w2);
-        dfree(ku); dfree(kv); dfree(kw); dfree(ku2); dfree(kv2); dfree(kw2);
-        dfree(cells); dfree(base); dfree(cavity);
-        dfree(pos); dfree(vel); dfree(pos2); dfree(vel2);
-        dfree(key_cell); dfree(key_sort); dfree(perm); dfree(ptmp); dfree(flag); dfree(off); dfree(drn);
-        dfree(hist_valid); dfree(hist_sort); dfree(start); dfree(fill); dfree(long_list); dfree(tsum);
-        dfree(dst);
-        dfree(lines_cnt); dfree(lv_cell); dfree(cflag); dfree(coff); dfree(level_start); dfree(pos_of_cell);
-        dfree(nbr); dfree(corder); dfree(cinv); dfree(prod); dfree(frec); dfree(brec); dfree(chunk_start); dfree(diag); dfree(nmask);
-        dfree(b); dfree(precon); dfree(p); dfree(r); dfree(z); dfree(s); dfree(as); dfree(q); dfree(pq);
-        dfree(partials); dfree(p_dense);
-        dfree(cand); dfree(moves); dfree(rds); dfree(lrec); dfree(vrec);
-        dfree(mcell); dfree(mpart); dfree(mout);
-        if (hst) cudaFreeHost(hst);
-        if (h_epos) cudaFreeHost(h_epos);
-        if (h_evel) cudaFreeHost(h_evel);
-        if (h_mout) cudaFreeHost(h_mout);
-        hst = nullptr; h_epos = nullptr; h_evel = nullptr; h_mout = nullptr;
+        dfree(sdf64, st); dfree(sdf32, st);
+        dfree(u, st); dfree(v, st); dfree(w, st); dfree(su, st); dfree(sv, st); dfree(sw, st); dfree(u2, st); dfree(v2, st); dfree(w2, st);
+        dfree(ku, st); dfree(kv, st); dfree(kw, st); dfree(ku2, st); dfree(kv2, st); dfree(kw2, st);
+        dfree(cells, st); dfree(base, st); dfree(cavity, st);
+        dfree(pos, st); dfree(vel, st); dfree(pos2, st); dfree(vel2, st);
+        dfree(key_cell, st); dfree(key_sort, st); dfree(perm, st); dfree(ptmp, st); dfree(flag, st); dfree(off, st); dfree(drn, st);
+        dfree(hist_valid, st); dfree(hist_sort, st); dfree(start, st); dfree(fill, st); dfree(long_list, st); dfree(tsum, st);
+        dfree(dst, st);
+        dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
+        dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
+        dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
+        dfree(partials, st); dfree(p_dense, st);
+        dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
+        dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
+        if (hst) hput(hst, 1);
+        if (h_epos) hput(h_epos, h_ecap);
+        if (h_evel) hput(h_evel, h_ecap);
+        if (h_mout) hput(h_mout, 1);
+        h_ecap = 0;
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (ev_block) cudaEventDestroy(ev_block);
@@ -380,12 +481,12 @@ struct sdr_solver {
         ensure_capacity((size_t)n + k);
         if (k > h_ecap) {
             CK(cudaStreamSynchronize(st));
-            if (h_epos) cudaFreeHost(h_epos);
-            if (h_evel) cudaFreeHost(h_evel);
-            h_epos = h_evel = nullptr;
+            if (h_epos) hput(h_epos, h_ecap);
+            if (h_evel) hput(h_evel, h_ecap);
+            h_ecap = 0;
             size_t c = std::max<size_t>(k * 2, 4096);
-            CK(cudaMallocHost((void**)&h_epos, c * sizeof(float4)));
-            CK(cudaMallocHost((void**)&h_evel, c * sizeof(float4)));
+            hget(h_epos, c, &c);
+            hget(h_evel, c);
             h_ecap = c;
         }
         V3 axis = vnorm0({needle.axis.x, needle.axis.y, needle.axis.z});
@@ -778,12 +879,24 @@ struct sdr_solver {
 };
 
 struct sdr_metrics {
-    sdr_solver* owner = nullptr;
+    sdr_solver* owner = nullptr;  // null once the solver is destroyed
     double cavity_volume = 0;
     uint8_t *is_wall = nullptr, *washed = nullptr, *wet = nullptr;
     uint64_t wall_count = 0;
     std::vector<sdr_frame_metrics> history;
     double injected_ml = 0.0;
+
+    // Device masks are released on the owning solver's stream, whichever of
+    // the two is destroyed first; the summary and history stay readable.
+    void release() {
+        if (!owner) return;
+        dfree(is_wall, owner->st);
+        dfree(washed, owner->st);
+        dfree(wet, owner->st);
+        auto& c = owner->collectors;
+        c.erase(std::remove(c.begin(), c.end(), this), c.end());
+        owner = nullptr;
+    }
 };
 
 // ---------------------------------------------------------------- helpers
@@ -923,23 +1036,23 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
             s->nv = nx * (ny + 1) * nz;
             s->nw = nx * ny * (nz + 1);
             size_t sn = sdf->nx * sdf->ny * sdf->nz;
-            dalloc(s->sdf64, sn);
-            dalloc(s->sdf32, sn);
+            dalloc(s->sdf64, sn, s->st);
+            dalloc(s->sdf32, sn, s->st);
             CK(cudaMemcpyAsync(s->sdf64, sdf->data, sn * 8, cudaMemcpyHostToDevice, s->st));
             LAUNCH(k_f64_to_f32, blocks(sn, 256), 256, 0, s->st, s->sdf64, s->sdf32, sn);
-            dalloc(s->dst, 1);
+            dalloc(s->dst, 1, s->st);
             CK(cudaMemsetAsync(s->dst, 0, sizeof(DevStatus), s->st));
-            dalloc(s->rds, 1);
+            dalloc(s->rds, 1, s->st);
             CK(cudaMemsetAsync(s->rds, 0, sizeof(RedistState), s->st));
-            CK(cudaMallocHost((void**)&s->hst, sizeof(DevStatus)));
-            CK(cudaMallocHost((void**)&s->h_mout, sizeof(MetricsOut)));
+            hget(s->hst, 1);
+            hget(s->h_mout, 1);
             std::memset(s->hst, 0, sizeof(DevStatus));
             s->alloc_grid();
             LAUNCH(k_cavity_and_base, blocks(s->ncell, 256), 256, 0, s->st, g, s->sdf_d(), 0, Aabb{}, s->cavity,
                    s->base, 1);
             size_t want = options && options->max_particles ? options->max_particles
                                                              : std::min<size_t>(s->ncell * 2, 1 << 22);
-            s->ensure_capacity(std::max<size_t>(want, 1 << 16));
+            s->ensure_capacity(std::max<size_t>(want, 256));
             CK(cudaStreamSynchronize(s->st));
         } catch (...) {
             s->free_all();
@@ -955,6 +1068,7 @@ int sdr_solver_destroy(sdr_solver* s) {
         if (!s) return;
         DeviceScope ds(s->device);
         if (s->st) cudaStreamSynchronize(s->st);
+        while (!s->collectors.empty()) s->collectors.back()->release();
         s->free_all();
         delete s;
     });
@@ -1314,10 +1428,11 @@ int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
         sdr_metrics* m = new sdr_metrics();
         try {
             m->owner = s;
+            s->collectors.push_back(m);
             m->cavity_volume = cavity_volume;
-            dalloc(m->is_wall, s->ncell);
-            dalloc(m->washed, s->ncell);
-            dalloc(m->wet, s->ncell);
+            dalloc(m->is_wall, s->ncell, s->st);
+            dalloc(m->washed, s->ncell, s->st);
+            dalloc(m->wet, s->ncell, s->st);
             CK(cudaMemsetAsync(m->washed, 0, s->ncell, s->st));
             CK(cudaMemsetAsync(m->wet, 0, s->ncell, s->st));
             CK(cudaMemsetAsync(&s->dst->wall_count, 0, 8, s->st));
@@ -1327,9 +1442,7 @@ int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
             copy_dev(s, &s->dst->wall_count, 8, &wc);
             m->wall_count = wc;
         } catch (...) {
-            dfree(m->is_wall);
-            dfree(m->washed);
-            dfree(m->wet);
+            m->release();
             delete m;
             throw;
         }
@@ -1340,9 +1453,10 @@ int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
 int sdr_metrics_destroy(sdr_metrics* m) {
     return guard([&] {
         if (!m) return;
-        dfree(m->is_wall);
-        dfree(m->washed);
-        dfree(m->wet);
+        if (m->owner) {
+            DeviceScope ds(m->owner->device);
+            m->release();
+        }
         delete m;
     });
 }
@@ -1657,11 +1771,10 @@ int sdr_frame_writer_submit(sdr_frame_writer* w, sdr_solver* s, uint64_t frame) 
         try {
             const size_t n = s->n;
             if (n > w->cap[slot]) {
-                if (w->host[slot]) cudaFreeHost(w->host[slot]);
-                w->host[slot] = nullptr;
+                if (w->host[slot]) hput(w->host[slot], w->cap[slot]);
                 w->cap[slot] = 0;
                 size_t c = std::max<size_t>(n + n / 2, 4096);
-                CK(cudaMallocHost((void**)&w->host[slot], c * sizeof(float4)));
+                hget(w->host[slot], c, &c);
                 w->cap[slot] = c;
             }
             if (!w->ev[slot] || w->ev_device[slot] != s->device) {
@@ -1707,7 +1820,7 @@ int sdr_frame_writer_destroy(sdr_frame_writer* w) {
     const int rc = w->err_code;
     const std::string msg = w->err;
     for (int i = 0; i < 2; ++i) {
-        if (w->host[i]) cudaFreeHost(w->host[i]);
+        if (w->host[i]) hput(w->host[i], w->cap[i]);
         if (w->ev[i]) cudaEventDestroy(w->ev[i]);
     }
     delete w;

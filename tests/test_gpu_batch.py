@@ -87,3 +87,31 @@ def test_server_budget_admits_one_at_a_time():
         st = srv.stats()
     assert all(r.status == _lib.REQ_DONE for r in res)
     assert st["peak_active"] == 1 and st["peak_bytes"] <= int(fp * 1.5)
+
+
+def test_metrics_outlive_solver_and_growth_matches_preallocated():
+    """Device buffers are released in stream order: a collector destroyed after
+    its solver still answers its summary, and particle arrays that grow mid-run
+    (a stream-ordered copy into the larger arrays) give the same scene as
+    arrays sized for the whole run up front."""
+    from sdr_b200.solver import MetricsCollector, Solver
+    spec = _specs(flows=(8.0,), frames=4)[0]
+
+    def run(max_particles):
+        s = Solver(spec.sdf, spec.sim_dx, spec.fluid, spec.needle, max_particles=max_particles)
+        s.solve = spec.solve
+        s.outlet = spec.outlet
+        m = MetricsCollector(s, spec.cavity_volume)
+        for f in range(spec.frames):
+            s.step(spec.frame_dt)
+            m.record(s, f)
+        n = len(s)
+        s.close()  # the solver goes first
+        out = m.summary()
+        m.close()
+        return out, n
+
+    small, n_small = run(256)  # grows several times while the jet fills the cavity
+    big, n_big = run(1 << 20)
+    assert n_small > 4 * 256 and n_small == n_big
+    _same(small, big)
