@@ -322,7 +322,9 @@ def main():
                  "solves"], diag["pcg_section_cycles"]) if k not in ("unused", "lvl_stage_wait")},
             "pcg_section_cycles_frame": "one untimed frame after the timed ones, in-kernel section timers on",
             "pcg": {"launches": prof["pcg_launches"], "mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
-                    "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1)}}
+                    "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1)},
+            "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
+                               "long_sweeps": prof["redist_long_sweeps"]}}
     if rank == 0 and not args.no_cpu:
         orc = oracle_for(w, sdf)
         pos, vel = solver.particles()

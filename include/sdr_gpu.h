@@ -139,6 +139,11 @@ typedef struct {
      * then per forward-sweep level: staging wait, compute, barrier, level
      * count; then the sum of sweep widths, of non-empty level ranges, and solves. */
     uint64_t pcg_section_cycles[16];
+    /* redistribution: candidates (particles in over-cap cells) replayed, replay
+     * sweeps run, and sweeps whose list was longer than the shared-memory one */
+    uint64_t redist_candidates;
+    uint64_t redist_sweeps;
+    uint64_t redist_long_sweeps;
 } sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */

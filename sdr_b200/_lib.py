@@ -77,7 +77,9 @@ class Profile(C.Structure):
                 ("pcg_ms", C.c_double), ("gradient_extrapolate_ms", C.c_double), ("g2p_advect_ms", C.c_double),
                 ("compact_ms", C.c_double), ("redistribute_ms", C.c_double), ("substeps", C.c_uint64),
                 ("pcg_launches", C.c_uint64), ("pcg_cell_iters", C.c_uint64), ("fluid_cells", C.c_uint64),
-                ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16)]
+                ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16),
+                ("redist_candidates", C.c_uint64), ("redist_sweeps", C.c_uint64),
+                ("redist_long_sweeps", C.c_uint64)]
 
     def to_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}

@@ -4,6 +4,7 @@
 // compaction of ParticleSet::retain, and the redistribution sweeps.
 #pragma once
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace sdr {
 
@@ -412,6 +413,9 @@ struct RedistState {
     uint32_t nmoves;  // moves of the last sweep
     uint32_t err;
     unsigned long long moves_total;
+    unsigned long long cand_total;   // candidates replayed, all sweeps so far
+    unsigned long long sweeps_total;  // replay sweeps that ran
+    unsigned long long long_total;    // of those, sweeps past the shared-memory list
 };
 
 __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
@@ -455,6 +459,8 @@ struct RedistArgs {
     const uint8_t* cavity;
     uint32_t* cand;          // candidate particles (sorted in place when long)
     uint32_t cand_cap;
+    uint32_t* bitmap;        // long lists: scratch of ceil(n_upper / 32) words
+    uint32_t n_upper;        // bound on the particle count (and on every candidate index)
     uint32_t cap;
     double down[6];          // dir . gdir for -x,+x,-y,+y,-z,+z (f64, solver.rs:490-511)
     uint32_t* moves;         // pairs (particle, destination cell)
@@ -509,14 +515,32 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
                 __syncthreads();
             }
     } else {
-        // rank sort in global memory through the moves buffer as scratch
+        // Long lists: mark the candidates in a bitmap over particle indices,
+        // then compact the bitmap in index order: O(n / 32 + candidates).
+        __shared__ uint32_t ssh[33];
+        const uint32_t nw = (a.n_upper + 31) >> 5;
+        for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) a.bitmap[t] = 0u;
+        __syncthreads();
         for (uint32_t t = threadIdx.x; t < nc; t += blockDim.x) {
-            uint32_t v = a.cand[t], r = 0;
-            for (uint32_t u = 0; u < nc; ++u) r += a.cand[u] < v;
-            a.moves[r] = v;
+            uint32_t p = a.cand[t];
+            if (p < a.n_upper) atomicOr(&a.bitmap[p >> 5], 1u << (p & 31));
         }
         __syncthreads();
-        for (uint32_t t = threadIdx.x; t < nc; t += blockDim.x) a.cand[t] = a.moves[t];
+        uint32_t base = 0;  // candidates written by earlier chunks (block-uniform)
+        for (uint32_t w0 = 0; w0 < nw; w0 += blockDim.x) {
+            const uint32_t w = w0 + threadIdx.x;
+            uint32_t bits = w < nw ? a.bitmap[w] : 0u;
+            uint32_t ex;
+            const uint32_t tot = block_exscan_u32((uint32_t)__popc(bits), ex, ssh);
+            uint32_t o = base + ex;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                if (o < nc) a.cand[o] = (w << 5) + (uint32_t)b;
+                ++o;
+            }
+            base += tot;
+        }
         __syncthreads();
     }
     const uint32_t* cl = in_smem ? scand : a.cand;
@@ -629,6 +653,9 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
         s_nm = nm;
         rs->nmoves = nm;
         rs->moves_total += nm;
+        rs->cand_total += nc;
+        rs->sweeps_total += 1;
+        rs->long_total += in_smem ? 0 : 1;
         rs->ncand = 0;
         if (nm == 0) rs->active = 0;
     }

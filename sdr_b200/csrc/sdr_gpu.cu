@@ -191,6 +191,7 @@ struct DevStatus {
     unsigned long long fluid_count;
     unsigned long long wall_count;
     unsigned long long pcg_cycles[16];
+    unsigned long long redist_cand, redist_sweeps, redist_long;  // cumulative
 };
 
 __global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
@@ -202,6 +203,9 @@ __global__ void k_redist_begin(RedistState* r) {
 __global__ void k_redist_end(const RedistState* r, DevStatus* s) {
     s->moves = r->moves_total;
     s->err |= r->err;
+    s->redist_cand = r->cand_total;
+    s->redist_sweeps = r->sweeps_total;
+    s->redist_long = r->long_total;
 }
 __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
     size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -304,6 +308,7 @@ struct sdr_solver {
     MetricsOut* mout = nullptr;
     MetricsOut* h_mout = nullptr;
     bool sorted_valid = false;  // perm/start describe the current particle set
+    unsigned long long redist_seen[3] = {0, 0, 0};  // device redistribution counters at the last status read
     // timing
     cudaEvent_t ev[10] = {};
     cudaEvent_t ev_block = nullptr;  // blocking-sync event (SDR_SOLVER_BLOCKING_SYNC)
@@ -724,6 +729,8 @@ struct sdr_solver {
         ra.cavity = cavity;
         ra.cand = cand;
         ra.cand_cap = (uint32_t)cap;
+        ra.bitmap = ptmp;  // free between the sort of one substep and the next
+        ra.n_upper = n_upper;
         ra.cap = cap_;
         const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
@@ -810,7 +817,13 @@ struct sdr_solver {
             prof.fluid_cells += hst->nf;
             prof.particles += n_before;
             for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
+            prof.redist_candidates += hst->redist_cand - redist_seen[0];
+            prof.redist_sweeps += hst->redist_sweeps - redist_seen[1];
+            prof.redist_long_sweeps += hst->redist_long - redist_seen[2];
         }
+        redist_seen[0] = hst->redist_cand;
+        redist_seen[1] = hst->redist_sweeps;
+        redist_seen[2] = hst->redist_long;
         time += dt;
         steps += 1;
     }

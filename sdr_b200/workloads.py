@@ -110,6 +110,45 @@ def scene_spec(w: Workload):
 WORKLOADS = {"plain_parametric": plain_parametric, "real_cavity": real_cavity, "large_parametric": large_parametric}
 
 
+def hash_jitter(keys: np.ndarray) -> np.ndarray:
+    """hash_jitter (solver.rs:916-930) for an array of u64 keys: a splitmix64
+    finaliser of 3k, 3k+1, 3k+2, the top 53 bits mapped to [-0.3, 0.3); (n, 3) f64."""
+    k3 = np.asarray(keys, dtype=np.uint64) * np.uint64(3)
+    out = np.empty((k3.shape[0], 3))
+    for c in range(3):
+        z = k3 + np.uint64(c) + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+        out[:, c] = ((z >> np.uint64(11)).astype(np.float64) / float(1 << 53) - 0.5) * 0.6
+    return out
+
+
+def preseed_pool(solver, target: int, ppc: int = 8):
+    """Pre-seeded pool: the lowest in-cavity cells along gravity (ties in cell
+    order), ``ppc`` particles each at the cell centre plus hash_jitter(index) * dx,
+    at rest, until ``target`` particles or the cavity is full. Returns (pos, vel)
+    in f64 for ``Solver.set_particles``."""
+    st = solver.stats()
+    nx, ny, nz, dx = int(st.nx), int(st.ny), int(st.nz), float(st.dx)
+    org = np.array([st.origin.x, st.origin.y, st.origin.z])
+    g = np.array(solver.fluid.gravity, dtype=np.float64)
+    cav = np.flatnonzero(solver.cavity_mask().reshape(-1))
+    i = cav % nx
+    j = (cav // nx) % ny
+    k = cav // (nx * ny)
+    centre = org + (np.stack([i, j, k], axis=1) + 0.5) * dx
+    gl = np.linalg.norm(g)
+    depth = centre @ (g / gl) if gl > 0 else np.zeros(len(cav))
+    order = np.argsort(-depth, kind="stable")  # deepest along gravity first
+    ncell = min(len(cav), -(-int(target) // ppc))
+    cells = order[:ncell]
+    n = min(int(target), ncell * ppc)
+    idx = np.arange(n, dtype=np.uint64)
+    pos = centre[cells].repeat(ppc, axis=0)[:n] + hash_jitter(idx) * dx
+    return pos, np.zeros_like(pos)
+
+
 def build_gpu(w: Workload, max_particles: int = 0):
     """Device SDF + solver for a workload; returns (solver, sdf, cavity_volume)."""
     from .solver import Solver, build_sdf, cavity_volume

@@ -264,6 +264,39 @@ def test_redistribute_moves_exact(pair):
     assert d.max() < POS_TOL
 
 
+def test_redistribute_long_candidate_list_exact():
+    """More over-cap particles than the replay keeps in shared memory (8192):
+    600 cavity cells with 20 particles each, in shuffled index order, so the
+    candidates are put in index order by the long-list path."""
+    gpu, orc, res = make_pair()
+    nx, ny, nz = gpu.grid_dims
+    dx = gpu.dx
+    st = gpu.stats()
+    org = np.array([st.origin.x, st.origin.y, st.origin.z])
+    cav = np.flatnonzero(gpu.cavity_mask().reshape(-1))[:600]
+    assert len(cav) == 600
+    ijk = np.stack([cav % nx, (cav // nx) % ny, cav // (nx * ny)], axis=1)
+    rng = np.random.default_rng(7)
+    pos = (org + (ijk.repeat(20, axis=0) + 0.5 + rng.uniform(-0.3, 0.3, (600 * 20, 3))) * dx)
+    pos = f32(pos[rng.permutation(len(pos))])
+    vel = np.zeros_like(pos)
+    gpu.set_particles(pos, vel)
+    orc.set_particles(pos, vel)
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_REDISTRIBUTE)
+    orc.phase(oracle.PHASE_REDISTRIBUTE)
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    moved_g = np.any(pg != pos, axis=1)
+    moved_o = np.any(po != pos, axis=1)
+    d = np.max(np.abs(pg - po), axis=1)
+    record("redistribute_long", {"candidates": int(len(pos)), "moved_gpu": int(moved_g.sum()),
+                                 "moved_orc": int(moved_o.sum()), "max_abs_pos": float(d.max())})
+    assert moved_o.sum() > 1000
+    assert np.array_equal(moved_g, moved_o)
+    assert d.max() < POS_TOL
+
+
 def test_full_substep_shadow():
     """One full substep from identical state: counts, labels and particle state."""
     gpu, orc, res = make_pair(warm_frames=4)
