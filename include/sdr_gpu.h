@@ -144,6 +144,7 @@ typedef struct {
     uint64_t redist_candidates;
     uint64_t redist_sweeps;
     uint64_t redist_long_sweeps;
+    uint64_t pcg_cluster_launches; /* solves that ran on the cluster kernel */
 } sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */
@@ -207,6 +208,16 @@ int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
  * block-tree order — deterministic run to run, faster, differing from the
  * reference in the last bits of each dot. */
 int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
+/* Pressure-solve kernel. SDR_PCG_ONE_BLOCK: one persistent block on one SM
+ * (lowest latency per wavefront level; the choice for small fluid regions).
+ * SDR_PCG_CLUSTER: one thread-block cluster of up to 16 SMs, each level of
+ * the MIC(0) sweeps spread over all of them (large fluid regions). Both run
+ * the same per-cell arithmetic (pressure.rs:341-609); with the reference dot
+ * order both equal the reference bit for bit. With the default tree order the
+ * dot rounding differs between the two. SDR_PCG_AUTO (default): the cluster
+ * from 200,000 fluid cells in the previous solve. */
+enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2 };
+int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel);
 /* Phase-group timing with CUDA events (adds one event record per group):
  * on = 1. on = 2 also turns on the section timers inside the pressure-solve
  * kernel (pcg_section_cycles), which cost a little on its critical path. */

@@ -60,6 +60,7 @@ class SolverOptions(C.Structure):
 
 
 SOLVER_BLOCKING_SYNC = 1
+PCG_AUTO, PCG_ONE_BLOCK, PCG_CLUSTER = 0, 1, 2
 
 
 class SolverStats(C.Structure):
@@ -79,7 +80,7 @@ class Profile(C.Structure):
                 ("pcg_launches", C.c_uint64), ("pcg_cell_iters", C.c_uint64), ("fluid_cells", C.c_uint64),
                 ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16),
                 ("redist_candidates", C.c_uint64), ("redist_sweeps", C.c_uint64),
-                ("redist_long_sweeps", C.c_uint64)]
+                ("redist_long_sweeps", C.c_uint64), ("pcg_cluster_launches", C.c_uint64)]
 
     def to_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}
@@ -159,6 +160,7 @@ SIGNATURES = {
     "sdr_solver_get_stats": (i32, [vp, P(SolverStats)]),
     "sdr_solver_set_scalars": (i32, [vp, d, d, u64, u64, u64]),
     "sdr_solver_set_dot_order": (i32, [vp, i32]),
+    "sdr_solver_set_pcg_kernel": (i32, [vp, i32]),
     "sdr_solver_set_profiling": (i32, [vp, i32]),
     "sdr_solver_get_profile": (i32, [vp, P(Profile)]),
     "sdr_solver_reset_profile": (i32, [vp]),

@@ -1,0 +1,314 @@
+// pcg (src/pressure.rs:341-397) on one thread-block cluster, for fluid
+// regions too large for the one-block kernel k_pcg.
+//
+// Same wavefront layout, vectors and per-cell f64 arithmetic as k_pcg: the
+// MIC(0) factor (pressure.rs:442-513) and the two triangular sweeps
+// (pressure.rs:517-570) walk the i+j+k levels in order, but every level is
+// spread over all threads of the cluster (up to 16 CTAs on 16 SMs) and the
+// levels are separated by the hardware cluster barrier (barrier.cluster with
+// release/acquire), not a software grid barrier: no thread spins on memory.
+// Values that other CTAs wrote during the solve are read through L2
+// (ld.global.cg), so no stale L1 line is ever used.
+//
+// Dot products: in exact mode the reference's 4096-cell chunks (pressure.rs:
+// 588-603) are folded one warp per chunk across the cluster and the chunk sums
+// added in chunk order, bit-identical to k_pcg and to the reference. In tree
+// mode every CTA reduces its cells with a block tree and the CTA partials are
+// added in CTA order (deterministic; rounding differs from k_pcg's one tree).
+#pragma once
+#include "pressure.cuh"
+
+namespace sdr {
+
+constexpr int kClBS = 512;           // threads per CTA
+constexpr int kClMaxCtas = 16;       // largest cluster (non-portable size)
+constexpr int kClMaxLevelsSmem = 4096;
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+struct ClusterCtx {
+    int rank, nctas;
+    int gtid, gthreads;   // thread index and count over the cluster
+    const int* lvs;       // level starts (shared memory, or global when many)
+    double* slots;        // 2 x kClMaxCtas CTA partials in global memory
+    int parity;           // which half of `slots` the next reduction uses
+};
+
+// Cluster-wide reductions: block tree per CTA, CTA partials through global
+// memory, then every thread combines them in CTA order (same value in all
+// CTAs). The two halves of `slots` alternate, so a partial is never
+// overwritten before every CTA has read it (a cluster barrier separates a
+// reduction from the one two steps later that reuses its half).
+__device__ __forceinline__ double cl_sum(ClusterCtx& c, double v, double* sh) {
+    double bs = block_sum<kClBS>(v, sh);
+    double* sl = c.slots + c.parity * kClMaxCtas;
+    c.parity ^= 1;
+    if (threadIdx.x == 0) sl[c.rank] = bs;
+    cluster_sync_all();
+    double s = 0.0;
+    for (int q = 0; q < c.nctas; ++q) s = dadd(s, __ldcg(sl + q));
+    return s;
+}
+__device__ __forceinline__ double cl_max(ClusterCtx& c, double v, double* sh) {
+    double bm = block_max<kClBS>(v, sh);
+    double* sl = c.slots + c.parity * kClMaxCtas;
+    c.parity ^= 1;
+    if (threadIdx.x == 0) sl[c.rank] = bm;
+    cluster_sync_all();
+    double m = 0.0;
+    for (int q = 0; q < c.nctas; ++q) m = fmax(m, __ldcg(sl + q));
+    return m;
+}
+
+// Exact reference dot over `prod` (cell order), written before the call by
+// any CTA: one warp per 4096-cell chunk folds it in cell order, then every
+// CTA adds the chunk sums in chunk order.
+__device__ double cl_chunk_sums(const PcgArgs& a, ClusterCtx& c, double* sh) {
+    cluster_sync_all();  // all products written
+    const int lane = threadIdx.x & 31;
+    const int gw = c.rank * (kClBS / 32) + (threadIdx.x >> 5), nw = c.nctas * (kClBS / 32);
+    for (int ch = gw; ch < a.nchunks; ch += nw) {
+        int t = a.chunk_start[ch], e = a.chunk_start[ch + 1];
+        double acc = 0.0;
+        for (; t < e; t += 512) {
+            double v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                int idx = t + u * 32 + lane;
+                v[u] = idx < e ? __ldcg(a.prod + idx) : 0.0;
+            }
+            int cnt = min(512, e - t);
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+#pragma unroll 8
+                for (int src = 0; src < 32; ++src) {
+                    double x = __shfl_sync(0xffffffffu, v[u], src);
+                    if (u * 32 + src < cnt) acc = dadd(acc, x);
+                }
+            }
+        }
+        if (lane == 0) a.partials[ch] = acc;
+    }
+    cluster_sync_all();
+    if (threadIdx.x == 0) {
+        double s = -0.0;
+        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, __ldcg(a.partials + ch));
+        sh[0] = s;
+    }
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// build_mic0 (pressure.rs:442-513): forward level sweep over the cluster,
+// the same per-cell arithmetic as pcg_build_mic0.
+__device__ void cl_build_mic0(const PcgArgs& a, const ClusterCtx& c, int l0, int l1) {
+    const double TAU = 0.97, SIGMA = 0.25;
+    for (int L = l0; L < l1; ++L) {
+        const int ls = c.lvs[L], le = c.lvs[L + 1];
+        for (int ps = ls + c.gtid; ps < le; ps += c.gthreads) {
+            const int* nb = a.nbr + (size_t)ps * 6;
+            double axi = 0, pxi = 0, axi_y = 0, axi_z = 0;
+            double ayj = 0, pyj = 0, ayj_x = 0, ayj_z = 0;
+            double azk = 0, pzk = 0, azk_x = 0, azk_y = 0;
+            int mm = nb[NB_MX];
+            if (mm >= 0) {
+                int mk = a.nmask[mm];
+                axi = -1.0;
+                pxi = __ldcg(a.precon + mm);
+                axi_y = (mk >> NB_PY & 1) ? -1.0 : 0.0;
+                axi_z = (mk >> NB_PZ & 1) ? -1.0 : 0.0;
+            }
+            mm = nb[NB_MY];
+            if (mm >= 0) {
+                int mk = a.nmask[mm];
+                ayj = -1.0;
+                pyj = __ldcg(a.precon + mm);
+                ayj_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
+                ayj_z = (mk >> NB_PZ & 1) ? -1.0 : 0.0;
+            }
+            mm = nb[NB_MZ];
+            if (mm >= 0) {
+                int mk = a.nmask[mm];
+                azk = -1.0;
+                pzk = __ldcg(a.precon + mm);
+                azk_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
+                azk_y = (mk >> NB_PY & 1) ? -1.0 : 0.0;
+            }
+            double tx = dmul(axi, pxi), ty = dmul(ayj, pyj), tz = dmul(azk, pzk);
+            double diag = (double)a.diag[ps];
+            double mx = dmul(dmul(dmul(axi, dadd(axi_y, axi_z)), pxi), pxi);
+            double my = dmul(dmul(dmul(ayj, dadd(ayj_x, ayj_z)), pyj), pyj);
+            double mz = dmul(dmul(dmul(azk, dadd(azk_x, azk_y)), pzk), pzk);
+            double e = dsub(dsub(dsub(dsub(diag, dmul(tx, tx)), dmul(ty, ty)), dmul(tz, tz)),
+                            dmul(TAU, dadd(dadd(mx, my), mz)));
+            if (e < dmul(SIGMA, diag)) e = diag;
+            a.precon[ps] = e > 0.0 ? ddiv(1.0, __dsqrt_rn(e)) : 0.0;
+        }
+        cluster_sync_all();
+    }
+}
+
+// apply_mic0 (pressure.rs:517-570): forward L q = r, backward L^T z = q, and
+// the z*r products of the following dot (exact mode: into `prod`; tree mode:
+// this thread's running sum, returned).
+__device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const double* r, double* z, int l0, int l1) {
+    for (int L = l0; L < l1; ++L) {
+        const int ls = c.lvs[L], le = c.lvs[L + 1];
+        for (int ps = ls + c.gtid; ps < le; ps += c.gthreads) {
+            const int* nb = a.nbr + (size_t)ps * 6;
+            const int mx = nb[NB_MX], my = nb[NB_MY], mz = nb[NB_MZ];
+            double t = __ldcg(r + ps);
+            double pc = __ldcg(a.precon + ps);
+            double vx = mx >= 0 ? __ldcg(a.pq + mx) : 0.0;
+            double vy = my >= 0 ? __ldcg(a.pq + my) : 0.0;
+            double vz = mz >= 0 ? __ldcg(a.pq + mz) : 0.0;
+            if (mx >= 0) t = dadd(t, vx);
+            if (my >= 0) t = dadd(t, vy);
+            if (mz >= 0) t = dadd(t, vz);
+            double qv = dmul(t, pc);
+            a.q[ps] = qv;
+            a.pq[ps] = dmul(pc, qv);
+        }
+        cluster_sync_all();
+    }
+    double zr = 0.0;
+    for (int L = l1 - 1; L >= l0; --L) {
+        const int ls = c.lvs[L], le = c.lvs[L + 1];
+        for (int ps = ls + c.gtid; ps < le; ps += c.gthreads) {
+            const int* nb = a.nbr + (size_t)ps * 6;
+            const int px = nb[NB_PX], py = nb[NB_PY], pz = nb[NB_PZ];
+            double pc = __ldcg(a.precon + ps);
+            double t = __ldcg(a.q + ps);
+            double vx = px >= 0 ? __ldcg(z + px) : 0.0;
+            double vy = py >= 0 ? __ldcg(z + py) : 0.0;
+            double vz = pz >= 0 ? __ldcg(z + pz) : 0.0;
+            if (px >= 0) t = dadd(t, dmul(pc, vx));
+            if (py >= 0) t = dadd(t, dmul(pc, vy));
+            if (pz >= 0) t = dadd(t, dmul(pc, vz));
+            double zv = dmul(t, pc);
+            z[ps] = zv;
+            double pr = dmul(zv, __ldcg(r + ps));
+            if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
+            else zr = dadd(zr, pr);
+        }
+        cluster_sync_all();
+    }
+    return zr;
+}
+
+// The solve. Launched as exactly one cluster (gridDim = cluster size).
+// `slots` holds 2 x kClMaxCtas doubles of scratch for the CTA partials.
+__global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a, double* slots) {
+    __shared__ int s_lvs[kClMaxLevelsSmem + 1];
+    __shared__ double sh[40];
+    __shared__ int s_l0, s_l1;
+    ClusterCtx c;
+    c.rank = (int)cluster_rank();
+    c.nctas = (int)cluster_size();
+    c.gtid = c.rank * kClBS + (int)threadIdx.x;
+    c.gthreads = c.nctas * kClBS;
+    c.slots = slots;
+    c.parity = 0;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (a.nlevels <= kClMaxLevelsSmem) {
+        for (int L = tid; L <= a.nlevels; L += nt) s_lvs[L] = a.level_start[L];
+        c.lvs = s_lvs;
+    } else {
+        c.lvs = a.level_start;
+    }
+    if (tid == 0) {
+        s_l0 = a.nlevels;
+        s_l1 = 0;
+    }
+    __syncthreads();
+    for (int L = tid; L < a.nlevels; L += nt) {
+        if (c.lvs[L + 1] > c.lvs[L]) {
+            atomicMin(&s_l0, L);
+            atomicMax(&s_l1, L + 1);
+        }
+    }
+    __syncthreads();
+    const int l0 = s_l0, l1 = s_l1;
+    const uint32_t nf = *a.nf;
+    const int G = c.gthreads, gt = c.gtid;
+
+    double mx = 0.0;
+    for (uint32_t i = gt; i < nf; i += G) mx = fmax(mx, fabs(a.b[i]));
+    double residual = cl_max(c, mx, sh);
+    int iters = 0;
+    if (residual > a.tol) {
+        cl_build_mic0(a, c, l0, l1);
+        for (uint32_t i = gt; i < nf; i += G) {
+            a.r[i] = a.b[i];
+            a.p[i] = 0.0;
+        }
+        cluster_sync_all();
+        double zr = cl_apply_mic0(a, c, a.r, a.z, l0, l1);
+        for (uint32_t i = gt; i < nf; i += G) a.s[i] = __ldcg(a.z + i);
+        double sigma = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, zr, sh);  // dot(z, r); also orders s
+        for (int it = 0; it < a.max_iters; ++it) {
+            iters = it + 1;
+            // apply_a (pressure.rs:400-439): diag*x, then +x,-x,+y,-y,+z,-z; and s*As.
+            double sas = 0.0;
+            for (uint32_t i = gt; i < nf; i += G) {
+                const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
+                int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
+                int nbv[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
+                double sv = __ldcg(a.s + i);
+                double nsv[6];
+#pragma unroll
+                for (int d = 0; d < 6; ++d) nsv[d] = nbv[d] >= 0 ? __ldcg(a.s + nbv[d]) : 0.0;
+                double v = dmul((double)a.diag[i], sv);
+                if (nbv[NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
+                if (nbv[NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
+                if (nbv[NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
+                if (nbv[NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
+                if (nbv[NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
+                if (nbv[NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
+                a.as[i] = v;
+                if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv, v);
+                else sas = dadd(sas, dmul(sv, v));
+            }
+            double denom = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, sas, sh);  // dot(s, As)
+            if (fabs(denom) < 1e-30) break;
+            double alpha = ddiv(sigma, denom);
+            double mr = 0.0;
+            for (uint32_t i = gt; i < nf; i += G) {
+                a.p[i] = dadd(a.p[i], dmul(alpha, a.s[i]));
+                double rv = dsub(a.r[i], dmul(alpha, a.as[i]));
+                a.r[i] = rv;
+                mr = fmax(mr, fabs(rv));
+            }
+            residual = cl_max(c, mr, sh);  // also orders r before the sweeps
+            if (residual <= a.tol) break;
+            zr = cl_apply_mic0(a, c, a.r, a.z, l0, l1);
+            double sigma_new = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, zr, sh);  // dot(z, r)
+            double beta = ddiv(sigma_new, sigma);
+            for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(a.z + i), dmul(beta, a.s[i]));
+            cluster_sync_all();  // s complete before the next matvec reads neighbours
+            sigma = sigma_new;
+        }
+        for (uint32_t i = gt; i < nf; i += G) a.p_dense[a.lv_cell[i]] = a.p[i];
+    }
+    if (c.rank == 0 && tid == 0) {
+        *a.out_iters = iters;
+        *a.out_residual = residual;
+    }
+    cluster_sync_all();  // no CTA exits while another may still read its slots
+}
+
+}  // namespace sdr

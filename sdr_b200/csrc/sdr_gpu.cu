@@ -29,6 +29,7 @@
 #include "metrics.cuh"
 #include "particles.cuh"
 #include "pressure.cuh"
+#include "pressure_cluster.cuh"
 #include "scan.cuh"
 #include "sdf.cuh"
 
@@ -60,6 +61,34 @@ struct Fail {
     } while (0)
 
 inline unsigned blocks(size_t n, unsigned bs) { return (unsigned)std::max<size_t>(1, (n + bs - 1) / bs); }
+
+// Fluid cells from which SDR_PCG_AUTO solves on a cluster instead of one block
+// (the fluid count of the previous solve decides).
+constexpr uint32_t kClusterMinFluidCells = 200000;
+
+// CTAs in the cluster of the large-system pressure solve, once per device:
+// 16 (one per SM, the largest non-portable cluster) when the device can
+// schedule it for this kernel, else the portable 8.
+int pcg_cluster_ctas(int device) {
+    static std::mutex mu;
+    static int ctas[64] = {};
+    if (device < 0 || device >= 64) throw Fail{SDR_ERR_CUDA, "device index out of range"};
+    std::lock_guard<std::mutex> lk(mu);
+    if (!ctas[device]) {
+        int n = 8;
+        if (cudaFuncSetAttribute(k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(kClMaxCtas);
+            cfg.blockDim = dim3(kClBS);
+            int mx = 0;
+            if (cudaOccupancyMaxPotentialClusterSize(&mx, k_pcg_cluster, &cfg) == cudaSuccess && mx >= kClMaxCtas)
+                n = kClMaxCtas;
+        }
+        cudaGetLastError();  // a refused query leaves the portable size
+        ctas[device] = n;
+    }
+    return ctas[device];
+}
 
 // Solver-owned device buffers come from one library memory pool per device,
 // allocated and released in the order of the owning solver's stream
@@ -315,6 +344,9 @@ struct sdr_solver {
     bool profiling = false;
     bool kernel_timers = false;  // profiling level 2: section timers inside k_pcg
     bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
+    int pcg_kernel = SDR_PCG_AUTO;  // which pressure-solve kernel (SDR_PCG_*)
+    uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
+    double* cl_slots = nullptr;     // CTA partials of the cluster solve
     sdr_profile prof{};
     uint64_t particle_substeps = 0, substeps_total = 0;
     double device_ms = 0.0;
@@ -427,6 +459,7 @@ struct sdr_solver {
         dalloc(b, nc, st); dalloc(precon, nc, st); dalloc(p, nc, st); dalloc(r, nc, st); dalloc(z, nc, st);
         dalloc(s, nc, st); dalloc(as, nc, st); dalloc(q, nc, st); dalloc(pq, nc, st);
         dalloc(partials, nchunks + 1, st);
+        if (!cl_slots) dalloc(cl_slots, 2 * kClMaxCtas, st);
         dalloc(corder, nc, st);
         dalloc(cinv, nc, st);
         dalloc(prod, nc, st);
@@ -453,7 +486,7 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(partials, st); dfree(p_dense, st);
+        dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
         if (hst) hput(hst, 1);
@@ -636,7 +669,30 @@ struct sdr_solver {
         a.out_residual = &dst->residual;
         a.timing = kernel_timers ? dst->pcg_cycles : nullptr;
         a.exact_dots = exact_dots ? 1 : 0;
-        LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+        const bool cluster = pcg_kernel == SDR_PCG_CLUSTER ||
+                             (pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells);
+        if (cluster) {
+            // One cluster of up to 16 CTAs (one per SM); the levels of each
+            // sweep are separated by the hardware cluster barrier.
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3((unsigned)pcg_cluster_ctas(device));
+            cfg.blockDim = dim3(kClBS);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cfg.gridDim.x;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            a.timing = nullptr;
+            CK(cudaLaunchKernelEx(&cfg, k_pcg_cluster, a, cl_slots));
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            if (profiling) prof.pcg_cluster_launches += 1;
+        } else {
+            LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+        }
     }
 
     void project_gradient(double dt) {
@@ -798,6 +854,7 @@ struct sdr_solver {
         sync_status();
         last_pcg_iters = (uint64_t)hst->iters;
         last_residual = hst->residual;
+        last_nf = hst->nf;
         read_grid_speed();
         device_ms += elapsed(0, 9);
         particle_substeps += n_before;
@@ -883,6 +940,7 @@ struct sdr_solver {
             if (ph == SDR_PHASE_PROJECT) {
                 last_pcg_iters = (uint64_t)hst->iters;
                 last_residual = hst->residual;
+                last_nf = hst->nf;
                 if (profiling)
                     for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
             }
@@ -1167,6 +1225,15 @@ int sdr_solver_set_dot_order(sdr_solver* s, int reference_order) {
     return guard([&] {
         require(s, "null solver");
         s->exact_dots = reference_order != 0;
+    });
+}
+
+int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel) {
+    return guard([&] {
+        require(s, "null solver");
+        if (kernel != SDR_PCG_AUTO && kernel != SDR_PCG_ONE_BLOCK && kernel != SDR_PCG_CLUSTER)
+            throw Fail{SDR_ERR_INVALID, "unknown pressure-solve kernel " + std::to_string(kernel)};
+        s->pcg_kernel = kernel;
     });
 }
 

@@ -164,6 +164,10 @@ class Solver:
         """Reference dot order in the PCG (bit-exact pressure) or the faster block tree."""
         check(_lib.load().sdr_solver_set_dot_order(self._h, 1 if reference_order else 0))
 
+    def set_pcg_kernel(self, kernel: int) -> None:
+        """_lib.PCG_AUTO, PCG_ONE_BLOCK (one SM) or PCG_CLUSTER (up to 16 SMs)."""
+        check(_lib.load().sdr_solver_set_pcg_kernel(self._h, int(kernel)))
+
     def set_profiling(self, on: bool, kernel_timers: bool = False) -> None:
         """Phase timing with CUDA events; kernel_timers adds the pressure-solve section timers."""
         check(_lib.load().sdr_solver_set_profiling(self._h, (2 if kernel_timers else 1) if on else 0))

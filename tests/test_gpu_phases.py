@@ -126,11 +126,10 @@ flow_rate_ml_s = 5.0
 """
 
 
-def test_project_wide_levels_bit_exact():
-    """The parametric cavity filled with fluid at 0.6 mm: wavefront levels are
-    wider than the block's shared-memory window, so the sweeps take their
-    global-memory path for those levels (and the window path around them);
-    the pressure is still bit-exact with the reference dot order."""
+def _wide_pair():
+    """The parametric cavity filled with fluid at 0.6 mm (one particle per cell
+    centre) and random faces: a solve whose wavefront levels are wider than the
+    one-block kernel's shared-memory window."""
     gpu, orc, res = make_pair(WIDE_TOML)
     (nx, ny, nz), origin, dx = orc.grid
     k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
@@ -145,26 +144,53 @@ def test_project_wide_levels_bit_exact():
         f = f32(0.05 * rng.standard_normal(orc.face(w).shape))
         gpu.set_face(w, f)
         orc.set_face(w, f)
+    gpu.run_phase(_lib.PHASE_CLASSIFY)
+    orc.phase(oracle.PHASE_CLASSIFY)
+    fluid = orc.cells().reshape(nz, ny, nx) == 1
+    widths = np.bincount((i + j + k)[fluid])
+    sync_faces(gpu, orc)
+    return gpu, orc, fluid, widths
+
+
+@pytest.mark.parametrize("kernel", [_lib.PCG_ONE_BLOCK, _lib.PCG_CLUSTER], ids=["one_block", "cluster"])
+def test_project_wide_levels_bit_exact(kernel):
+    """Wide wavefront levels: the one-block kernel takes its global-memory path
+    for them (and the window path around them); the cluster kernel spreads
+    every level over its CTAs. With the reference dot order both give the
+    reference's pressure and iteration count bit for bit."""
+    gpu, orc, fluid, widths = _wide_pair()
     gpu.set_dot_order(True)
-    try:
-        gpu.run_phase(_lib.PHASE_CLASSIFY)
-        orc.phase(oracle.PHASE_CLASSIFY)
-        fluid = orc.cells().reshape(nz, ny, nx) == 1
-        widths = np.bincount((i + j + k)[fluid])
-        sync_faces(gpu, orc)
-        gpu.run_phase(_lib.PHASE_PROJECT, 1e-4)
-        orc.phase(oracle.PHASE_PROJECT, 1e-4)
-    finally:
-        gpu.set_dot_order(False)
+    gpu.set_pcg_kernel(kernel)
+    gpu.set_profiling(True)
+    gpu.run_phase(_lib.PHASE_PROJECT, 1e-4)
+    orc.phase(oracle.PHASE_PROJECT, 1e-4)
+    prof = gpu.profile()
     pg, po = gpu.pressure(), orc.pressure()
     it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
     diff = int(np.sum(pg.view(np.uint64) != po.view(np.uint64)))
-    record("project_wide", {"fluid_cells": int(fluid.sum()), "max_level_width": int(widths.max()),
-                            "levels_over_736": int((widths > 736).sum()), "iters_gpu": it_g, "iters_orc": it_o,
-                            "pressure_bit_mismatch": diff})
+    name = "project_wide" if kernel == _lib.PCG_ONE_BLOCK else "project_wide_cluster"
+    record(name, {"fluid_cells": int(fluid.sum()), "max_level_width": int(widths.max()),
+                  "levels_over_736": int((widths > 736).sum()), "iters_gpu": it_g, "iters_orc": it_o,
+                  "pressure_bit_mismatch": diff, "pcg_ms": prof["pcg_ms"]})
+    assert prof["pcg_cluster_launches"] == (1 if kernel == _lib.PCG_CLUSTER else 0)
     assert widths.max() > 768
     assert it_g == it_o
     assert diff == 0
+
+
+def test_project_cluster_tree_dots():
+    """The cluster kernel with its default tree dots (per-CTA trees added in
+    CTA order): pressure within the tree-order tolerance of the reference."""
+    gpu, orc, fluid, widths = _wide_pair()
+    gpu.set_pcg_kernel(_lib.PCG_CLUSTER)
+    gpu.run_phase(_lib.PHASE_PROJECT, 1e-4)
+    orc.phase(oracle.PHASE_PROJECT, 1e-4)
+    pg, po = gpu.pressure(), orc.pressure()
+    it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
+    e = rel_err(pg, po)
+    record("project_cluster_tree", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_rel_err": e})
+    assert abs(it_g - it_o) <= 1
+    assert e < PRESSURE_TOL
 
 
 PRESSURE_TOL = 1e-8  # block-tree dots: pressure relative to its max, f64
