@@ -27,6 +27,11 @@ dominated by the finest, fastest jets. The scenes run one after another
 through the public calls (the plain path), all at once (sdr_batch_run), and as
 Poisson arrivals into the request server (sdr_server_*, 150 GB admission
 budget) with p50/p99 time-to-summary.
+
+``large`` (one GPU): the 0.2 mm parametric cavity (207 x 217 x 161 cells)
+with a pre-seeded pool of 9.5 M particles at rest, ``--large-substeps``
+substeps at the fixed jet CFL step after ``--large-warmup``, device-timed;
+the oracle times one substep of the identical state.
 """
 from __future__ import annotations
 
@@ -214,6 +219,62 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
     }
 
 
+def large_bench(n_sub: int, warm: int, cpu: bool) -> dict:
+    """The 0.2 mm parametric cavity (207 x 217 x 161 cells) with a pre-seeded
+    pool: the deepest cavity cells filled at 8 particles per cell with
+    hash_jitter offsets, at rest (9.5 M particles, the cavity holds fewer than
+    the 30 M asked for), then substeps at the fixed jet CFL step. Inputs are far
+    larger than L2. The oracle times one substep of the identical state."""
+    import numpy as np
+    from sdr_b200 import workloads
+    w = workloads.large_parametric()
+    t0 = time.perf_counter()
+    solver, sdf, vol = workloads.build_gpu(w, max_particles=12_000_000)
+    pos, vel = workloads.preseed_pool(solver, 30_000_000)
+    pos = pos.astype(np.float32).astype(np.float64)  # the stored (f32) state, shared with the oracle
+    solver.set_particles(pos, vel)
+    setup_s = time.perf_counter() - t0
+    jet = solver.needle.flow_rate / (np.pi * solver.needle.radius ** 2)
+    dt = solver.dx / jet
+    solver.set_profiling(True)
+    for _ in range(warm):
+        solver.substep(dt)
+    solver.reset_profile()
+    st0 = solver.stats()
+    t0 = time.perf_counter()
+    for _ in range(n_sub):
+        solver.substep(dt)
+    wall = time.perf_counter() - t0
+    st1 = solver.stats()
+    prof = solver.profile()
+    dev_ms = st1.device_ms - st0.device_ms
+    ps = st1.particle_substeps - st0.particle_substeps
+    out = {"workload": "large_parametric, pre-seeded pool", "grid": [st1.nx, st1.ny, st1.nz],
+           "particles": int(len(pos)), "dt_s": dt, "warmup_substeps": warm, "substeps": n_sub,
+           "particle_substeps_per_s": ps / (dev_ms / 1e3), "wall_particle_substeps_per_s": ps / wall,
+           "ms_per_substep": dev_ms / n_sub, "setup_s": setup_s,
+           "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
+           "pcg": {"mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
+                   "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1),
+                   "cluster_launches": prof["pcg_cluster_launches"]},
+           "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
+                              "long_sweeps": prof["redist_long_sweeps"]}}
+    solver.close()
+    if cpu:
+        import oracle
+        orc = oracle_for(w, sdf)
+        orc.set_particles(pos, vel)
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        t0 = time.perf_counter()
+        orc.substep(dt)
+        ct = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(pos) / ct, "unit": "particle-substeps/s", "cores": threads,
+                               "kind": "port", "sample": f"one substep of the pre-seeded state ({ct:.1f} s); "
+                                                         "C++ restatement of the reference solver, f64"}
+    return {"large": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,6 +289,9 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=48)
     ap.add_argument("--batch-cfl", type=int, default=150)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--large-substeps", type=int, default=5)
+    ap.add_argument("--large-warmup", type=int, default=3)
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -342,6 +406,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_batch and args.batch_scenes > 0:
         solver.close()
         line.update(batch_bench(args.batch_scenes, args.batch_cfl))
+    if rank == 0 and world == 1 and not args.no_large:
+        solver.close()  # idempotent
+        line.update(large_bench(args.large_substeps, args.large_warmup, cpu=not args.no_cpu))
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

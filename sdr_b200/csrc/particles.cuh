@@ -431,17 +431,30 @@ __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const ui
 }
 
 // Particles in over-cap cells, appended in arbitrary order (sorted later).
-__global__ void k_redist_append(const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
-                                const uint32_t* __restrict__ n_dev, uint32_t cap, RedistState* __restrict__ rs,
-                                uint32_t* __restrict__ cand, uint32_t cand_cap) {
+// A particle is left out when no face neighbour of its cell is an in-cavity
+// cell below the cap at the start of the sweep: within a sweep a cell only
+// receives while below the cap and a source never drains below it, so such a
+// cell never gains a receiver and the reference loop (solver.rs:476-555)
+// leaves every one of its particles where it is. The moves are unchanged.
+__global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
+                                const uint8_t* __restrict__ cavity, const uint32_t* __restrict__ n_dev,
+                                uint32_t cap, RedistState* __restrict__ rs, uint32_t* __restrict__ cand,
+                                uint32_t cand_cap) {
     if (!rs->active) return;
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= *n_dev) return;
     int c = key_cell[p];
-    if (c >= 0 && count[c] > cap) {
-        uint32_t s = atomicAdd(&rs->ncand, 1u);
-        if (s < cand_cap) cand[s] = p;
-    }
+    if (c < 0 || count[c] <= cap) return;
+    const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+    const int sxy = g.nx * g.ny;
+    const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                       j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
+    bool room = false;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) room |= nb[q] >= 0 && cavity[nb[q]] && count[nb[q]] < cap;
+    if (!room) return;
+    uint32_t s = atomicAdd(&rs->ncand, 1u);
+    if (s < cand_cap) cand[s] = p;
 }
 
 constexpr int kRedistTable = 4096;   // shared-memory hash slots (power of two)

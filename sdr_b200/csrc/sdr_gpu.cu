@@ -796,7 +796,7 @@ struct sdr_solver {
         for (int sweep = 0; sweep < 4; ++sweep) {
             CK(cudaMemsetAsync(hist_valid, 0, ncell * 4, st));
             LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), rds, key_cell, hist_valid);
-            LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, key_cell, hist_valid, dn(), cap_, rds, cand,
+            LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, g, key_cell, hist_valid, cavity, dn(), cap_, rds, cand,
                    (uint32_t)cap);
             LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
         }
