@@ -234,4 +234,20 @@ __device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t* sh) {
     return r;
 }
 
+// Thread-block clusters: the hardware barrier over every thread of every CTA
+// of the cluster (release/acquire at cluster scope), and the CTA's place in it.
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
 }  // namespace sdr

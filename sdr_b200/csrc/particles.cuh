@@ -416,6 +416,10 @@ struct RedistState {
     unsigned long long cand_total;   // candidates replayed, all sweeps so far
     unsigned long long sweeps_total;  // replay sweeps that ran
     unsigned long long long_total;    // of those, sweeps past the shared-memory list
+    uint32_t par;         // 1: the list is long; k_redist_par decides and applies this sweep
+    uint32_t round_base;  // claim stamps used so far by k_redist_par (grows across sweeps)
+    uint32_t nmoves_par;  // moves appended by k_redist_par this sweep
+    uint32_t pad;
 };
 
 __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
@@ -478,7 +482,28 @@ struct RedistArgs {
     double down[6];          // dir . gdir for -x,+x,-y,+y,-z,+z (f64, solver.rs:490-511)
     uint32_t* moves;         // pairs (particle, destination cell)
     RedistState* rs;
+    unsigned long long* claim;  // per cell: the latest claim stamp (k_redist_par); zero at allocation
+    double* slots;              // 2 x 16 doubles: CTA partials of k_redist_par's reductions
 };
+
+// A move: the particle goes near the destination centre with its index-keyed
+// jitter (hash_jitter, solver.rs:916-930), pushed inside, with the local grid
+// velocity (solver.rs:545-554).
+__device__ __forceinline__ void redist_apply_move(const RedistArgs& a, uint32_t p, uint32_t c) {
+    const Grid& g = a.g;
+    int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+    uint64_t key = p;
+    double jx = jitter_mix(key * 3), jy = jitter_mix(key * 3 + 1), jz = jitter_mix(key * 3 + 2);
+    double cx = dadd(g.ox, dmul((double)i + 0.5, g.dx));
+    double cy = dadd(g.oy, dmul((double)j + 0.5, g.dx));
+    double cz = dadd(g.oz, dmul((double)k + 0.5, g.dx));
+    float3 q = make_float3((float)dadd(cx, dmul(jx, g.dx)), (float)dadd(cy, dmul(jy, g.dx)),
+                           (float)dadd(cz, dmul(jz, g.dx)));
+    q = project_inside(a.sdf, 0.5f * g.dxf, q);
+    float3 v = velocity_at(g, a.f, q.x, q.y, q.z);
+    a.pos[p] = make_float4(q.x, q.y, q.z, 0.0f);
+    a.vel[p] = make_float4(v.x, v.y, v.z, 0.0f);
+}
 
 __device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761u) & (kRedistTable - 1); }
 
@@ -555,6 +580,10 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
             base += tot;
         }
         __syncthreads();
+        // The list is now in index order in a.cand: k_redist_par (the next
+        // launch) decides the moves in parallel rounds and applies them.
+        if (threadIdx.x == 0) rs->par = 1;
+        return;
     }
     const uint32_t* cl = in_smem ? scand : a.cand;
     // ---- hash table of referenced cells
@@ -676,24 +705,168 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     // ---- apply the moves: near the destination centre with the index-keyed
     // jitter, pushed inside, with the local grid velocity.
     const uint32_t nm = s_nm;
-    for (uint32_t mv = threadIdx.x; mv < nm; mv += blockDim.x) {
-        uint32_t p = a.moves[2 * mv], c = a.moves[2 * mv + 1];
-        int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
-        uint64_t key = p;
-        double jx = jitter_mix(key * 3), jy = jitter_mix(key * 3 + 1), jz = jitter_mix(key * 3 + 2);
-        double cx = dadd(g.ox, dmul((double)i + 0.5, g.dx));
-        double cy = dadd(g.oy, dmul((double)j + 0.5, g.dx));
-        double cz = dadd(g.oz, dmul((double)k + 0.5, g.dx));
-        float3 q = make_float3((float)dadd(cx, dmul(jx, g.dx)), (float)dadd(cy, dmul(jy, g.dx)),
-                               (float)dadd(cz, dmul(jz, g.dx)));
-        q = project_inside(a.sdf, 0.5f * g.dxf, q);
-        float3 v = velocity_at(g, a.f, q.x, q.y, q.z);
-        a.pos[p] = make_float4(q.x, q.y, q.z, 0.0f);
-        a.vel[p] = make_float4(v.x, v.y, v.z, 0.0f);
-    }
+    for (uint32_t mv = threadIdx.x; mv < nm; mv += blockDim.x) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
 }
 
 constexpr size_t kRedistSmem = (size_t)kRedistTable * 4 * 2 + (size_t)kRedistSmemCand * 4 +
                                (size_t)kRedistSmemCand * 7 * 2 + kRedistTable;
+
+// ---------------------------------------------------------------------------
+// Long candidate lists: the reference's sequential loop (solver.rs:476-555)
+// replayed in parallel rounds on one thread-block cluster, with the same moves.
+//
+// Within a sweep a cell only receives while below the cap and a source cell
+// (above the cap) only loses particles and never drops below the cap. So a
+// candidate's decision reads just two kinds of changing counts: its own cell's
+// (changed only by candidates of that cell) and those of its neighbours that
+// are below the cap (changed only by candidates that may choose them); every
+// other neighbour is full or outside the cavity for the rest of the sweep.
+// Each round every pending candidate m claims its cell and each neighbour
+// still below the cap with a stamp that orders lower indices first; m runs
+// when it holds all its claims, i.e. when no lower pending candidate can
+// change what m reads or read what m changes. Those candidates run at once
+// (their cells are disjoint), which is the sequential result. Candidates whose
+// cell is back at the cap, or whose neighbours are all full, can never move
+// again and leave the list. The lowest pending candidate always runs, so the
+// rounds end; a bound on them still records an error bit if they did not.
+constexpr int kRpBS = 512;
+constexpr uint32_t kResolved = 0x80000000u;
+
+__device__ __forceinline__ double rp_cluster_sum(double v, double* slots, int& parity, double* sh) {
+    double bs = block_sum<kRpBS>(v, sh);
+    double* sl = slots + parity * 16;
+    parity ^= 1;
+    if (threadIdx.x == 0) sl[cluster_rank()] = bs;
+    cluster_sync_all();
+    double s = 0.0;
+    const int n = (int)cluster_size();
+    for (int q = 0; q < n; ++q) s += __ldcg(sl + q);
+    return s;
+}
+
+__global__ void __launch_bounds__(kRpBS, 1) k_redist_par(RedistArgs a) {
+    __shared__ double sh[40];
+    RedistState* rs = a.rs;
+    if (!rs->active || !rs->par) return;  // written by earlier launches: the same in every CTA
+    const int rank = (int)cluster_rank(), nct = (int)cluster_size();
+    const uint32_t gt = (uint32_t)(rank * kRpBS + threadIdx.x), G = (uint32_t)(nct * kRpBS);
+    const uint32_t nc = rs->ncand, cap = a.cap;
+    const Grid& g = a.g;
+    const int sxy = g.nx * g.ny;
+    uint32_t base = rs->round_base;
+    cluster_sync_all();  // every CTA has read the state before it changes
+    if (base > 0xF0000000u) {  // stamps about to wrap: clear the claims and start again
+        const size_t nce = (size_t)g.nx * g.ny * g.nz;
+        for (size_t c = gt; c < nce; c += G) a.claim[c] = 0ull;
+        base = 0;
+        cluster_sync_all();
+    }
+    int parity = 0;
+    uint32_t round = 0;
+    bool done = nc == 0;
+    while (!done) {
+        ++round;
+        const unsigned long long stamp = (unsigned long long)(base + round) << 32;
+        // claims (or leave the list)
+        for (uint32_t m = gt; m < nc; m += G) {
+            const uint32_t p = a.cand[m];
+            if (p & kResolved) continue;
+            const int c = a.key_cell[p];
+            if (__ldcg(a.count + c) <= cap) {
+                a.cand[m] = p | kResolved;
+                continue;
+            }
+            const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / sxy;
+            const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                               j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
+            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const int n = nb[q];
+                if (n >= 0 && a.cavity[n] && __ldcg(a.count + n) < cap) {
+                    atomicMax(a.claim + n, key);
+                    any = true;
+                }
+            }
+            if (!any) {
+                a.cand[m] = p | kResolved;
+                continue;
+            }
+            atomicMax(a.claim + c, key);
+        }
+        cluster_sync_all();
+        // candidates holding all their claims run (counts are as in the claim step)
+        double pending = 0.0;
+        for (uint32_t m = gt; m < nc; m += G) {
+            const uint32_t p = a.cand[m];
+            if (p & kResolved) continue;
+            const int c = a.key_cell[p];
+            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+            const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / sxy;
+            const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
+                               j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
+            uint32_t cnt[6];
+            bool ready = __ldcg(a.claim + c) == key;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const int n = nb[q];
+                cnt[q] = 0xFFFFFFFFu;
+                if (n >= 0 && a.cavity[n]) {
+                    cnt[q] = __ldcg(a.count + n);
+                    if (cnt[q] < cap && __ldcg(a.claim + n) != key) ready = false;
+                }
+            }
+            if (!ready) {
+                pending += 1.0;
+                continue;
+            }
+            int best = -1;
+            double best_down = -INFINITY;
+            uint32_t best_room = 0;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
+                if (cnt[q] >= cap) continue;  // full, outside the cavity, or out of bounds
+                const uint32_t room = cap - cnt[q];
+                const double dn = a.down[q];
+                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                    best = nb[q];
+                    best_down = dn;
+                    best_room = room;
+                }
+            }
+            if (best < 0) {  // its last neighbour with room was filled this round by a lower candidate
+                a.cand[m] = p | kResolved;
+                continue;
+            }
+            a.count[c] = __ldcg(a.count + c) - 1u;
+            a.count[best] = __ldcg(a.count + best) + 1u;
+            const uint32_t slot = atomicAdd(&rs->nmoves_par, 1u);
+            a.moves[2 * slot] = p;
+            a.moves[2 * slot + 1] = (uint32_t)best;
+            a.cand[m] = p | kResolved;
+        }
+        done = rp_cluster_sum(pending, a.slots, parity, sh) == 0.0;
+        if (!done && round > nc) {  // cannot happen: the lowest pending candidate always runs
+            if (rank == 0 && threadIdx.x == 0) atomicOr(&rs->err, 4u);
+            done = true;
+        }
+    }
+    const uint32_t nm = __ldcg(&rs->nmoves_par);
+    for (uint32_t mv = gt; mv < nm; mv += G) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
+    cluster_sync_all();
+    if (rank == 0 && threadIdx.x == 0) {
+        rs->nmoves = nm;
+        rs->moves_total += nm;
+        rs->cand_total += nc;
+        rs->sweeps_total += 1;
+        rs->long_total += 1;
+        rs->ncand = 0;
+        rs->par = 0;
+        rs->nmoves_par = 0;
+        rs->round_base = base + round + 1;
+        if (nm == 0) rs->active = 0;
+    }
+}
 
 }  // namespace sdr

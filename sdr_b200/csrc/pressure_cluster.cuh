@@ -24,19 +24,6 @@ constexpr int kClBS = 512;           // threads per CTA
 constexpr int kClMaxCtas = 16;       // largest cluster (non-portable size)
 constexpr int kClMaxLevelsSmem = 4096;
 
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_size() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-    return r;
-}
 
 struct ClusterCtx {
     int rank, nctas;
@@ -164,48 +151,127 @@ __device__ void cl_build_mic0(const PcgArgs& a, const ClusterCtx& c, int l0, int
 
 // apply_mic0 (pressure.rs:517-570): forward L q = r, backward L^T z = q, and
 // the z*r products of the following dot (exact mode: into `prod`; tree mode:
-// this thread's running sum, returned).
+// this thread's running sum, returned). A thread's first cell of the next
+// level (its neighbour indices, operand and factor, none of which the sweep
+// writes) is loaded before the level barrier, so after the barrier only the
+// neighbours' sweep values are on the critical path; further cells of wide
+// levels load inline.
 __device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const double* r, double* z, int l0, int l1) {
+    const int G = c.gthreads;
+    // ---------------- forward
+    int ps = c.lvs[l0] + c.gtid, le = c.lvs[l0 + 1];
+    int mx = -1, my = -1, mz = -1;
+    double rv = 0.0, pc = 0.0;
+    if (ps < le) {
+        const int* nb = a.nbr + (size_t)ps * 6;
+        mx = nb[NB_MX]; my = nb[NB_MY]; mz = nb[NB_MZ];
+        rv = __ldcg(r + ps);
+        pc = __ldcg(a.precon + ps);
+    }
     for (int L = l0; L < l1; ++L) {
-        const int ls = c.lvs[L], le = c.lvs[L + 1];
-        for (int ps = ls + c.gtid; ps < le; ps += c.gthreads) {
-            const int* nb = a.nbr + (size_t)ps * 6;
-            const int mx = nb[NB_MX], my = nb[NB_MY], mz = nb[NB_MZ];
-            double t = __ldcg(r + ps);
-            double pc = __ldcg(a.precon + ps);
+        const int nps = le + c.gtid, nle = L + 1 < l1 ? c.lvs[L + 2] : le;
+        int nmx = -1, nmy = -1, nmz = -1;
+        double nrv = 0.0, npc = 0.0;
+        if (nps < nle) {
+            const int* nb = a.nbr + (size_t)nps * 6;
+            nmx = nb[NB_MX]; nmy = nb[NB_MY]; nmz = nb[NB_MZ];
+            nrv = __ldcg(r + nps);
+            npc = __ldcg(a.precon + nps);
+        }
+        if (ps < le) {
             double vx = mx >= 0 ? __ldcg(a.pq + mx) : 0.0;
             double vy = my >= 0 ? __ldcg(a.pq + my) : 0.0;
             double vz = mz >= 0 ? __ldcg(a.pq + mz) : 0.0;
+            double t = rv;
             if (mx >= 0) t = dadd(t, vx);
             if (my >= 0) t = dadd(t, vy);
             if (mz >= 0) t = dadd(t, vz);
             double qv = dmul(t, pc);
             a.q[ps] = qv;
             a.pq[ps] = dmul(pc, qv);
+            for (int p2 = ps + G; p2 < le; p2 += G) {
+                const int* nb = a.nbr + (size_t)p2 * 6;
+                const int x = nb[NB_MX], y = nb[NB_MY], zz = nb[NB_MZ];
+                double t2 = __ldcg(r + p2), pc2 = __ldcg(a.precon + p2);
+                double wx = x >= 0 ? __ldcg(a.pq + x) : 0.0;
+                double wy = y >= 0 ? __ldcg(a.pq + y) : 0.0;
+                double wz = zz >= 0 ? __ldcg(a.pq + zz) : 0.0;
+                if (x >= 0) t2 = dadd(t2, wx);
+                if (y >= 0) t2 = dadd(t2, wy);
+                if (zz >= 0) t2 = dadd(t2, wz);
+                double q2 = dmul(t2, pc2);
+                a.q[p2] = q2;
+                a.pq[p2] = dmul(pc2, q2);
+            }
         }
         cluster_sync_all();
+        ps = nps; le = nle;
+        mx = nmx; my = nmy; mz = nmz;
+        rv = nrv; pc = npc;
     }
+    // ---------------- backward
     double zr = 0.0;
+    int ls = c.lvs[l1 - 1];
+    ps = ls + c.gtid;
+    le = c.lvs[l1];
+    int px = -1, py = -1, pz = -1;
+    double qv = 0.0, rr = 0.0;
+    pc = 0.0;
+    if (ps < le) {
+        const int* nb = a.nbr + (size_t)ps * 6;
+        px = nb[NB_PX]; py = nb[NB_PY]; pz = nb[NB_PZ];
+        qv = __ldcg(a.q + ps);
+        rr = __ldcg(r + ps);
+        pc = __ldcg(a.precon + ps);
+    }
     for (int L = l1 - 1; L >= l0; --L) {
-        const int ls = c.lvs[L], le = c.lvs[L + 1];
-        for (int ps = ls + c.gtid; ps < le; ps += c.gthreads) {
-            const int* nb = a.nbr + (size_t)ps * 6;
-            const int px = nb[NB_PX], py = nb[NB_PY], pz = nb[NB_PZ];
-            double pc = __ldcg(a.precon + ps);
-            double t = __ldcg(a.q + ps);
+        const int nls = L - 1 >= l0 ? c.lvs[L - 1] : ls;
+        const int nps = nls + c.gtid, nle = ls;
+        int npx = -1, npy = -1, npz = -1;
+        double nqv = 0.0, nrr = 0.0, npc = 0.0;
+        if (nps < nle) {
+            const int* nb = a.nbr + (size_t)nps * 6;
+            npx = nb[NB_PX]; npy = nb[NB_PY]; npz = nb[NB_PZ];
+            nqv = __ldcg(a.q + nps);
+            nrr = __ldcg(r + nps);
+            npc = __ldcg(a.precon + nps);
+        }
+        if (ps < le) {
             double vx = px >= 0 ? __ldcg(z + px) : 0.0;
             double vy = py >= 0 ? __ldcg(z + py) : 0.0;
             double vz = pz >= 0 ? __ldcg(z + pz) : 0.0;
+            double t = qv;
             if (px >= 0) t = dadd(t, dmul(pc, vx));
             if (py >= 0) t = dadd(t, dmul(pc, vy));
             if (pz >= 0) t = dadd(t, dmul(pc, vz));
             double zv = dmul(t, pc);
             z[ps] = zv;
-            double pr = dmul(zv, __ldcg(r + ps));
+            double pr = dmul(zv, rr);
             if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
             else zr = dadd(zr, pr);
+            for (int p2 = ps + G; p2 < le; p2 += G) {
+                const int* nb = a.nbr + (size_t)p2 * 6;
+                const int x = nb[NB_PX], y = nb[NB_PY], zz = nb[NB_PZ];
+                double pc2 = __ldcg(a.precon + p2);
+                double t2 = __ldcg(a.q + p2);
+                double wx = x >= 0 ? __ldcg(z + x) : 0.0;
+                double wy = y >= 0 ? __ldcg(z + y) : 0.0;
+                double wz = zz >= 0 ? __ldcg(z + zz) : 0.0;
+                if (x >= 0) t2 = dadd(t2, dmul(pc2, wx));
+                if (y >= 0) t2 = dadd(t2, dmul(pc2, wy));
+                if (zz >= 0) t2 = dadd(t2, dmul(pc2, wz));
+                double z2 = dmul(t2, pc2);
+                z[p2] = z2;
+                double pr2 = dmul(z2, __ldcg(r + p2));
+                if (a.exact_dots) a.prod[a.cinv[p2]] = pr2;
+                else zr = dadd(zr, pr2);
+            }
         }
         cluster_sync_all();
+        ls = nls;
+        ps = nps; le = nle;
+        px = npx; py = npy; pz = npz;
+        qv = nqv; rr = nrr; pc = npc;
     }
     return zr;
 }

@@ -66,28 +66,48 @@ inline unsigned blocks(size_t n, unsigned bs) { return (unsigned)std::max<size_t
 // (the fluid count of the previous solve decides).
 constexpr uint32_t kClusterMinFluidCells = 200000;
 
-// CTAs in the cluster of the large-system pressure solve, once per device:
+// CTAs in the cluster of a one-cluster kernel, once per device and kernel:
 // 16 (one per SM, the largest non-portable cluster) when the device can
-// schedule it for this kernel, else the portable 8.
-int pcg_cluster_ctas(int device) {
+// schedule it for that kernel, else the portable 8.
+template <class Kern>
+int cluster_ctas(Kern kernel, int slot, int threads, int device) {
     static std::mutex mu;
-    static int ctas[64] = {};
+    static int ctas[2][64] = {};
     if (device < 0 || device >= 64) throw Fail{SDR_ERR_CUDA, "device index out of range"};
     std::lock_guard<std::mutex> lk(mu);
-    if (!ctas[device]) {
+    if (!ctas[slot][device]) {
         int n = 8;
-        if (cudaFuncSetAttribute(k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(kClMaxCtas);
-            cfg.blockDim = dim3(kClBS);
+            cfg.blockDim = dim3(threads);
             int mx = 0;
-            if (cudaOccupancyMaxPotentialClusterSize(&mx, k_pcg_cluster, &cfg) == cudaSuccess && mx >= kClMaxCtas)
+            if (cudaOccupancyMaxPotentialClusterSize(&mx, kernel, &cfg) == cudaSuccess && mx >= kClMaxCtas)
                 n = kClMaxCtas;
         }
         cudaGetLastError();  // a refused query leaves the portable size
-        ctas[device] = n;
+        ctas[slot][device] = n;
     }
-    return ctas[device];
+    return ctas[slot][device];
+}
+
+// Launch a kernel as exactly one cluster of `ctas` CTAs on `st`.
+template <class Kern, class... Args>
+void launch_one_cluster(Kern kernel, int ctas, int threads, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)ctas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kernel, args...));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 // Solver-owned device buffers come from one library memory pool per device,
@@ -228,6 +248,8 @@ __global__ void k_redist_begin(RedistState* r) {
     r->ncand = 0;
     r->active = 1;
     r->nmoves = 0;
+    r->par = 0;
+    r->nmoves_par = 0;
 }
 __global__ void k_redist_end(const RedistState* r, DevStatus* s) {
     s->moves = r->moves_total;
@@ -346,7 +368,8 @@ struct sdr_solver {
     bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
     int pcg_kernel = SDR_PCG_AUTO;  // which pressure-solve kernel (SDR_PCG_*)
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
-    double* cl_slots = nullptr;     // CTA partials of the cluster solve
+    double* cl_slots = nullptr;     // CTA partials of the cluster kernels
+    unsigned long long* rclaim = nullptr;  // per cell: claim stamps of the parallel redistribution replay
     sdr_profile prof{};
     uint64_t particle_substeps = 0, substeps_total = 0;
     double device_ms = 0.0;
@@ -460,6 +483,8 @@ struct sdr_solver {
         dalloc(s, nc, st); dalloc(as, nc, st); dalloc(q, nc, st); dalloc(pq, nc, st);
         dalloc(partials, nchunks + 1, st);
         if (!cl_slots) dalloc(cl_slots, 2 * kClMaxCtas, st);
+        dalloc(rclaim, ncell, st);
+        CK(cudaMemsetAsync(rclaim, 0, ncell * sizeof(unsigned long long), st));
         dalloc(corder, nc, st);
         dalloc(cinv, nc, st);
         dalloc(prod, nc, st);
@@ -486,7 +511,7 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st);
+        dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
         if (hst) hput(hst, 1);
@@ -674,21 +699,8 @@ struct sdr_solver {
         if (cluster) {
             // One cluster of up to 16 CTAs (one per SM); the levels of each
             // sweep are separated by the hardware cluster barrier.
-            cudaLaunchConfig_t cfg{};
-            cfg.gridDim = dim3((unsigned)pcg_cluster_ctas(device));
-            cfg.blockDim = dim3(kClBS);
-            cfg.dynamicSmemBytes = 0;
-            cfg.stream = st;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = cfg.gridDim.x;
-            at[0].val.clusterDim.y = 1;
-            at[0].val.clusterDim.z = 1;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
             a.timing = nullptr;
-            CK(cudaLaunchKernelEx(&cfg, k_pcg_cluster, a, cl_slots));
-            g_launches.fetch_add(1, std::memory_order_relaxed);
+            launch_one_cluster(k_pcg_cluster, cluster_ctas(k_pcg_cluster, 0, kClBS, device), kClBS, st, a, cl_slots);
             if (profiling) prof.pcg_cluster_launches += 1;
         } else {
             LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
@@ -787,6 +799,9 @@ struct sdr_solver {
         ra.cand_cap = (uint32_t)cap;
         ra.bitmap = ptmp;  // free between the sort of one substep and the next
         ra.n_upper = n_upper;
+        ra.claim = rclaim;
+        ra.slots = cl_slots;
+        const int rp_ctas = cluster_ctas(k_redist_par, 1, kRpBS, device);
         ra.cap = cap_;
         const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
@@ -799,6 +814,8 @@ struct sdr_solver {
             LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, g, key_cell, hist_valid, cavity, dn(), cap_, rds, cand,
                    (uint32_t)cap);
             LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
+            // long lists only (the replay kernel hands over through the state; otherwise it returns at once)
+            launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
         }
         LAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
         sorted_valid = false;
@@ -874,6 +891,15 @@ struct sdr_solver {
             prof.fluid_cells += hst->nf;
             prof.particles += n_before;
             for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
+        }
+        account_redistribution();
+        time += dt;
+        steps += 1;
+    }
+
+    // Device redistribution counters since the last status read, into the profile.
+    void account_redistribution() {
+        if (profiling) {
             prof.redist_candidates += hst->redist_cand - redist_seen[0];
             prof.redist_sweeps += hst->redist_sweeps - redist_seen[1];
             prof.redist_long_sweeps += hst->redist_long - redist_seen[2];
@@ -881,8 +907,6 @@ struct sdr_solver {
         redist_seen[0] = hst->redist_cand;
         redist_seen[1] = hst->redist_sweeps;
         redist_seen[2] = hst->redist_long;
-        time += dt;
-        steps += 1;
     }
 
     double cfl_dt() const {  // solver.rs:262-281
@@ -945,6 +969,7 @@ struct sdr_solver {
                     for (int q = 0; q < 16; ++q) prof.pcg_section_cycles[q] = hst->pcg_cycles[q];
             }
             if (ph == SDR_PHASE_EXTRAPOLATE) read_grid_speed();
+            if (ph == SDR_PHASE_REDISTRIBUTE) account_redistribution();
         }
     }
 };

@@ -292,32 +292,41 @@ def test_redistribute_moves_exact(pair):
 
 def test_redistribute_long_candidate_list_exact():
     """More over-cap particles than the replay keeps in shared memory (8192):
-    600 cavity cells with 20 particles each, in shuffled index order, so the
-    candidates are put in index order by the long-list path."""
+    24 particles in every cavity cell of even i+j+k and none in the others (a
+    checkerboard, so every over-cap cell has room next to it and no candidate
+    is left out), in shuffled index order. The list is put in index order
+    through the bitmap and the moves are decided in parallel rounds on a
+    cluster (k_redist_par): the same moves as the reference's sequential loop."""
     gpu, orc, res = make_pair()
     nx, ny, nz = gpu.grid_dims
     dx = gpu.dx
     st = gpu.stats()
     org = np.array([st.origin.x, st.origin.y, st.origin.z])
-    cav = np.flatnonzero(gpu.cavity_mask().reshape(-1))[:600]
-    assert len(cav) == 600
+    cav = np.flatnonzero(gpu.cavity_mask().reshape(-1))
     ijk = np.stack([cav % nx, (cav // nx) % ny, cav // (nx * ny)], axis=1)
+    ijk = ijk[ijk.sum(axis=1) % 2 == 0]
+    assert len(ijk) * 24 > 8192
     rng = np.random.default_rng(7)
-    pos = (org + (ijk.repeat(20, axis=0) + 0.5 + rng.uniform(-0.3, 0.3, (600 * 20, 3))) * dx)
+    pos = (org + (ijk.repeat(24, axis=0) + 0.5 + rng.uniform(-0.3, 0.3, (len(ijk) * 24, 3))) * dx)
     pos = f32(pos[rng.permutation(len(pos))])
     vel = np.zeros_like(pos)
     gpu.set_particles(pos, vel)
     orc.set_particles(pos, vel)
     sync_faces(gpu, orc)
+    gpu.set_profiling(True)
     gpu.run_phase(_lib.PHASE_REDISTRIBUTE)
     orc.phase(oracle.PHASE_REDISTRIBUTE)
+    prof = gpu.profile()
     pg, vg = gpu.particles()
     po, vo = orc.particles()
     moved_g = np.any(pg != pos, axis=1)
     moved_o = np.any(po != pos, axis=1)
     d = np.max(np.abs(pg - po), axis=1)
-    record("redistribute_long", {"candidates": int(len(pos)), "moved_gpu": int(moved_g.sum()),
-                                 "moved_orc": int(moved_o.sum()), "max_abs_pos": float(d.max())})
+    record("redistribute_long", {"particles": int(len(pos)), "candidates": prof["redist_candidates"],
+                                 "sweeps": prof["redist_sweeps"], "long_sweeps": prof["redist_long_sweeps"],
+                                 "moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
+                                 "max_abs_pos": float(d.max())})
+    assert prof["redist_long_sweeps"] >= 1
     assert moved_o.sum() > 1000
     assert np.array_equal(moved_g, moved_o)
     assert d.max() < POS_TOL
