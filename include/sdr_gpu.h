@@ -343,6 +343,20 @@ int sdr_surface_nets_volume(const double* values, const uint64_t dims[3], sdr_ve
  * triples). */
 enum { SDR_FORMAT_VTK = 0, SDR_FORMAT_XYZ = 1 };
 /* n points from host memory, xyz interleaved. */
+/* Metrics files. serde_json's to_string_pretty layout: shortest round-trip
+ * digits for every f64 (plain notation with at least one fractional digit for
+ * 1e-5 <= |v| < 1e16, else d.ddde[-]x; null if not finite), two-space indent.
+ * MetricsCollector::write_json (src/metrics.rs:385-391): the frames as a JSON array. */
+int sdr_metrics_write_json(const sdr_metrics* m, const char* path);
+/* MetricsCollector::write_csv (src/metrics.rs:394-431): header + one row per
+ * frame, each value as Rust's `{}` prints it. */
+int sdr_metrics_write_csv(const sdr_metrics* m, const char* path);
+/* The same two files from a caller's array of frames. */
+int sdr_frames_write_json(const sdr_frame_metrics* frames, size_t n, const char* path);
+int sdr_frames_write_csv(const sdr_frame_metrics* frames, size_t n, const char* path);
+/* summary.json of cmd_simulate (src/main.rs:306-310). */
+int sdr_summary_write_json(const sdr_summary* summary, const char* path);
+
 int sdr_write_points(const char* path, int32_t format, const float* xyz, size_t n);
 /* frame_path (output.rs:114-122): "<dir>/<prefix>_<frame, 6 digits>.<vtk|xyz>". */
 int sdr_frame_path(const char* dir, const char* prefix, uint64_t frame, int32_t format, char* out, size_t cap);

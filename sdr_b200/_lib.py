@@ -13,6 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsdr_gpu.so")
 
 SDR_OK = 0
+(SDR_ERR_INVALID, SDR_ERR_CUDA, SDR_ERR_OOM, SDR_ERR_CAPACITY, SDR_ERR_DEVICE_TIMEOUT, SDR_ERR_NO_DEVICE,
+ SDR_ERR_BUFFER, SDR_ERR_IO) = range(1, 9)
 NOALLOC_MAX_TRIANGLES = 32768
 ERRORS = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "CAPACITY", 5: "DEVICE_TIMEOUT", 6: "NO_DEVICE", 7: "BUFFER"}
 
@@ -190,6 +192,11 @@ SIGNATURES = {
     "sdr_sdf_from_mesh_noalloc": (i32, [vp, sz, Vec3, d, P(u64), vp, vp]),
     "sdr_surface_nets_volume": (i32, [P(d), P(u64), Vec3, d, P(d), P(u64)]),
     "sdr_write_points": (i32, [C.c_char_p, C.c_int32, P(C.c_float), sz]),
+    "sdr_metrics_write_json": (i32, [vp, C.c_char_p]),
+    "sdr_metrics_write_csv": (i32, [vp, C.c_char_p]),
+    "sdr_frames_write_json": (i32, [P(FrameMetricsC), sz, C.c_char_p]),
+    "sdr_frames_write_csv": (i32, [P(FrameMetricsC), sz, C.c_char_p]),
+    "sdr_summary_write_json": (i32, [P(SummaryC), C.c_char_p]),
     "sdr_frame_path": (i32, [C.c_char_p, C.c_char_p, u64, C.c_int32, C.c_char_p, sz]),
     "sdr_frame_writer_create": (i32, [C.c_char_p, C.c_char_p, C.c_int32, P(vp)]),
     "sdr_frame_writer_submit": (i32, [vp, vp, u64]),

@@ -1079,6 +1079,11 @@ double* noalloc_scratch() {
 // serving layer report its own failures through sdr_last_error.
 void sdr_internal_set_error(const std::string& msg) { g_err = msg; }
 
+// Metrics files (output.cpp).
+std::string sdr_internal_frames_json(const sdr_frame_metrics* frames, size_t n);
+std::string sdr_internal_frames_csv(const sdr_frame_metrics* frames, size_t n);
+int sdr_internal_write_text(const char* path, const std::string& t, std::string& err);
+
 extern "C" {
 
 int sdr_abi_version(void) { return SDR_ABI_VERSION; }
@@ -1552,6 +1557,24 @@ int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
             throw;
         }
         *out = m;
+    });
+}
+
+int sdr_metrics_write_json(const sdr_metrics* m, const char* path) {
+    return guard([&] {
+        require(m && path, "null argument");
+        std::string err;
+        int rc = sdr_internal_write_text(path, sdr_internal_frames_json(m->history.data(), m->history.size()), err);
+        if (rc != SDR_OK) throw Fail{rc, err};
+    });
+}
+
+int sdr_metrics_write_csv(const sdr_metrics* m, const char* path) {
+    return guard([&] {
+        require(m && path, "null argument");
+        std::string err;
+        int rc = sdr_internal_write_text(path, sdr_internal_frames_csv(m->history.data(), m->history.size()), err);
+        if (rc != SDR_OK) throw Fail{rc, err};
     });
 }
 

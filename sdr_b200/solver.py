@@ -10,7 +10,6 @@ with the SDF voxelised on the device. Every call goes through
 from __future__ import annotations
 
 import ctypes as C
-import json
 import math
 from dataclasses import dataclass
 from typing import Optional
@@ -366,19 +365,19 @@ class MetricsCollector:
         check(_lib.load().sdr_metrics_summary(self._h, C.byref(sm)))
         return sm.to_dict()
 
-    def write_json(self, path: str) -> None:  # metrics.rs:385-391
-        with open(path, "w") as f:
-            json.dump(self.history, f, indent=2)
+    def write_json(self, path: str) -> None:
+        """metrics.json (metrics.rs:385-391), byte for byte as serde_json writes it."""
+        check(_lib.load().sdr_metrics_write_json(self._h, str(path).encode()))
 
-    def write_csv(self, path: str) -> None:  # metrics.rs:394-431
-        keys = ["frame", "time_s", "particles", "fluid_volume_ml", "drained_volume_ml", "fill_fraction",
-                "wall_coverage", "mean_pressure_pa", "max_pressure_pa", "max_pressure_mmhg", "wall_pressure_pa",
-                "peak_wall_pressure_pa", "peak_wall_pressure_mmhg", "membrane_artifacts", "max_speed_m_s",
-                "kinetic_energy", "pcg_iters"]
-        with open(path, "w") as f:
-            f.write(",".join(keys) + "\n")
-            for m in self.history:
-                f.write(",".join(repr(m[k]) if isinstance(m[k], float) else str(m[k]) for k in keys) + "\n")
+    def write_csv(self, path: str) -> None:
+        """metrics.csv (metrics.rs:394-431), values as Rust's `{}` prints them."""
+        check(_lib.load().sdr_metrics_write_csv(self._h, str(path).encode()))
+
+    def write_summary_json(self, path: str) -> None:
+        """summary.json of cmd_simulate (main.rs:306-310)."""
+        sm = _lib.SummaryC()
+        check(_lib.load().sdr_metrics_summary(self._h, C.byref(sm)))
+        check(_lib.load().sdr_summary_write_json(C.byref(sm), str(path).encode()))
 
 
 @dataclass
