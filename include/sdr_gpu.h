@@ -343,6 +343,33 @@ int sdr_surface_nets_volume(const double* values, const uint64_t dims[3], sdr_ve
  * triples). */
 enum { SDR_FORMAT_VTK = 0, SDR_FORMAT_XYZ = 1 };
 /* n points from host memory, xyz interleaved. */
+/* ---------------------------------------------------------------- previews
+ * src/render.rs. SlicePlane (render.rs:45-56): in-plane horizontal and
+ * vertical axes, the axis sliced along (0 = x, 1 = y, 2 = z), the slice
+ * coordinate and the half-thickness of the particle band, whether larger
+ * vertical coordinates go up (flip_v), a silhouette projection instead of a
+ * slice, and the amber pool instead of speed-coloured dots. */
+typedef struct {
+    int32_t hax, vax, oax, flip_v, project, amber;
+    double slice, slab;
+} sdr_slice_plane;
+/* SlicePlane::xy / xz / yz / projected_along_gravity (render.rs:64-136). */
+int sdr_slice_plane_xy(double slice, double slab, sdr_slice_plane* out);
+int sdr_slice_plane_xz(double slice, double slab, sdr_slice_plane* out);
+int sdr_slice_plane_yz(double slice, double slab, sdr_slice_plane* out);
+int sdr_slice_plane_gravity(sdr_vec3 gravity, sdr_slice_plane* out);
+/* render_slice (render.rs:139-236) of the solver's current state, drawn on
+ * the device: RGB8 rows top to bottom into rgb (cap bytes, at least
+ * 3 * w * h; w and h are written first, so a call with rgb = NULL returns
+ * SDR_ERR_BUFFER with the size). vmax <= 0 scales speed to the peak. */
+int sdr_render_slice(sdr_solver* s, const sdr_slice_plane* plane, uint32_t target_px, double vmax, uint8_t* rgb,
+                     size_t cap, uint32_t* w, uint32_t* h);
+/* render_timeseries (render.rs:351-406) of a run's frames. */
+int sdr_render_timeseries(const sdr_frame_metrics* frames, size_t n, uint32_t w, uint32_t h, uint8_t* rgb,
+                          size_t cap);
+/* save_png (render.rs:409-414): 8-bit RGB PNG. */
+int sdr_write_png(const char* path, const uint8_t* rgb, uint32_t w, uint32_t h);
+
 /* Metrics files. serde_json's to_string_pretty layout: shortest round-trip
  * digits for every f64 (plain notation with at least one fractional digit for
  * 1e-5 <= |v| < 1e16, else d.ddde[-]x; null if not finite), two-space indent.

@@ -69,6 +69,11 @@ def _fields(spec):
     return [(n.split(":")[0], C.c_uint64 if n.endswith(":u") else C.c_double) for n in spec]
 
 
+class OrcSlicePlane(C.Structure):  # render.rs:45-56
+    _fields_ = [("hax", C.c_int32), ("vax", C.c_int32), ("oax", C.c_int32), ("flip_v", C.c_int32),
+                ("project", C.c_int32), ("amber", C.c_int32), ("slice", C.c_double), ("slab", C.c_double)]
+
+
 class OrcFrameMetrics(C.Structure):
     _fields_ = _fields(_FM)
 
@@ -157,6 +162,9 @@ def _declare(L):
         "orc_metrics_get_masks": (None, [vp, P(C.c_uint8), P(C.c_uint8)]),
         "orc_membrane_stats": (None, [P(d), C.c_size_t, d, P(d), P(d), P(u64)]),
         "orc_hash_jitter": (None, [u64, P(d)]),
+        "orc_render_slice_dims": (None, [vp, P(OrcSlicePlane), C.c_uint32, P(C.c_uint32), P(C.c_uint32)]),
+        "orc_render_slice": (None, [vp, P(OrcSlicePlane), C.c_uint32, d, P(C.c_uint8)]),
+        "orc_render_timeseries": (None, [P(OrcFrameMetrics), C.c_size_t, C.c_uint32, C.c_uint32, P(C.c_uint8)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -538,6 +546,17 @@ class Solver:
     def max_pressure(self): return lib().orc_solver_max_pressure(self._h)
     def mean_pressure(self): return lib().orc_solver_mean_pressure(self._h)
     def max_speed(self): return lib().orc_solver_max_speed(self._h)
+
+    def render_slice(self, plane: dict, target_px: int, vmax: float = 0.0) -> np.ndarray:
+        """render_slice (render.rs:139-236) as an (h, w, 3) uint8 image; plane has the
+        SlicePlane fields (hax, vax, oax, slice, slab, flip_v, project, amber)."""
+        pl = OrcSlicePlane(**{k: plane[k] for k, _ in OrcSlicePlane._fields_})
+        w, h = C.c_uint32(), C.c_uint32()
+        lib().orc_render_slice_dims(self._h, C.byref(pl), int(target_px), C.byref(w), C.byref(h))
+        img = np.zeros((h.value, w.value, 3), dtype=np.uint8)
+        lib().orc_render_slice(self._h, C.byref(pl), int(target_px), float(vmax),
+                               img.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return img
     def kinetic_energy(self): return lib().orc_solver_kinetic_energy(self._h)
     def max_particles_per_cell(self): return int(lib().orc_solver_max_particles_per_cell(self._h))
     def cells_fluid_count(self): return int(lib().orc_solver_cells_fluid_count(self._h))
@@ -589,3 +608,14 @@ class Metrics:
         b = np.zeros(n, dtype=np.uint8)
         lib().orc_metrics_get_masks(self._h, _u8p(a), _u8p(b))
         return a, b
+
+
+def render_timeseries(frames, width: int, height: int) -> np.ndarray:
+    """render_timeseries (render.rs:351-406): frames are FrameMetrics dicts."""
+    arr = (OrcFrameMetrics * max(len(frames), 1))()
+    for i, f in enumerate(frames):
+        for k, _ in OrcFrameMetrics._fields_:
+            setattr(arr[i], k, f[k])
+    img = np.zeros((height, width, 3), dtype=np.uint8)
+    lib().orc_render_timeseries(arr, len(frames), int(width), int(height), img.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return img

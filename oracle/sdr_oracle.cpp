@@ -1313,6 +1313,108 @@ void membrane_stats(const std::vector<double>& values, double cap, double& mean,
 }  // namespace
 
 // ================================================================= C ABI
+// ---------------------------------------------------------------- render.rs
+// render_slice / render_timeseries (render.rs:139-415) into an RGB8 buffer.
+namespace {
+
+const uint8_t RC_BG[3] = {18, 18, 22};        // render.rs:22-25
+const uint8_t RC_INTERIOR[3] = {232, 236, 244};
+const uint8_t RC_WALL[3] = {44, 44, 54};
+const uint8_t RC_NEEDLE[3] = {255, 80, 80};
+const uint8_t RC_FILM[3] = {242, 178, 92};     // render.rs:31-32
+const uint8_t RC_DEEP[3] = {150, 78, 18};
+
+struct Rgb8 {
+    uint32_t w, h;
+    uint8_t* px;
+    void set(uint32_t x, uint32_t y, const uint8_t c[3]) { std::memcpy(px + 3 * ((size_t)y * w + x), c, 3); }
+    void put(int64_t x, int64_t y, const uint8_t c[3]) {  // render.rs:430-434
+        if (x >= 0 && y >= 0 && (uint64_t)x < w && (uint64_t)y < h) set((uint32_t)x, (uint32_t)y, c);
+    }
+};
+
+int64_t as_i64(double f) {  // Rust `as i64`: truncation, saturating, NaN -> 0
+    if (std::isnan(f)) return 0;
+    if (f >= 9223372036854775807.0) return INT64_MAX;
+    if (f <= -9223372036854775808.0) return INT64_MIN;
+    return (int64_t)f;
+}
+uint8_t as_u8(double f) {  // Rust `as u8`
+    if (std::isnan(f) || f <= 0.0) return 0;
+    if (f >= 255.0) return 255;
+    return (uint8_t)f;
+}
+double clamp01(double t) { return t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t); }
+
+void r_disk(Rgb8& im, int64_t cx, int64_t cy, int64_t r, const uint8_t c[3]) {  // render.rs:436-444
+    for (int64_t dy = -r; dy <= r; ++dy)
+        for (int64_t dx = -r; dx <= r; ++dx)
+            if (dx * dx + dy * dy <= r * r) im.put(cx + dx, cy + dy, c);
+}
+
+void r_line(Rgb8& im, int64_t x0, int64_t y0, int64_t x1, int64_t y1, const uint8_t c[3]) {  // render.rs:447-468
+    int64_t dx = x1 - x0 < 0 ? x0 - x1 : x1 - x0;
+    int64_t dy = -(y1 - y0 < 0 ? y0 - y1 : y1 - y0);
+    int64_t sx = x0 < x1 ? 1 : -1, sy = y0 < y1 ? 1 : -1;
+    int64_t err = dx + dy;
+    for (;;) {
+        im.put(x0, y0, c);
+        if (x0 == x1 && y0 == y1) break;
+        int64_t e2 = 2 * err;
+        if (e2 >= dy) {
+            err += dy;
+            x0 += sx;
+        }
+        if (e2 <= dx) {
+            err += dx;
+            y0 += sy;
+        }
+    }
+}
+
+uint8_t r_lerp(uint8_t a, uint8_t b, double t) {  // render.rs:311-316
+    t = clamp01(t);
+    double v = std::round((double)a * (1.0 - t) + (double)b * t);
+    v = v < 0.0 ? 0.0 : (v > 255.0 ? 255.0 : v);
+    return (uint8_t)v;
+}
+
+void r_speed(double t, uint8_t c[3]) {  // render.rs:417-428
+    t = clamp01(t);
+    double r, g, b;
+    if (t < 0.5) {
+        double u = t / 0.5;
+        r = 0.0; g = u; b = 1.0 - u;
+    } else {
+        double u = (t - 0.5) / 0.5;
+        r = u; g = 1.0 - u; b = 0.0;
+    }
+    c[0] = as_u8(r * 255.0);
+    c[1] = as_u8(g * 255.0);
+    c[2] = as_u8(b * 255.0);
+}
+
+double comp(V3 a, int axis) { return axis == 0 ? a.x : (axis == 1 ? a.y : a.z); }
+
+}  // namespace
+
+static void slice_dims(const orc_solver& s, const orc_slice_plane& p, uint32_t target, uint32_t& w, uint32_t& h,
+                       double mn[3], double mx[3], double& wm, double& hm) {  // render.rs:139-156
+    Aabb bb = s.solid.bounds();
+    mn[0] = bb.min.x; mn[1] = bb.min.y; mn[2] = bb.min.z;
+    mx[0] = bb.max.x; mx[1] = bb.max.y; mx[2] = bb.max.z;
+    wm = fmax_(mx[p.hax] - mn[p.hax], 1e-9);
+    hm = fmax_(mx[p.vax] - mn[p.vax], 1e-9);
+    uint32_t t = target > 1 ? target : 1;
+    if (wm >= hm) {
+        w = t;
+        h = (uint32_t)fmax_(std::round((double)target * hm / wm), 1.0);
+    } else {
+        w = (uint32_t)fmax_(std::round((double)target * wm / hm), 1.0);
+        h = t;
+    }
+}
+
 extern "C" {
 
 void orc_set_threads(int n) { g_threads = n; }
@@ -1819,4 +1921,140 @@ void orc_membrane_stats(const double* values, size_t n, double cap, double* mean
 
 void orc_hash_jitter(uint64_t key, double out[3]) { to(hash_jitter(key), out); }
 
+
+void orc_render_slice_dims(const orc_solver* s, const orc_slice_plane* p, uint32_t target_px, uint32_t* w,
+                           uint32_t* h) {
+    double mn[3], mx[3], wm, hm;
+    slice_dims(*s, *p, target_px, *w, *h, mn, mx, wm, hm);
+}
+
+void orc_render_slice(const orc_solver* s, const orc_slice_plane* pl, uint32_t target_px, double vmax,
+                      uint8_t* rgb) {  // render.rs:139-236
+    const orc_slice_plane& p = *pl;
+    double mn[3], mx[3], wm, hm;
+    uint32_t w, h;
+    slice_dims(*s, p, target_px, w, h, mn, mx, wm, hm);
+    Rgb8 im{w, h, rgb};
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x) im.set(x, y, RC_BG);
+    const double oa_lo = mn[p.oax];
+    const double oa_span = fmax_(mx[p.oax] - mn[p.oax], 1e-9);
+    const int PROJ_SAMPLES = 96;
+    for (uint32_t py = 0; py < h; ++py)
+        for (uint32_t px = 0; px < w; ++px) {  // in_plane_world, render.rs:319-338
+            double wx = mn[p.hax] + ((double)px + 0.5) / (double)w * wm;
+            double wy = p.flip_v ? mx[p.vax] - ((double)py + 0.5) / (double)h * hm
+                                 : mn[p.vax] + ((double)py + 0.5) / (double)h * hm;
+            double c[3] = {0, 0, 0};
+            c[p.hax] = wx;
+            c[p.vax] = wy;
+            bool interior = false;
+            if (p.project) {
+                for (int q = 0; q < PROJ_SAMPLES && !interior; ++q) {
+                    c[p.oax] = oa_lo + ((double)q + 0.5) / (double)PROJ_SAMPLES * oa_span;
+                    interior = s->solid.sample(v3(c[0], c[1], c[2])) < 0.0;
+                }
+            } else {
+                c[p.oax] = p.slice;
+                interior = s->solid.sample(v3(c[0], c[1], c[2])) < 0.0;
+            }
+            im.set(px, py, interior ? RC_INTERIOR : RC_WALL);
+        }
+    auto to_px = [&](V3 a, int64_t& cx, int64_t& cy) {
+        double fx = (comp(a, p.hax) - mn[p.hax]) / wm * (double)w;
+        double fy = p.flip_v ? (mx[p.vax] - comp(a, p.vax)) / hm * (double)h
+                             : (comp(a, p.vax) - mn[p.vax]) / hm * (double)h;
+        cx = as_i64(fx);
+        cy = as_i64(fy);
+    };
+    if (p.amber) {  // draw_amber_pool, render.rs:238-308
+        const double longest = (double)(w > h ? w : h);
+        const int64_t r = as_i64(fmax_(std::round(longest / 80.0), 3.0));
+        const double PEAK = 0.22;
+        const double rr = (double)(r * r);
+        std::vector<double> cov((size_t)w * h, 0.0);
+        for (V3 q : s->pos) {
+            if (std::fabs(comp(q, p.oax) - p.slice) > p.slab) continue;
+            int64_t cx, cy;
+            to_px(q, cx, cy);
+            for (int64_t dy = -r; dy <= r; ++dy)
+                for (int64_t dx = -r; dx <= r; ++dx) {
+                    double d2 = (double)(dx * dx + dy * dy);
+                    if (d2 > rr) continue;
+                    int64_t x = cx + dx, y = cy + dy;
+                    if (x < 0 || y < 0 || (uint64_t)x >= w || (uint64_t)y >= h) continue;
+                    double a = PEAK * (1.0 - d2 / rr);
+                    size_t idx = (size_t)y * w + (size_t)x;
+                    cov[idx] += (1.0 - cov[idx]) * a;
+                }
+        }
+        for (uint32_t py = 0; py < h; ++py)
+            for (uint32_t px = 0; px < w; ++px) {
+                double c = clamp01(cov[(size_t)py * w + px]);
+                if (c <= 1.0 / 255.0) continue;
+                uint8_t amber[3], out[3];
+                const uint8_t* bg = rgb + 3 * ((size_t)py * w + px);
+                for (int k = 0; k < 3; ++k) amber[k] = r_lerp(RC_FILM[k], RC_DEEP[k], c);
+                for (int k = 0; k < 3; ++k) out[k] = r_lerp(bg[k], amber[k], c);
+                im.set(px, py, out);
+            }
+    } else {
+        double vm = vmax > 0.0 ? vmax : fmax_(s->max_speed(), 1e-6);
+        for (size_t i = 0; i < s->pos.size(); ++i) {
+            V3 q = s->pos[i];
+            if (std::fabs(comp(q, p.oax) - p.slice) > p.slab) continue;
+            int64_t cx, cy;
+            to_px(q, cx, cy);
+            uint8_t col[3];
+            r_speed(clamp01(length(s->vel[i]) / vm), col);
+            r_disk(im, cx, cy, 2, col);
+        }
+    }
+    V3 tip = s->needle.tip;  // render.rs:224-231
+    V3 back = tip - s->needle.axis * 0.012;
+    int64_t ax, ay, bx, by;
+    to_px(back, ax, ay);
+    to_px(tip, bx, by);
+    r_line(im, ax, ay, bx, by, RC_NEEDLE);
+    r_disk(im, bx, by, 3, RC_NEEDLE);
+}
+
+void orc_render_timeseries(const orc_frame_metrics* frames, size_t n, uint32_t width, uint32_t height,
+                           uint8_t* rgb) {  // render.rs:351-406
+    Rgb8 im{width, height, rgb};
+    const uint8_t bgc[3] = {250, 250, 252};
+    for (uint32_t y = 0; y < height; ++y)
+        for (uint32_t x = 0; x < width; ++x) im.set(x, y, bgc);
+    const int64_t x0 = 8, x1 = (int64_t)width - 8, y0 = 8, y1 = (int64_t)height - 8;
+    const uint8_t grid[3] = {220, 220, 226}, axis[3] = {120, 120, 130};
+    for (int64_t g = 0; g <= 4; ++g) {
+        int64_t y = y1 - (y1 - y0) * g / 4;
+        r_line(im, x0, y, x1, y, grid);
+    }
+    r_line(im, x0, y0, x0, y1, axis);
+    r_line(im, x0, y1, x1, y1, axis);
+    if (n < 2) return;
+    double peak_p = 0.0;
+    for (size_t i = 0; i < n; ++i) peak_p = fmax_(peak_p, frames[i].peak_wall_pressure_pa);
+    peak_p = fmax_(peak_p, 1e-9);
+    auto map = [&](size_t i, double val, int64_t& px, int64_t& py) {
+        double fx = (double)x0 + (double)(x1 - x0) * (double)i / (double)(n - 1);
+        double v = clamp01(val);
+        double fy = (double)y1 - (double)(y1 - y0) * v;
+        px = as_i64(fx);
+        py = as_i64(fy);
+    };
+    const uint8_t cols[3][3] = {{40, 90, 220}, {30, 160, 60}, {210, 60, 50}};
+    for (int sidx = 0; sidx < 3; ++sidx) {
+        auto f = [&](const orc_frame_metrics& m) {
+            return sidx == 0 ? m.fill_fraction : (sidx == 1 ? m.wall_coverage : m.peak_wall_pressure_pa / peak_p);
+        };
+        for (size_t i = 1; i < n; ++i) {
+            int64_t xa, ya, xb, yb;
+            map(i - 1, f(frames[i - 1]), xa, ya);
+            map(i, f(frames[i]), xb, yb);
+            r_line(im, xa, ya, xb, yb, cols[sidx]);
+        }
+    }
+}
 }  // extern "C"

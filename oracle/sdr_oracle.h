@@ -189,6 +189,17 @@ void orc_membrane_stats(const double* values, size_t n, double cap, double* mean
 /* hash_jitter (solver.rs:916-930) */
 void orc_hash_jitter(uint64_t key, double out[3]);
 
+/* ---- render (src/render.rs) into RGB8 buffers of w*h*3 bytes ---- */
+typedef struct {
+    int32_t hax, vax, oax, flip_v, project, amber;
+    double slice, slab;
+} orc_slice_plane;
+void orc_render_slice_dims(const orc_solver* s, const orc_slice_plane* p, uint32_t target_px, uint32_t* w,
+                           uint32_t* h);
+void orc_render_slice(const orc_solver* s, const orc_slice_plane* p, uint32_t target_px, double vmax,
+                      uint8_t* rgb);
+void orc_render_timeseries(const orc_frame_metrics* frames, size_t n, uint32_t w, uint32_t h, uint8_t* rgb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,11 @@ class Profile(C.Structure):
         return d
 
 
+class SlicePlaneC(C.Structure):
+    _fields_ = [("hax", C.c_int32), ("vax", C.c_int32), ("oax", C.c_int32), ("flip_v", C.c_int32),
+                ("project", C.c_int32), ("amber", C.c_int32), ("slice", C.c_double), ("slab", C.c_double)]
+
+
 _FM = ["frame:u", "time_s", "particles:u", "fluid_volume_ml", "drained_volume_ml", "fill_fraction",
        "wall_coverage", "mean_pressure_pa", "max_pressure_pa", "max_pressure_mmhg", "wall_pressure_pa",
        "peak_wall_pressure_pa", "peak_wall_pressure_mmhg", "membrane_artifacts:u", "max_speed_m_s",
@@ -193,6 +198,13 @@ SIGNATURES = {
     "sdr_surface_nets_volume": (i32, [P(d), P(u64), Vec3, d, P(d), P(u64)]),
     "sdr_write_points": (i32, [C.c_char_p, C.c_int32, P(C.c_float), sz]),
     "sdr_metrics_write_json": (i32, [vp, C.c_char_p]),
+    "sdr_slice_plane_xy": (i32, [d, d, P(SlicePlaneC)]),
+    "sdr_slice_plane_xz": (i32, [d, d, P(SlicePlaneC)]),
+    "sdr_slice_plane_yz": (i32, [d, d, P(SlicePlaneC)]),
+    "sdr_slice_plane_gravity": (i32, [Vec3, P(SlicePlaneC)]),
+    "sdr_render_slice": (i32, [vp, P(SlicePlaneC), C.c_uint32, d, P(C.c_uint8), sz, P(C.c_uint32), P(C.c_uint32)]),
+    "sdr_render_timeseries": (i32, [P(FrameMetricsC), sz, C.c_uint32, C.c_uint32, P(C.c_uint8), sz]),
+    "sdr_write_png": (i32, [C.c_char_p, P(C.c_uint8), C.c_uint32, C.c_uint32]),
     "sdr_metrics_write_csv": (i32, [vp, C.c_char_p]),
     "sdr_frames_write_json": (i32, [P(FrameMetricsC), sz, C.c_char_p]),
     "sdr_frames_write_csv": (i32, [P(FrameMetricsC), sz, C.c_char_p]),

@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
-           "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *sources()]
+           "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *sources(), "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

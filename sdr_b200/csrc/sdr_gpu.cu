@@ -30,6 +30,7 @@
 #include "particles.cuh"
 #include "pressure.cuh"
 #include "pressure_cluster.cuh"
+#include "render.cuh"
 #include "scan.cuh"
 #include "sdf.cuh"
 
@@ -1079,6 +1080,12 @@ double* noalloc_scratch() {
 // serving layer report its own failures through sdr_last_error.
 void sdr_internal_set_error(const std::string& msg) { g_err = msg; }
 
+// Pixel primitives (render.cpp).
+void sdr_internal_draw_disk(uint8_t* rgb, uint32_t w, uint32_t h, int64_t cx, int64_t cy, int64_t r,
+                            const uint8_t c[3]);
+void sdr_internal_draw_line(uint8_t* rgb, uint32_t w, uint32_t h, int64_t x0, int64_t y0, int64_t x1, int64_t y1,
+                            const uint8_t c[3]);
+
 // Metrics files (output.cpp).
 std::string sdr_internal_frames_json(const sdr_frame_metrics* frames, size_t n);
 std::string sdr_internal_frames_csv(const sdr_frame_metrics* frames, size_t n);
@@ -1557,6 +1564,116 @@ int sdr_metrics_create(sdr_solver* s, double cavity_volume, sdr_metrics** out) {
             throw;
         }
         *out = m;
+    });
+}
+
+int sdr_render_slice(sdr_solver* s, const sdr_slice_plane* plane, uint32_t target_px, double vmax, uint8_t* rgb,
+                     size_t cap, uint32_t* w_out, uint32_t* h_out) {
+    return guard([&] {
+        require(s && plane && w_out && h_out, "null argument");
+        const sdr_slice_plane& p = *plane;
+        require(p.hax >= 0 && p.hax < 3 && p.vax >= 0 && p.vax < 3 && p.oax >= 0 && p.oax < 3 && p.hax != p.vax &&
+                    p.hax != p.oax && p.vax != p.oax,
+                "slice plane axes must be a permutation of 0, 1, 2");
+        DeviceScope ds(s->device);
+        // image size (render.rs:139-156) from the solid SDF's bounds
+        RenderView v{};
+        v.hax = p.hax; v.vax = p.vax; v.oax = p.oax;
+        v.flip_v = p.flip_v ? 1 : 0; v.project = p.project ? 1 : 0; v.amber = p.amber ? 1 : 0;
+        v.slice = p.slice; v.slab = p.slab;
+        const double org[3] = {s->sox, s->soy, s->soz};
+        const int nn[3] = {s->snx, s->sny, s->snz};
+        for (int a = 0; a < 3; ++a) {
+            v.mn[a] = org[a];
+            v.mx[a] = org[a] + (double)(nn[a] - 1) * s->sdx;
+        }
+        v.wm = std::fmax(v.mx[v.hax] - v.mn[v.hax], 1e-9);
+        v.hm = std::fmax(v.mx[v.vax] - v.mn[v.vax], 1e-9);
+        const uint32_t t = target_px > 1 ? target_px : 1;
+        if (v.wm >= v.hm) {
+            v.w = t;
+            v.h = (uint32_t)std::fmax(std::round((double)target_px * v.hm / v.wm), 1.0);
+        } else {
+            v.w = (uint32_t)std::fmax(std::round((double)target_px * v.wm / v.hm), 1.0);
+            v.h = t;
+        }
+        *w_out = v.w;
+        *h_out = v.h;
+        const size_t npx = (size_t)v.w * v.h;
+        if (!rgb || cap < 3 * npx)
+            throw Fail{SDR_ERR_BUFFER, "image buffer too small: need " + std::to_string(3 * npx) + " bytes"};
+        cudaStream_t st = s->st;
+        uint8_t* img = nullptr;
+        dalloc(img, 3 * npx, st);
+        LAUNCH(k_render_bg, blocks(npx, 256), 256, 0, st, v, s->sdf_d(), img);
+        const uint32_t n = s->n;
+        uint32_t *owner = nullptr, *key = nullptr, *hist = nullptr, *start = nullptr, *fill = nullptr,
+                 *perm = nullptr, *longl = nullptr, *tmp = nullptr, *lcount = nullptr;
+        unsigned long long* peak = nullptr;
+        int2* cxy = nullptr;
+        if (v.amber) {  // draw_amber_pool (render.rs:238-308)
+            const double longest = (double)std::max(v.w, v.h);
+            const int r = (int)std::fmax(std::round(longest / 80.0), 3.0);
+            const int T = r;
+            const int ntx = (int)((v.w + T - 1) / T), nty = (int)((v.h + T - 1) / T);
+            const uint32_t nb = (uint32_t)(ntx + 2) * (uint32_t)(nty + 2) + 1;  // with the dump bin
+            dalloc(hist, nb + 1, st);
+            dalloc(start, nb + 1, st);
+            dalloc(fill, nb, st);
+            dalloc(longl, nb, st);
+            dalloc(lcount, 1, st);
+            dalloc(key, n, st);
+            dalloc(cxy, n, st);
+            dalloc(perm, n, st);
+            dalloc(tmp, n, st);
+            CK(cudaMemsetAsync(hist, 0, (nb + 1) * 4, st));
+            CK(cudaMemsetAsync(lcount, 0, 4, st));
+            if (n) LAUNCH(k_render_amber_keys, blocks(n, 256), 256, 0, st, v, s->pos, n, T, ntx, nty, key, cxy, hist);
+            s->scan(hist, start, nb + 1, nullptr);
+            CK(cudaMemcpyAsync(fill, start, nb * 4, cudaMemcpyDeviceToDevice, st));
+            if (n) LAUNCH(k_sort_scatter, blocks(n, 256), 256, 0, st, key, n, fill, perm);
+            LAUNCH(k_sort_segments, blocks(nb, 256), 256, 0, st, start, nb, perm, longl, lcount);
+            LAUNCH(k_sort_long, 148, 256, 0, st, start, longl, lcount, perm, tmp);
+            LAUNCH(k_render_amber_pixels, blocks(npx, 256), 256, 0, st, v, r, T, ntx, start, perm, cxy, img);
+        } else {  // speed-coloured dots (render.rs:201-221)
+            dalloc(owner, npx, st);
+            dalloc(peak, 1, st);
+            CK(cudaMemsetAsync(owner, 0, npx * 4, st));
+            CK(cudaMemsetAsync(peak, 0, 8, st));
+            if (n && !(vmax > 0.0)) LAUNCH(k_render_max_speed, blocks(n, 256), 256, 0, st, s->vel, n, peak);
+            if (n) LAUNCH(k_render_dots_mark, blocks(n, 256), 256, 0, st, v, s->pos, n, owner);
+            LAUNCH(k_render_dots_color, blocks(npx, 256), 256, 0, st, v, s->vel, owner, peak, vmax, img);
+        }
+        copy_dev(s, img, 3 * npx, rgb);
+        for (auto* q : {owner, key, hist, start, fill, perm, longl, tmp, lcount}) {
+            uint32_t* qq = q;
+            dfree(qq, st);
+        }
+        dfree(peak, st);
+        dfree(cxy, st);
+        dfree(img, st);
+        // the needle on top (render.rs:224-231): a 12 mm segment behind the tip and a disk at it
+        auto to_px = [&](double x, double y, double z, int64_t& cx, int64_t& cy) {
+            const double a[3] = {x, y, z};
+            const double fx = (a[v.hax] - v.mn[v.hax]) / v.wm * (double)v.w;
+            const double fy = v.flip_v ? (v.mx[v.vax] - a[v.vax]) / v.hm * (double)v.h
+                                       : (a[v.vax] - v.mn[v.vax]) / v.hm * (double)v.h;
+            auto cvt = [](double f) -> int64_t {
+                if (std::isnan(f)) return 0;
+                if (f >= 9223372036854775807.0) return INT64_MAX;
+                if (f <= -9223372036854775808.0) return INT64_MIN;
+                return (int64_t)f;
+            };
+            cx = cvt(fx);
+            cy = cvt(fy);
+        };
+        const sdr_vec3 tip = s->needle.tip, ax = s->needle.axis;
+        int64_t bx0, by0, tx0, ty0;
+        to_px(tip.x - ax.x * 0.012, tip.y - ax.y * 0.012, tip.z - ax.z * 0.012, bx0, by0);
+        to_px(tip.x, tip.y, tip.z, tx0, ty0);
+        const uint8_t needle[3] = {255, 80, 80};
+        sdr_internal_draw_line(rgb, v.w, v.h, bx0, by0, tx0, ty0, needle);
+        sdr_internal_draw_disk(rgb, v.w, v.h, tx0, ty0, 3, needle);
     });
 }
 
