@@ -28,6 +28,10 @@ through the public calls (the plain path), all at once (sdr_batch_run), and as
 Poisson arrivals into the request server (sdr_server_*, 150 GB admission
 budget) with p50/p99 time-to-summary.
 
+``render``: preview images (render_slice, 600 px) of the final state, the
+slice through the needle tip and the gravity projection, timed through the
+public call, beside the oracle drawing the same state.
+
 ``large`` (one GPU): the 0.2 mm parametric cavity (207 x 217 x 161 cells)
 with a pre-seeded pool of 9.5 M particles at rest, ``--large-substeps``
 substeps at the fixed jet CFL step after ``--large-warmup``, device-timed;
@@ -219,6 +223,35 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
     }
 
 
+def render_bench(solver, w, sdf, cpu: bool, px: int = 600, reps: int = 5) -> dict:
+    """Preview images (render_slice) of the solver's current state: the slice
+    through the needle tip (speed dots) and the gravity projection (amber
+    pool), public call to host image; the oracle draws the same state."""
+    from sdr_b200.render import SlicePlane, render_slice
+    planes = {"slice": SlicePlane.xy(w.res.needle.tip[2], w.res.sim_dx),
+              "gravity": SlicePlane.projected_along_gravity(w.res.fluid.gravity)}
+    out = {"px": px, "particles": len(solver)}
+    imgs = {}
+    for name, plane in planes.items():
+        imgs[name] = render_slice(solver, plane, px)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            render_slice(solver, plane, px)
+        out[f"{name}_ms"] = 1e3 * (time.perf_counter() - t0) / reps
+    if cpu:
+        orc = oracle_for(w, sdf)
+        pos, vel = solver.particles()
+        orc.set_particles(pos, vel)
+        same = True
+        for name, plane in planes.items():
+            t0 = time.perf_counter()
+            ref = orc.render_slice(plane.as_dict(), px)
+            out[f"cpu_{name}_ms"] = 1e3 * (time.perf_counter() - t0)
+            same = same and bool((ref == imgs[name]).all())
+        out["identical_to_oracle"] = same
+    return {"render": out}
+
+
 def large_bench(n_sub: int, warm: int, cpu: bool) -> dict:
     """The 0.2 mm parametric cavity (207 x 217 x 161 cells) with a pre-seeded
     pool: the deepest cavity cells filled at 8 particles per cell with
@@ -403,6 +436,8 @@ def main():
                                 "sample": f"{csub} substeps from the GPU state one frame after the timed frames "
                                           f"({cps} particle-substeps, {ct:.1f} s); C++ restatement of the "
                                           "reference solver, f64, rayon-parallel parts on all host threads"}
+    if rank == 0 and world == 1:
+        line.update(render_bench(solver, w, sdf, cpu=not args.no_cpu))
     if rank == 0 and world == 1 and not args.no_batch and args.batch_scenes > 0:
         solver.close()
         line.update(batch_bench(args.batch_scenes, args.batch_cfl))

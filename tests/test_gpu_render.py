@@ -73,3 +73,32 @@ def test_render_fixed_vmax_and_determinism(state):
     assert np.array_equal(a, orc.render_slice(plane.as_dict(), 300, 2.0))
     g = _planes(res)["gravity"]
     assert np.array_equal(render_slice(gpu, g, 300), render_slice(gpu, g, 300))  # render.rs:558-565
+
+
+def test_render_dense_pool_matches_oracle():
+    """16 particles in every cavity cell (tiles far beyond the short-segment
+    sort) plus particles off the image (beyond the margin tiles and partly
+    covering the edges), random velocities: amber pool and dots match."""
+    from tests.gpu_common import f32
+    gpu, orc, res = make_pair(SHORT_RUN)
+    nx, ny, nz = gpu.grid_dims
+    dx = gpu.dx
+    st = gpu.stats()
+    org = np.array([st.origin.x, st.origin.y, st.origin.z])
+    cav = np.flatnonzero(gpu.cavity_mask().reshape(-1))
+    ijk = np.stack([cav % nx, (cav // nx) % ny, cav // (nx * ny)], axis=1)
+    rng = np.random.default_rng(9)
+    pos = org + (ijk.repeat(16, axis=0) + 0.5 + rng.uniform(-0.45, 0.45, (len(ijk) * 16, 3))) * dx
+    span = np.array([nx, ny, nz]) * dx
+    outside = org + rng.uniform(-0.3, 1.3, (500, 3)) * span  # some off the image, some near its edges
+    pos = f32(np.concatenate([pos, outside]))
+    vel = f32(rng.normal(0.0, 0.5, pos.shape))
+    gpu.set_particles(pos, vel)
+    orc.set_particles(pos, vel)
+    for name, plane in _planes(res).items():
+        for px in (300, 600):
+            got = render_slice(gpu, plane, px, 0.0)
+            ref = orc.render_slice(plane.as_dict(), px, 0.0)
+            diff = int((got != ref).any(axis=2).sum())
+            record(f"render_dense_{name}_{px}", {"particles": int(len(pos)), "pixels_differing": diff})
+            assert diff == 0, (name, px)
