@@ -464,6 +464,7 @@ __global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const 
 constexpr int kRedistTable = 4096;   // shared-memory hash slots (power of two)
 constexpr int kRedistBS = 1024;
 constexpr int kRedistSmemCand = 8192;  // candidates sorted and replayed in shared memory
+constexpr uint32_t kResolved = 0x80000000u;  // candidate-list flag: decided (particle indices are < 2^31)
 
 struct RedistArgs {
     Grid g;
@@ -514,7 +515,8 @@ __device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761
 // memory, thread 0 replays against the global counts (same result, slower).
 __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     extern __shared__ __align__(16) unsigned char rsm[];
-    int* tkey = (int*)rsm;                                  // kRedistTable
+    unsigned long long* tclaim = (unsigned long long*)rsm;  // kRedistTable: claim stamps of the rounds
+    int* tkey = (int*)(tclaim + kRedistTable);              // kRedistTable
     uint32_t* tcnt = (uint32_t*)(tkey + kRedistTable);      // kRedistTable
     uint32_t* scand = tcnt + kRedistTable;                  // kRedistSmemCand
     short* slots = (short*)(scand + kRedistSmemCand);       // 7 per candidate
@@ -587,7 +589,10 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     }
     const uint32_t* cl = in_smem ? scand : a.cand;
     // ---- hash table of referenced cells
-    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) tkey[s] = -1;
+    for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) {
+        tkey[s] = -1;
+        tclaim[s] = 0ull;
+    }
     if (threadIdx.x == 0) {
         overflow = in_smem ? 0 : 1;
         s_nm = 0;
@@ -627,40 +632,94 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
         }
     }
     __syncthreads();
-    // ---- sequential decisions
-    if (threadIdx.x == 0) {
-        const uint32_t cap = a.cap;
-        uint32_t nm = 0;
-        if (!overflow) {
-            for (uint32_t m = 0; m < nc; ++m) {
+    // ---- decisions. The reference's loop (solver.rs:476-555) in index order,
+    // replayed in parallel rounds (the rule of k_redist_par below, on the
+    // shared-memory table): every pending candidate claims its cell's slot and
+    // the slots of its neighbours below the cap with a stamp ordering lower
+    // indices first, and runs once it holds all of them. The cells such
+    // candidates touch are disjoint, so the moves are the sequential ones.
+    const uint32_t cap = a.cap;
+    if (!overflow) {
+        for (uint32_t round = 1;; ++round) {
+            const unsigned long long stamp = (unsigned long long)round << 32;
+            for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
+                const uint32_t p = scand[m];
+                if (p & kResolved) continue;
                 const short* sl = slots + (size_t)m * 7;
-                int s0 = sl[0];
-                if (tcnt[s0] <= cap) continue;
+                const int s0 = sl[0];
+                if (tcnt[s0] <= cap) {  // back at the cap: stays there for this sweep
+                    scand[m] = p | kResolved;
+                    continue;
+                }
+                const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+                bool any = false;
+#pragma unroll
+                for (int q = 1; q < 7; ++q) {
+                    const int sq = sl[q];
+                    if (sq >= 0 && tcav[sq] && tcnt[sq] < cap) {
+                        atomicMax(tclaim + sq, key);
+                        any = true;
+                    }
+                }
+                if (!any) {  // no neighbour with room now, none later
+                    scand[m] = p | kResolved;
+                    continue;
+                }
+                atomicMax(tclaim + s0, key);
+            }
+            __syncthreads();
+            int pend = 0;
+            for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
+                const uint32_t p = scand[m];
+                if (p & kResolved) continue;
+                const short* sl = slots + (size_t)m * 7;
+                const int s0 = sl[0];
+                const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+                bool ready = tclaim[s0] == key;
+                uint32_t cnt[6];
+#pragma unroll
+                for (int q = 1; q < 7; ++q) {
+                    const int sq = sl[q];
+                    cnt[q - 1] = (sq >= 0 && tcav[sq]) ? tcnt[sq] : 0xFFFFFFFFu;
+                    if (cnt[q - 1] < cap && tclaim[sq] != key) ready = false;
+                }
+                if (!ready) {
+                    pend = 1;
+                    continue;
+                }
                 int best = -1;
                 double best_down = -INFINITY;
                 uint32_t best_room = 0;
 #pragma unroll
-                for (int q = 1; q < 7; ++q) {
-                    int s = sl[q];
-                    if (s < 0) continue;
-                    if (!tcav[s] || tcnt[s] >= cap) continue;
-                    uint32_t room = cap - tcnt[s];
-                    double dn = a.down[q - 1];
+                for (int q = 1; q < 7; ++q) {  // most downhill, then emptiest, then visit order
+                    if (cnt[q - 1] >= cap) continue;
+                    const uint32_t room = cap - cnt[q - 1];
+                    const double dn = a.down[q - 1];
                     if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                        best = s;
+                        best = sl[q];
                         best_down = dn;
                         best_room = room;
                     }
                 }
-                if (best >= 0) {
-                    tcnt[s0] -= 1;
-                    tcnt[best] += 1;
-                    a.moves[2 * nm] = cl[m];
-                    a.moves[2 * nm + 1] = (uint32_t)tkey[best];
-                    ++nm;
-                }
+                scand[m] = p | kResolved;
+                if (best < 0) continue;  // its last neighbour with room was filled this round by a lower candidate
+                tcnt[s0] -= 1;
+                tcnt[best] += 1;
+                const uint32_t slot = atomicAdd(&s_nm, 1u);
+                a.moves[2 * slot] = p;
+                a.moves[2 * slot + 1] = (uint32_t)tkey[best];
             }
-        } else {
+            if (__syncthreads_count(pend) == 0) break;
+            if (round > nc) {  // cannot happen: the lowest pending candidate always runs
+                if (threadIdx.x == 0) atomicOr(&rs->err, 4u);
+                break;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        uint32_t nm = s_nm;
+        if (overflow) {
             uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
             for (uint32_t m = 0; m < nc; ++m) {
                 int c = a.key_cell[cl[m]];
@@ -708,8 +767,8 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     for (uint32_t mv = threadIdx.x; mv < nm; mv += blockDim.x) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
 }
 
-constexpr size_t kRedistSmem = (size_t)kRedistTable * 4 * 2 + (size_t)kRedistSmemCand * 4 +
-                               (size_t)kRedistSmemCand * 7 * 2 + kRedistTable;
+constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable * 4 * 2 +
+                               (size_t)kRedistSmemCand * 4 + (size_t)kRedistSmemCand * 7 * 2 + kRedistTable;
 
 // ---------------------------------------------------------------------------
 // Long candidate lists: the reference's sequential loop (solver.rs:476-555)
@@ -730,7 +789,6 @@ constexpr size_t kRedistSmem = (size_t)kRedistTable * 4 * 2 + (size_t)kRedistSme
 // again and leave the list. The lowest pending candidate always runs, so the
 // rounds end; a bound on them still records an error bit if they did not.
 constexpr int kRpBS = 512;
-constexpr uint32_t kResolved = 0x80000000u;
 
 __device__ __forceinline__ double rp_cluster_sum(double v, double* slots, int& parity, double* sh) {
     double bs = block_sum<kRpBS>(v, sh);
