@@ -175,25 +175,33 @@ __device__ __forceinline__ double corner_w(double gcoord, int n, int node) {
     return d == 0 ? dsub(1.0, f) : (d == 1 ? f : -1.0);
 }
 
-// One thread per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]; it owns the u, v
-// and w faces with that index. It visits the 27 cells around the node in
-// fixed (k, j, i) order — for each (k, j) the three cells i-1..i+1 are one
-// contiguous run of the sorted records — and, within a cell, particles in
-// ascending index, accumulating the trilinear_scatter weights (grid.rs:52-88,
-// w = wx*wy*wz) in f64. Then it normalises (solver.rs:944-952), saves the FLIP
-// copy (save_grid), and optionally adds gravity and zeroes solid faces.
+// Eight lanes per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]; the node owns
+// the u, v and w faces with that index. The lanes split the particles of the
+// 27 cells around the node — for each (k, j) the three cells i-1..i+1 are one
+// contiguous run of the sorted records, and lane l takes every eighth record
+// of each run from the l-th — accumulating the trilinear_scatter weights
+// (grid.rs:52-88, w = wx*wy*wz) in f64; a fixed xor tree of shuffles then
+// adds the eight partial sums (the same bits in every lane: each step adds the
+// same pair). The order is fixed, so the result is deterministic; busy nodes
+// (the jet clump) no longer hold their warp for hundreds of sequential
+// particles. Lane 0 normalises (solver.rs:944-952), saves the FLIP copy
+// (save_grid), and optionally adds gravity and zeroes solid faces.
+constexpr int kP2GLanes = 8;
 __global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
     const Grid& g = a.g;
-    int i, j, k;
-    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-    const bool hu = j < g.ny && k < g.nz, hv = i < g.nx && k < g.nz, hw = i < g.nx && j < g.ny;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = (int)(t % kP2GLanes);
+    int i = 0, j = 0, k = 0;
+    const bool node = node_of(g, t / kP2GLanes, i, j, k);  // no early return: the group shuffles below
+    const bool hu = node && j < g.ny && k < g.nz, hv = node && i < g.nx && k < g.nz,
+               hw = node && i < g.nx && j < g.ny;
     double su = 0, wu = 0, sv = 0, wv = 0, sw = 0, ww = 0;
     const int ci0 = max(i - 1, 0), ci1 = min(i + 1, g.nx - 1);
-    for (int ck = max(k - 1, 0); ck <= min(k + 1, g.nz - 1); ++ck)
+    for (int ck = max(k - 1, 0); node && ck <= min(k + 1, g.nz - 1); ++ck)
         for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj) {
             uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx;
             uint32_t s0 = a.start[c + ci0], s1 = a.start[c + ci1 + 1];
-            for (uint32_t s = s0; s < s1; ++s) {
+            for (uint32_t s = s0 + lane; s < s1; s += kP2GLanes) {
                 double4 l = a.lrec[s];
                 float4 vel = a.vrec[s];
                 if (hu) {
@@ -225,6 +233,16 @@ __global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
                 }
             }
         }
+#pragma unroll
+    for (int o = kP2GLanes / 2; o > 0; o >>= 1) {
+        su = dadd(su, __shfl_xor_sync(0xffffffffu, su, o, kP2GLanes));
+        wu = dadd(wu, __shfl_xor_sync(0xffffffffu, wu, o, kP2GLanes));
+        sv = dadd(sv, __shfl_xor_sync(0xffffffffu, sv, o, kP2GLanes));
+        wv = dadd(wv, __shfl_xor_sync(0xffffffffu, wv, o, kP2GLanes));
+        sw = dadd(sw, __shfl_xor_sync(0xffffffffu, sw, o, kP2GLanes));
+        ww = dadd(ww, __shfl_xor_sync(0xffffffffu, ww, o, kP2GLanes));
+    }
+    if (lane != 0) return;
     if (hu) {
         size_t f = ((size_t)k * g.ny + j) * (g.nx + 1) + i;
         float val = wu > 1e-12 ? (float)ddiv(su, wu) : 0.0f;

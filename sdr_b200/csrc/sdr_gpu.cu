@@ -613,7 +613,7 @@ struct sdr_solver {
         a.gdt[2] = fluid.gravity.z * dt;
         a.add_forces = fused;
         a.enforce = fused;
-        LAUNCH(k_p2g, blocks(nnodes(), kBS), kBS, 0, st, a);
+        LAUNCH(k_p2g, blocks(nnodes() * kP2GLanes, kBS), kBS, 0, st, a);
     }
 
     void add_forces(double dt) {  // solver.rs:593-604
