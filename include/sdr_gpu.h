@@ -93,6 +93,10 @@ typedef struct {
 /* The host thread sleeps while it waits for the solver's stream (instead of
  * spinning): for many solvers driven by more host threads than cores. */
 #define SDR_SOLVER_BLOCKING_SYNC 1
+/* The GPU is shared with other scenes (batches, the request server): every
+ * pressure solve holds one SM instead of a cluster of them. Results are the
+ * same either way. */
+#define SDR_SOLVER_SHARED_GPU 2
 
 /* Solver's public scalar fields (src/solver.rs:143-167) plus GPU-side counters. */
 typedef struct {
@@ -205,19 +209,26 @@ int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
  * (fixed 4096-cell chunks summed sequentially, partials in chunk order,
  * src/pressure.rs:588-603) — pressure and iteration counts then equal the
  * reference's bit for bit given the same right-hand side. 0 (default): a fixed
- * block-tree order — deterministic run to run, faster, differing from the
+ * tree order (cells in wavefront order in 256-cell tiles, each added by a
+ * fixed lane pattern and shuffle tree, the tiles likewise) — deterministic,
+ * independent of the kernel and its CTA count, faster, differing from the
  * reference in the last bits of each dot. */
 int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
-/* Pressure-solve kernel. SDR_PCG_ONE_BLOCK: one persistent block on one SM
- * (lowest latency per wavefront level; the choice for small fluid regions).
+/* Pressure-solve kernel. SDR_PCG_ONE_BLOCK: the MIC(0) wavefront sweeps on
+ * one SM (lowest latency per level; the choice for small fluid regions), the
+ * matvec, updates and dots on a cluster (sdr_solver_set_pcg_ctas).
  * SDR_PCG_CLUSTER: one thread-block cluster of up to 16 SMs, each level of
- * the MIC(0) sweeps spread over all of them (large fluid regions). Both run
- * the same per-cell arithmetic (pressure.rs:341-609); with the reference dot
- * order both equal the reference bit for bit. With the default tree order the
- * dot rounding differs between the two. SDR_PCG_AUTO (default): the cluster
- * from 200,000 fluid cells in the previous solve. */
+ * the sweeps spread over all of them (large fluid regions). Both run the same
+ * per-cell arithmetic (pressure.rs:341-609) and the same dot orders, so they
+ * give the same pressure bits (with the reference dot order, the
+ * reference's). SDR_PCG_AUTO (default): the cluster from 200,000 fluid cells
+ * in the previous solve. */
 enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2 };
 int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel);
+/* CTAs of the SDR_PCG_ONE_BLOCK solve's cluster (CTA 0 runs the sweeps).
+ * 0 (default): 1 with SDR_SOLVER_SHARED_GPU, else the largest cluster the
+ * device schedules. Results do not depend on it. */
+int sdr_solver_set_pcg_ctas(sdr_solver* s, int ctas);
 /* Phase-group timing with CUDA events (adds one event record per group):
  * on = 1. on = 2 also turns on the section timers inside the pressure-solve
  * kernel (pcg_section_cycles), which cost a little on its critical path. */

@@ -62,6 +62,7 @@ class SolverOptions(C.Structure):
 
 
 SOLVER_BLOCKING_SYNC = 1
+SOLVER_SHARED_GPU = 2
 PCG_AUTO, PCG_ONE_BLOCK, PCG_CLUSTER = 0, 1, 2
 
 
@@ -168,6 +169,7 @@ SIGNATURES = {
     "sdr_solver_set_scalars": (i32, [vp, d, d, u64, u64, u64]),
     "sdr_solver_set_dot_order": (i32, [vp, i32]),
     "sdr_solver_set_pcg_kernel": (i32, [vp, i32]),
+    "sdr_solver_set_pcg_ctas": (i32, [vp, i32]),
     "sdr_solver_set_profiling": (i32, [vp, i32]),
     "sdr_solver_get_profile": (i32, [vp, P(Profile)]),
     "sdr_solver_reset_profile": (i32, [vp]),

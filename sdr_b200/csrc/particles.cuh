@@ -175,74 +175,11 @@ __device__ __forceinline__ double corner_w(double gcoord, int n, int node) {
     return d == 0 ? dsub(1.0, f) : (d == 1 ? f : -1.0);
 }
 
-// Eight lanes per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]; the node owns
-// the u, v and w faces with that index. The lanes split the particles of the
-// 27 cells around the node — for each (k, j) the three cells i-1..i+1 are one
-// contiguous run of the sorted records, and lane l takes every eighth record
-// of each run from the l-th — accumulating the trilinear_scatter weights
-// (grid.rs:52-88, w = wx*wy*wz) in f64; a fixed xor tree of shuffles then
-// adds the eight partial sums (the same bits in every lane: each step adds the
-// same pair). The order is fixed, so the result is deterministic; busy nodes
-// (the jet clump) no longer hold their warp for hundreds of sequential
-// particles. Lane 0 normalises (solver.rs:944-952), saves the FLIP copy
-// (save_grid), and optionally adds gravity and zeroes solid faces.
-constexpr int kP2GLanes = 8;
-__global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
+// Normalise (solver.rs:944-952), save the FLIP copy (save_grid), optionally
+// add gravity and zero solid faces: the faces owned by node (i, j, k).
+__device__ __forceinline__ void p2g_store(const P2GArgs& a, int i, int j, int k, bool hu, bool hv, bool hw,
+                                          double su, double wu, double sv, double wv, double sw, double ww) {
     const Grid& g = a.g;
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = (int)(t % kP2GLanes);
-    int i = 0, j = 0, k = 0;
-    const bool node = node_of(g, t / kP2GLanes, i, j, k);  // no early return: the group shuffles below
-    const bool hu = node && j < g.ny && k < g.nz, hv = node && i < g.nx && k < g.nz,
-               hw = node && i < g.nx && j < g.ny;
-    double su = 0, wu = 0, sv = 0, wv = 0, sw = 0, ww = 0;
-    const int ci0 = max(i - 1, 0), ci1 = min(i + 1, g.nx - 1);
-    for (int ck = max(k - 1, 0); node && ck <= min(k + 1, g.nz - 1); ++ck)
-        for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj) {
-            uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx;
-            uint32_t s0 = a.start[c + ci0], s1 = a.start[c + ci1 + 1];
-            for (uint32_t s = s0 + lane; s < s1; s += kP2GLanes) {
-                double4 l = a.lrec[s];
-                float4 vel = a.vrec[s];
-                if (hu) {
-                    double wx = corner_w(l.x, g.nx + 1, i), wy = corner_w(l.y - 0.5, g.ny, j),
-                           wz = corner_w(l.z - 0.5, g.nz, k);
-                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
-                        double wgt = dmul(dmul(wx, wy), wz);
-                        su = dadd(su, dmul(wgt, (double)vel.x));
-                        wu = dadd(wu, wgt);
-                    }
-                }
-                if (hv) {
-                    double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y, g.ny + 1, j),
-                           wz = corner_w(l.z - 0.5, g.nz, k);
-                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
-                        double wgt = dmul(dmul(wx, wy), wz);
-                        sv = dadd(sv, dmul(wgt, (double)vel.y));
-                        wv = dadd(wv, wgt);
-                    }
-                }
-                if (hw) {
-                    double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y - 0.5, g.ny, j),
-                           wz = corner_w(l.z, g.nz + 1, k);
-                    if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
-                        double wgt = dmul(dmul(wx, wy), wz);
-                        sw = dadd(sw, dmul(wgt, (double)vel.z));
-                        ww = dadd(ww, wgt);
-                    }
-                }
-            }
-        }
-#pragma unroll
-    for (int o = kP2GLanes / 2; o > 0; o >>= 1) {
-        su = dadd(su, __shfl_xor_sync(0xffffffffu, su, o, kP2GLanes));
-        wu = dadd(wu, __shfl_xor_sync(0xffffffffu, wu, o, kP2GLanes));
-        sv = dadd(sv, __shfl_xor_sync(0xffffffffu, sv, o, kP2GLanes));
-        wv = dadd(wv, __shfl_xor_sync(0xffffffffu, wv, o, kP2GLanes));
-        sw = dadd(sw, __shfl_xor_sync(0xffffffffu, sw, o, kP2GLanes));
-        ww = dadd(ww, __shfl_xor_sync(0xffffffffu, ww, o, kP2GLanes));
-    }
-    if (lane != 0) return;
     if (hu) {
         size_t f = ((size_t)k * g.ny + j) * (g.nx + 1) + i;
         float val = wu > 1e-12 ? (float)ddiv(su, wu) : 0.0f;
@@ -266,6 +203,103 @@ __global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a) {
         if (a.add_forces && a.gdt[2] != 0.0) val = (float)dadd((double)val, a.gdt[2]);
         if (a.enforce && (solid_at(g, a.cells, i, j, k - 1) || solid_at(g, a.cells, i, j, k))) val = 0.0f;
         a.w[f] = val;
+    }
+}
+
+
+// P2G, first pass: one thread per grid node (i,j,k) in [0,nx]x[0,ny]x[0,nz]
+// (the node owns the u, v and w faces with that index). A node with no
+// particle in the 27 cells around it gets its faces at once (all sums +0);
+// the others are queued for k_p2g.
+__global__ void __launch_bounds__(kBS) k_p2g_nodes(P2GArgs a, uint32_t* __restrict__ list,
+                                                   uint32_t* __restrict__ count) {
+    const Grid& g = a.g;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!node_of(g, t, i, j, k)) return;
+    uint32_t cnt = 0;
+    const int ci0 = max(i - 1, 0), ci1 = min(i + 1, g.nx - 1);
+    for (int ck = max(k - 1, 0); ck <= min(k + 1, g.nz - 1); ++ck)
+        for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj) {
+            const uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx;
+            cnt += a.start[c + ci1 + 1] - a.start[c + ci0];
+        }
+    if (cnt) list[atomicAdd(count, 1u)] = (uint32_t)t;
+    else p2g_store(a, i, j, k, j < g.ny && k < g.nz, i < g.nx && k < g.nz, i < g.nx && j < g.ny, 0, 0, 0, 0, 0, 0);
+}
+
+// P2G gather of the queued nodes, eight lanes each. The lanes split the
+// particles of the 27 cells around the node — for each (k, j) the three cells
+// i-1..i+1 are one contiguous run of the sorted records, and lane l takes
+// every eighth record of each run from the l-th — accumulating the
+// trilinear_scatter weights (grid.rs:52-88, w = wx*wy*wz) in f64; a fixed
+// xor tree of shuffles then adds the eight partial sums (the same bits in
+// every lane: each step adds the same pair). The order is fixed, so the
+// result is deterministic; busy nodes (the jet clump) do not hold their warp
+// for hundreds of sequential particles. The loop over the queue takes the
+// same trips in every thread, so the shuffles always see whole warps.
+constexpr int kP2GLanes = 8;
+__global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a, const uint32_t* __restrict__ list,
+                                             const uint32_t* __restrict__ count) {
+    const Grid& g = a.g;
+    const uint32_t nq = *count;
+    const uint32_t groups = (uint32_t)(gridDim.x * blockDim.x / kP2GLanes);
+    const uint32_t gid = (uint32_t)((blockIdx.x * blockDim.x + threadIdx.x) / kP2GLanes);
+    const int lane = (int)(threadIdx.x % kP2GLanes);
+    for (uint32_t base = 0; base < nq; base += groups) {
+        const uint32_t h = base + gid;
+        int i = 0, j = 0, k = 0;
+        const bool node = h < nq && node_of(g, list[min(h, nq - 1)], i, j, k);
+        const bool hu = node && j < g.ny && k < g.nz, hv = node && i < g.nx && k < g.nz,
+                   hw = node && i < g.nx && j < g.ny;
+        double su = 0, wu = 0, sv = 0, wv = 0, sw = 0, ww = 0;
+        const int ci0 = max(i - 1, 0), ci1 = min(i + 1, g.nx - 1);
+        for (int ck = max(k - 1, 0); node && ck <= min(k + 1, g.nz - 1); ++ck)
+            for (int cj = max(j - 1, 0); cj <= min(j + 1, g.ny - 1); ++cj) {
+                uint32_t c = ((uint32_t)ck * g.ny + cj) * g.nx;
+                uint32_t s0 = a.start[c + ci0], s1 = a.start[c + ci1 + 1];
+                for (uint32_t s = s0 + lane; s < s1; s += kP2GLanes) {
+                    double4 l = a.lrec[s];
+                    float4 vel = a.vrec[s];
+                    if (hu) {
+                        double wx = corner_w(l.x, g.nx + 1, i), wy = corner_w(l.y - 0.5, g.ny, j),
+                               wz = corner_w(l.z - 0.5, g.nz, k);
+                        if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                            double wgt = dmul(dmul(wx, wy), wz);
+                            su = dadd(su, dmul(wgt, (double)vel.x));
+                            wu = dadd(wu, wgt);
+                        }
+                    }
+                    if (hv) {
+                        double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y, g.ny + 1, j),
+                               wz = corner_w(l.z - 0.5, g.nz, k);
+                        if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                            double wgt = dmul(dmul(wx, wy), wz);
+                            sv = dadd(sv, dmul(wgt, (double)vel.y));
+                            wv = dadd(wv, wgt);
+                        }
+                    }
+                    if (hw) {
+                        double wx = corner_w(l.x - 0.5, g.nx, i), wy = corner_w(l.y - 0.5, g.ny, j),
+                               wz = corner_w(l.z, g.nz + 1, k);
+                        if (wx >= 0.0 && wy >= 0.0 && wz >= 0.0) {
+                            double wgt = dmul(dmul(wx, wy), wz);
+                            sw = dadd(sw, dmul(wgt, (double)vel.z));
+                            ww = dadd(ww, wgt);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+        for (int o = kP2GLanes / 2; o > 0; o >>= 1) {
+            su = dadd(su, __shfl_xor_sync(0xffffffffu, su, o, kP2GLanes));
+            wu = dadd(wu, __shfl_xor_sync(0xffffffffu, wu, o, kP2GLanes));
+            sv = dadd(sv, __shfl_xor_sync(0xffffffffu, sv, o, kP2GLanes));
+            wv = dadd(wv, __shfl_xor_sync(0xffffffffu, wv, o, kP2GLanes));
+            sw = dadd(sw, __shfl_xor_sync(0xffffffffu, sw, o, kP2GLanes));
+            ww = dadd(ww, __shfl_xor_sync(0xffffffffu, ww, o, kP2GLanes));
+        }
+        if (node && lane == 0) p2g_store(a, i, j, k, hu, hv, hw, su, wu, sv, wv, sw, ww);
     }
 }
 
@@ -502,6 +536,7 @@ struct RedistArgs {
     uint32_t* moves;         // pairs (particle, destination cell)
     RedistState* rs;
     unsigned long long* claim;  // per cell: the latest claim stamp (k_redist_par); zero at allocation
+    int rounds;                 // short lists: parallel rounds (1) or one thread in index order (0)
     double* slots;              // 2 x 16 doubles: CTA partials of k_redist_par's reductions
 };
 
@@ -657,7 +692,7 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     // indices first, and runs once it holds all of them. The cells such
     // candidates touch are disjoint, so the moves are the sequential ones.
     const uint32_t cap = a.cap;
-    if (!overflow) {
+    if (!overflow && a.rounds) {
         for (uint32_t round = 1;; ++round) {
             const unsigned long long stamp = (unsigned long long)round << 32;
             for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
@@ -737,6 +772,38 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     }
     if (threadIdx.x == 0) {
         uint32_t nm = s_nm;
+        if (!overflow && !a.rounds) {
+            // One thread in index order: cheaper than rounds when a few cells
+            // hold most candidates (a fresh jet), whose moves can only run one
+            // per round; the moves are the same.
+            for (uint32_t m = 0; m < nc; ++m) {
+                const short* sl = slots + (size_t)m * 7;
+                const int s0 = sl[0];
+                if (tcnt[s0] <= cap) continue;
+                int best = -1;
+                double best_down = -INFINITY;
+                uint32_t best_room = 0;
+#pragma unroll
+                for (int q = 1; q < 7; ++q) {
+                    const int sq = sl[q];
+                    if (sq < 0 || !tcav[sq] || tcnt[sq] >= cap) continue;
+                    const uint32_t room = cap - tcnt[sq];
+                    const double dn = a.down[q - 1];
+                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                        best = sq;
+                        best_down = dn;
+                        best_room = room;
+                    }
+                }
+                if (best >= 0) {
+                    tcnt[s0] -= 1;
+                    tcnt[best] += 1;
+                    a.moves[2 * nm] = cl[m];
+                    a.moves[2 * nm + 1] = (uint32_t)tkey[best];
+                    ++nm;
+                }
+            }
+        }
         if (overflow) {
             uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
             for (uint32_t m = 0; m < nc; ++m) {

@@ -172,8 +172,10 @@ struct PcgArgs {
     double* as;
     double* q;
     double* pq;
-    double* prod;       // per-cell products in cell order (reference dot order)
-    double* partials;   // nchunks (global fallback when they do not fit in shared memory)
+    double* prod;       // per-cell products: cell order (reference dots) or wavefront order (tree dots)
+    double* partials;   // nchunks: reference-order chunk sums
+    double* tpart;      // ceil(nf / kTile): tree-order tile sums
+    double* slots;      // 2 x 16: CTA partials of cluster-wide maxima
     int4* frec;         // per cell: forward sweep record (precon + window slots of -x,-y,-z)
     int4* brec;         // per cell: backward sweep record (precon + window slots of +x,+y,+z)
     double tol;
@@ -253,12 +255,88 @@ __device__ __forceinline__ void produce_level(const PcgSmem& m, int L, int lo, i
     cp_commit();
 }
 
+// ---------------------------------------------------------------- cluster pieces
+// The solve kernels run as one thread-block cluster (k_pcg: 1 CTA when the
+// GPU is shared with other scenes, else up to 16; k_pcg_cluster: 16). These
+// helpers split elementwise work and reductions over every thread of the
+// cluster; a cluster barrier (hardware, release/acquire) orders the phases,
+// and values another CTA wrote are read through L2.
+constexpr int kTile = 256;      // cells per tile of the tree-order dot (wavefront order)
+constexpr int kMaxCtas = 16;
+
+struct PcgCl {
+    int rank, nct;
+    uint32_t gt, G;  // thread index and count over the cluster
+    int gw, nw;      // warp index and count over the cluster
+    int parity;      // half of `slots` the next maximum uses
+};
+
+__device__ __forceinline__ PcgCl pcg_cl() {
+    PcgCl c;
+    c.rank = (int)cluster_rank();
+    c.nct = (int)cluster_size();
+    c.gt = (uint32_t)c.rank * blockDim.x + threadIdx.x;
+    c.G = (uint32_t)c.nct * blockDim.x;
+    c.gw = c.rank * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5);
+    c.nw = c.nct * (int)(blockDim.x >> 5);
+    c.parity = 0;
+    return c;
+}
+
+__device__ __forceinline__ double warp_tree_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;  // the same bits in every lane (each step adds the same pair)
+}
+
+// Maximum over the cluster (order-free): per-CTA block maxima through a
+// double-buffered slot array; a barrier separates a use of one half from the
+// next use of the same half.
+template <int BS>
+__device__ __forceinline__ double pcg_cl_max(PcgCl& c, const PcgArgs& a, double v, double* sh) {
+    double bm = block_max<BS>(v, sh);
+    double* sl = a.slots + c.parity * kMaxCtas;
+    c.parity ^= 1;
+    if (threadIdx.x == 0) sl[c.rank] = bm;
+    cluster_sync_all();
+    double m = 0.0;
+    for (int q = 0; q < c.nct; ++q) m = fmax(m, __ldcg(sl + q));
+    return m;
+}
+
+// Tree-order dot (the default). Cells in wavefront order form tiles of
+// kTile; lane l of the warp that owns a tile adds its cells l, l+32, ... in
+// order and a fixed xor tree adds the 32 lanes; the tile sums are added the
+// same way (lane l: tiles l, l+32, ...). The order depends on neither the
+// number of CTAs nor the kernel, so every solve kernel gives the same bits.
+__device__ __forceinline__ double pcg_tile_total(const PcgArgs& a, uint32_t ntile) {
+    double s = 0.0;
+    for (uint32_t t = threadIdx.x & 31; t < ntile; t += 32) s = dadd(s, __ldcg(a.tpart + t));
+    return warp_tree_sum(s);
+}
+
+__device__ __forceinline__ double pcg_tree_dot_prod(const PcgArgs& a, const PcgCl& c, uint32_t nf) {
+    cluster_sync_all();  // products complete
+    const int lane = threadIdx.x & 31;
+    const uint32_t ntile = (nf + kTile - 1) / kTile;
+    for (uint32_t t = (uint32_t)c.gw; t < ntile; t += (uint32_t)c.nw) {
+        double s = 0.0;
+        const uint32_t e = min((t + 1) * kTile, nf);
+        for (uint32_t i = t * kTile + lane; i < e; i += 32) s = dadd(s, __ldcg(a.prod + i));
+        s = warp_tree_sum(s);
+        if (lane == 0) a.tpart[t] = s;
+    }
+    cluster_sync_all();
+    return pcg_tile_total(a, ntile);
+}
+
 // Exact reference dot (pressure.rs:588-603) over `prod` (cell order): one
-// warp per 4096-cell chunk folds its products in cell order from registers
-// through shuffles, then one thread sums the partials in chunk order.
-__device__ __forceinline__ double pcg_chunk_sums(const PcgArgs& a, const PcgSmem& m, double* sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int ch = warp; ch < a.nchunks; ch += nw) {
+// warp per 4096-cell chunk across the cluster folds its products in cell
+// order, then every CTA adds the chunk sums in chunk order.
+__device__ double pcg_exact_dot(const PcgArgs& a, const PcgCl& c, double* sh) {
+    cluster_sync_all();  // products complete
+    const int lane = threadIdx.x & 31;
+    for (int ch = c.gw; ch < a.nchunks; ch += c.nw) {
         int t = a.chunk_start[ch], e = a.chunk_start[ch + 1];
         double acc = 0.0;
         for (; t < e; t += 512) {
@@ -266,7 +344,7 @@ __device__ __forceinline__ double pcg_chunk_sums(const PcgArgs& a, const PcgSmem
 #pragma unroll
             for (int u = 0; u < 16; ++u) {
                 int idx = t + u * 32 + lane;
-                v[u] = idx < e ? a.prod[idx] : 0.0;
+                v[u] = idx < e ? __ldcg(a.prod + idx) : 0.0;
             }
             int cnt = min(512, e - t);
 #pragma unroll
@@ -278,18 +356,42 @@ __device__ __forceinline__ double pcg_chunk_sums(const PcgArgs& a, const PcgSmem
                 }
             }
         }
-        if (lane == 0) m.part[ch] = acc;
+        if (lane == 0) a.partials[ch] = acc;
     }
-    __syncthreads();
+    cluster_sync_all();
     if (threadIdx.x == 0) {
         double s = -0.0;
-        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, m.part[ch]);
+        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, __ldcg(a.partials + ch));
         sh[0] = s;
     }
     __syncthreads();
     double r = sh[0];
     __syncthreads();
     return r;
+}
+
+// dot over the products a sweep or the matvec stored in `prod`.
+__device__ __forceinline__ double pcg_dot_prod(const PcgArgs& a, const PcgCl& c, uint32_t nf, double* sh) {
+    return a.exact_dots ? pcg_exact_dot(a, c, sh) : pcg_tree_dot_prod(a, c, nf);
+}
+
+// Tree dot of the products one CTA stored itself (the sweeps): that CTA forms
+// the tile sums (same tiles and order as pcg_tree_dot_prod) and one cluster
+// barrier publishes them. Called by every CTA; only `owner` does the tiles.
+__device__ __forceinline__ double pcg_tree_dot_own(const PcgArgs& a, bool owner, uint32_t nf) {
+    const uint32_t ntile = (nf + kTile - 1) / kTile;
+    if (owner) {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (uint32_t t = w; t < ntile; t += nw) {
+            double s = 0.0;
+            const uint32_t e = min((t + 1) * kTile, nf);
+            for (uint32_t i = t * kTile + lane; i < e; i += 32) s = dadd(s, a.prod[i]);
+            s = warp_tree_sum(s);
+            if (lane == 0) a.tpart[t] = s;
+        }
+    }
+    cluster_sync_all();
+    return pcg_tile_total(a, ntile);
 }
 
 // build_mic0 (pressure.rs:442-513) as a forward level sweep. precon and the
@@ -552,9 +654,7 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
                     double zv = dmul(t, pc);
                     cur[tid] = zv;
                     z[lsA + tid] = zv;
-                    double pr = dmul(zv, cr);
-                    if (a.exact_dots) a.prod[a.cinv[lsA + tid]] = pr;
-                    else zr = dadd(zr, pr);
+                    a.prod[a.exact_dots ? a.cinv[lsA + tid] : lsA + tid] = dmul(zv, cr);
                 }
             } else {
                 for (int ps = lsA + tid; ps < lsN; ps += sw) {
@@ -574,9 +674,7 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
                     double zv = dmul(t, pc);
                     z[ps] = zv;
                     if (wcur <= kPcgBS) cur[ps - lsA] = zv;  // the next level reads the window
-                    double pr = dmul(zv, r[ps]);
-                    if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
-                    else zr = dadd(zr, pr);
+                    a.prod[a.exact_dots ? a.cinv[ps] : ps] = dmul(zv, r[ps]);
                 }
             }
         }
@@ -598,7 +696,13 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
     return zr;
 }
 
-// pcg (pressure.rs:341-397) in one persistent block.
+// pcg (pressure.rs:341-397) as one thread-block cluster of C CTAs (C = 1
+// when the GPU is shared with other scenes). CTA 0 runs the MIC(0) factor
+// and both triangular sweeps in its shared memory exactly as a single block
+// would (their cost is the per-level latency, which more SMs do not lower);
+// the matvec, the updates of p, r and s, the norms and the dots are spread
+// over all CTAs, whose extra bandwidth they are bound by. Phases are ordered
+// by cluster barriers.
 __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[40];
@@ -615,13 +719,15 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
         m.m1 = (int*)q; q += (size_t)kPcgBS * 4;
         m.lvs = (int*)q;
     }
+    PcgCl c = pcg_cl();
+    const bool lead = c.rank == 0;  // the CTA that runs the sweeps
     if (a.nlevels > kMaxLevelsSmem) m.lvs = const_cast<int*>(a.level_start);
     else
         for (int L = threadIdx.x; L <= a.nlevels; L += blockDim.x) m.lvs[L] = a.level_start[L];
-    if (a.nchunks > kMaxChunksSmem) m.part = a.partials;
     __syncthreads();
     const uint32_t nf = *a.nf;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t ntile = (nf + kTile - 1) / kTile;
+    const int tid = threadIdx.x, lane = tid & 31;
     // Non-empty level range and the widest level -> sweep width (warps).
     __shared__ int s_l0, s_l1, s_wmax;
     if (tid == 0) {
@@ -630,7 +736,7 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
         s_wmax = 0;
     }
     __syncthreads();
-    for (int L = tid; L < a.nlevels; L += nt) {
+    for (int L = tid; L < a.nlevels; L += blockDim.x) {
         int w = m.lvs[L + 1] - m.lvs[L];
         if (w > 0) {
             atomicMin(&s_l0, L);
@@ -642,9 +748,9 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
     const int l0 = s_l0, l1 = s_l1;
     const int sw = min(kSweepMax, max(32, (s_wmax + 31) & ~31));
 
-    // Section timers (thread 0 only, kept in shared memory to spare registers).
+    // Section timers (CTA 0, thread 0; kept in shared memory to spare registers).
     __shared__ unsigned long long tsec[8], ltim[4], tck;
-    const bool timed = a.timing != nullptr;
+    const bool timed = a.timing != nullptr && lead;
     if (tid == 0) {
         for (int q = 0; q < 8; ++q) tsec[q] = 0;
         for (int q = 0; q < 4; ++q) ltim[q] = 0;
@@ -660,97 +766,98 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
         }                                              \
     } while (0)
     double mx = 0.0;
-    for (uint32_t i = tid; i < nf; i += nt) mx = fmax(mx, fabs(a.b[i]));
-    double residual = block_max<kPcgBS>(mx, sh);
+    for (uint32_t i = c.gt; i < nf; i += c.G) mx = fmax(mx, fabs(a.b[i]));
+    double residual = pcg_cl_max<kPcgBS>(c, a, mx, sh);
     int iters = 0;
     if (residual > a.tol) {
         SECTION(7);
-        pcg_build_mic0(a, m, sw, l0, l1);
-        pcg_build_records(a, m, nf);
+        if (lead) {
+            pcg_build_mic0(a, m, sw, l0, l1);
+            pcg_build_records(a, m, nf);
+        }
         SECTION(0);
-        for (uint32_t i = tid; i < nf; i += nt) {
+        for (uint32_t i = c.gt; i < nf; i += c.G) {
             a.r[i] = a.b[i];
             a.p[i] = 0.0;
         }
-        __syncthreads();
-        double zr = pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1);
+        cluster_sync_all();  // r complete before the sweeps read it
+        if (lead) pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1);
         SECTION(1);
-        for (uint32_t i = tid; i < nf; i += nt) a.s[i] = a.z[i];
-        __syncthreads();
-        double sigma = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(zr, sh);  // dot(z, r)
+        // dot(z, r); its barriers also publish z
+        double sigma = a.exact_dots ? pcg_exact_dot(a, c, sh) : pcg_tree_dot_own(a, lead, nf);
         SECTION(4);
+        for (uint32_t i = c.gt; i < nf; i += c.G) a.s[i] = __ldcg(a.z + i);
+        cluster_sync_all();  // s complete before the matvec reads neighbours
         for (int it = 0; it < a.max_iters; ++it) {
             iters = it + 1;
             // apply_a (pressure.rs:400-439): diag*x, then +x,-x,+y,-y,+z,-z; and s*As.
-            // Two cells per thread per round, index loads first for memory parallelism.
-            double sas = 0.0;
-            for (uint32_t i0 = tid; i0 < nf; i0 += 2 * nt) {
-                int nbv[2][6];
-                double sv[2];
+            // Tiles of kTile cells per warp (the tree dot's tiles): lane l takes
+            // cells l, l+32, ... of the tile.
+            for (uint32_t t = (uint32_t)c.gw; t < ntile; t += (uint32_t)c.nw) {
+                double acc = 0.0;
+#pragma unroll 2
+                for (int u = 0; u < kTile / 32; ++u) {
+                    const uint32_t i = t * kTile + lane + 32u * u;
+                    if (i >= nf) break;
+                    const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
+                    const int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
+                    const int nbv[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
+                    const double sv = __ldcg(a.s + i);
+                    double nsv[6];
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    uint32_t i = i0 + u * nt;
-                    if (i < nf) {
-                        const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
-                        int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
-                        nbv[u][0] = x0.x; nbv[u][1] = x0.y; nbv[u][2] = x1.x;
-                        nbv[u][3] = x1.y; nbv[u][4] = x2.x; nbv[u][5] = x2.y;
-                        sv[u] = a.s[i];
-                    }
+                    for (int d = 0; d < 6; ++d) nsv[d] = nbv[d] >= 0 ? __ldcg(a.s + nbv[d]) : 0.0;
+                    double v = dmul((double)a.diag[i], sv);
+                    if (nbv[NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
+                    if (nbv[NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
+                    if (nbv[NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
+                    if (nbv[NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
+                    if (nbv[NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
+                    if (nbv[NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
+                    a.as[i] = v;
+                    if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv, v);
+                    else acc = dadd(acc, dmul(sv, v));
                 }
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    uint32_t i = i0 + u * nt;
-                    if (i < nf) {
-                        double nsv[6];
-#pragma unroll
-                        for (int d = 0; d < 6; ++d) nsv[d] = nbv[u][d] >= 0 ? a.s[nbv[u][d]] : 0.0;
-                        double v = dmul((double)a.diag[i], sv[u]);
-                        if (nbv[u][NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
-                        if (nbv[u][NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
-                        if (nbv[u][NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
-                        if (nbv[u][NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
-                        if (nbv[u][NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
-                        if (nbv[u][NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
-                        a.as[i] = v;
-                        if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv[u], v);
-                        else sas = dadd(sas, dmul(sv[u], v));
-                    }
+                if (!a.exact_dots) {
+                    acc = warp_tree_sum(acc);
+                    if (lane == 0) a.tpart[t] = acc;
                 }
             }
-            __syncthreads();
             SECTION(3);
-            double denom = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(sas, sh);  // dot(s, As)
+            double denom;  // dot(s, As)
+            if (a.exact_dots) {
+                denom = pcg_exact_dot(a, c, sh);
+            } else {
+                cluster_sync_all();
+                denom = pcg_tile_total(a, ntile);
+            }
             SECTION(4);
             if (fabs(denom) < 1e-30) break;
             double alpha = ddiv(sigma, denom);
             double mr = 0.0;
-#pragma unroll 4
-            for (uint32_t i = tid; i < nf; i += nt) {
-                a.p[i] = dadd(a.p[i], dmul(alpha, a.s[i]));
-                double rv = dsub(a.r[i], dmul(alpha, a.as[i]));
+            for (uint32_t i = c.gt; i < nf; i += c.G) {
+                a.p[i] = dadd(a.p[i], dmul(alpha, __ldcg(a.s + i)));
+                double rv = dsub(a.r[i], dmul(alpha, __ldcg(a.as + i)));
                 a.r[i] = rv;
                 mr = fmax(mr, fabs(rv));
             }
-            residual = block_max<kPcgBS>(mr, sh);
+            residual = pcg_cl_max<kPcgBS>(c, a, mr, sh);  // its barrier also publishes r
             SECTION(5);
             if (residual <= a.tol) break;
-            zr = pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1, lt);
+            if (lead) pcg_apply_mic0(a, m, a.r, a.z, sw, l0, l1, lt);
             SECTION(1);
-            double sigma_new = a.exact_dots ? pcg_chunk_sums(a, m, sh) : block_sum<kPcgBS>(zr, sh);  // dot(z, r)
+            double sigma_new = a.exact_dots ? pcg_exact_dot(a, c, sh) : pcg_tree_dot_own(a, lead, nf);  // dot(z, r)
             SECTION(4);
             double beta = ddiv(sigma_new, sigma);
-#pragma unroll 4
-            for (uint32_t i = tid; i < nf; i += nt) a.s[i] = dadd(a.z[i], dmul(beta, a.s[i]));
-            __syncthreads();
+            for (uint32_t i = c.gt; i < nf; i += c.G) a.s[i] = dadd(__ldcg(a.z + i), dmul(beta, a.s[i]));
+            cluster_sync_all();
             SECTION(6);
             sigma = sigma_new;
         }
-        for (uint32_t i = tid; i < nf; i += nt) a.p_dense[a.lv_cell[i]] = a.p[i];
+        for (uint32_t i = c.gt; i < nf; i += c.G) a.p_dense[a.lv_cell[i]] = a.p[i];
     }
     SECTION(7);
 #undef SECTION
-    if (tid == 0) {
+    if (lead && tid == 0) {
         *a.out_iters = iters;
         *a.out_residual = residual;
         if (a.timing) {

@@ -10,11 +10,11 @@
 // Values that other CTAs wrote during the solve are read through L2
 // (ld.global.cg), so no stale L1 line is ever used.
 //
-// Dot products: in exact mode the reference's 4096-cell chunks (pressure.rs:
-// 588-603) are folded one warp per chunk across the cluster and the chunk sums
-// added in chunk order, bit-identical to k_pcg and to the reference. In tree
-// mode every CTA reduces its cells with a block tree and the CTA partials are
-// added in CTA order (deterministic; rounding differs from k_pcg's one tree).
+// Dot products: the helpers of pressure.cuh. In exact mode the reference's
+// 4096-cell chunks (pressure.rs:588-603) are folded one warp per chunk across
+// the cluster and the chunk sums added in chunk order, bit-identical to k_pcg
+// and to the reference; the default tree order (fixed 256-cell tiles) is the
+// same as k_pcg's too, so both kernels give the same pressure bits.
 #pragma once
 #include "pressure.cuh"
 
@@ -29,76 +29,7 @@ struct ClusterCtx {
     int rank, nctas;
     int gtid, gthreads;   // thread index and count over the cluster
     const int* lvs;       // level starts (shared memory, or global when many)
-    double* slots;        // 2 x kClMaxCtas CTA partials in global memory
-    int parity;           // which half of `slots` the next reduction uses
 };
-
-// Cluster-wide reductions: block tree per CTA, CTA partials through global
-// memory, then every thread combines them in CTA order (same value in all
-// CTAs). The two halves of `slots` alternate, so a partial is never
-// overwritten before every CTA has read it (a cluster barrier separates a
-// reduction from the one two steps later that reuses its half).
-__device__ __forceinline__ double cl_sum(ClusterCtx& c, double v, double* sh) {
-    double bs = block_sum<kClBS>(v, sh);
-    double* sl = c.slots + c.parity * kClMaxCtas;
-    c.parity ^= 1;
-    if (threadIdx.x == 0) sl[c.rank] = bs;
-    cluster_sync_all();
-    double s = 0.0;
-    for (int q = 0; q < c.nctas; ++q) s = dadd(s, __ldcg(sl + q));
-    return s;
-}
-__device__ __forceinline__ double cl_max(ClusterCtx& c, double v, double* sh) {
-    double bm = block_max<kClBS>(v, sh);
-    double* sl = c.slots + c.parity * kClMaxCtas;
-    c.parity ^= 1;
-    if (threadIdx.x == 0) sl[c.rank] = bm;
-    cluster_sync_all();
-    double m = 0.0;
-    for (int q = 0; q < c.nctas; ++q) m = fmax(m, __ldcg(sl + q));
-    return m;
-}
-
-// Exact reference dot over `prod` (cell order), written before the call by
-// any CTA: one warp per 4096-cell chunk folds it in cell order, then every
-// CTA adds the chunk sums in chunk order.
-__device__ double cl_chunk_sums(const PcgArgs& a, ClusterCtx& c, double* sh) {
-    cluster_sync_all();  // all products written
-    const int lane = threadIdx.x & 31;
-    const int gw = c.rank * (kClBS / 32) + (threadIdx.x >> 5), nw = c.nctas * (kClBS / 32);
-    for (int ch = gw; ch < a.nchunks; ch += nw) {
-        int t = a.chunk_start[ch], e = a.chunk_start[ch + 1];
-        double acc = 0.0;
-        for (; t < e; t += 512) {
-            double v[16];
-#pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                int idx = t + u * 32 + lane;
-                v[u] = idx < e ? __ldcg(a.prod + idx) : 0.0;
-            }
-            int cnt = min(512, e - t);
-#pragma unroll
-            for (int u = 0; u < 16; ++u) {
-#pragma unroll 8
-                for (int src = 0; src < 32; ++src) {
-                    double x = __shfl_sync(0xffffffffu, v[u], src);
-                    if (u * 32 + src < cnt) acc = dadd(acc, x);
-                }
-            }
-        }
-        if (lane == 0) a.partials[ch] = acc;
-    }
-    cluster_sync_all();
-    if (threadIdx.x == 0) {
-        double s = -0.0;
-        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, __ldcg(a.partials + ch));
-        sh[0] = s;
-    }
-    __syncthreads();
-    double r = sh[0];
-    __syncthreads();
-    return r;
-}
 
 // build_mic0 (pressure.rs:442-513): forward level sweep over the cluster,
 // the same per-cell arithmetic as pcg_build_mic0.
@@ -150,13 +81,13 @@ __device__ void cl_build_mic0(const PcgArgs& a, const ClusterCtx& c, int l0, int
 }
 
 // apply_mic0 (pressure.rs:517-570): forward L q = r, backward L^T z = q, and
-// the z*r products of the following dot (exact mode: into `prod`; tree mode:
-// this thread's running sum, returned). A thread's first cell of the next
-// level (its neighbour indices, operand and factor, none of which the sweep
-// writes) is loaded before the level barrier, so after the barrier only the
-// neighbours' sweep values are on the critical path; further cells of wide
+// the z*r products of the following dot into `prod` (cell order for the
+// reference dots, wavefront order for the tree dots). A thread's first cell of
+// the next level (its neighbour indices, operand and factor, none of which the
+// sweep writes) is loaded before the level barrier, so after the barrier only
+// the neighbours' sweep values are on the critical path; further cells of wide
 // levels load inline.
-__device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const double* r, double* z, int l0, int l1) {
+__device__ void cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const double* r, double* z, int l0, int l1) {
     const int G = c.gthreads;
     // ---------------- forward
     int ps = c.lvs[l0] + c.gtid, le = c.lvs[l0 + 1];
@@ -210,7 +141,6 @@ __device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const dou
         rv = nrv; pc = npc;
     }
     // ---------------- backward
-    double zr = 0.0;
     int ls = c.lvs[l1 - 1];
     ps = ls + c.gtid;
     le = c.lvs[l1];
@@ -246,9 +176,7 @@ __device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const dou
             if (pz >= 0) t = dadd(t, dmul(pc, vz));
             double zv = dmul(t, pc);
             z[ps] = zv;
-            double pr = dmul(zv, rr);
-            if (a.exact_dots) a.prod[a.cinv[ps]] = pr;
-            else zr = dadd(zr, pr);
+            a.prod[a.exact_dots ? a.cinv[ps] : ps] = dmul(zv, rr);
             for (int p2 = ps + G; p2 < le; p2 += G) {
                 const int* nb = a.nbr + (size_t)p2 * 6;
                 const int x = nb[NB_PX], y = nb[NB_PY], zz = nb[NB_PZ];
@@ -262,9 +190,7 @@ __device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const dou
                 if (zz >= 0) t2 = dadd(t2, dmul(pc2, wz));
                 double z2 = dmul(t2, pc2);
                 z[p2] = z2;
-                double pr2 = dmul(z2, __ldcg(r + p2));
-                if (a.exact_dots) a.prod[a.cinv[p2]] = pr2;
-                else zr = dadd(zr, pr2);
+                a.prod[a.exact_dots ? a.cinv[p2] : p2] = dmul(z2, __ldcg(r + p2));
             }
         }
         cluster_sync_all();
@@ -273,12 +199,11 @@ __device__ double cl_apply_mic0(const PcgArgs& a, const ClusterCtx& c, const dou
         px = npx; py = npy; pz = npz;
         qv = nqv; rr = nrr; pc = npc;
     }
-    return zr;
 }
 
 // The solve. Launched as exactly one cluster (gridDim = cluster size).
 // `slots` holds 2 x kClMaxCtas doubles of scratch for the CTA partials.
-__global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a, double* slots) {
+__global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a) {
     __shared__ int s_lvs[kClMaxLevelsSmem + 1];
     __shared__ double sh[40];
     __shared__ int s_l0, s_l1;
@@ -287,8 +212,6 @@ __global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a, double* slo
     c.nctas = (int)cluster_size();
     c.gtid = c.rank * kClBS + (int)threadIdx.x;
     c.gthreads = c.nctas * kClBS;
-    c.slots = slots;
-    c.parity = 0;
     const int tid = threadIdx.x, nt = blockDim.x;
     if (a.nlevels <= kClMaxLevelsSmem) {
         for (int L = tid; L <= a.nlevels; L += nt) s_lvs[L] = a.level_start[L];
@@ -312,9 +235,12 @@ __global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a, double* slo
     const uint32_t nf = *a.nf;
     const int G = c.gthreads, gt = c.gtid;
 
+    PcgCl pc = pcg_cl();
+    const uint32_t ntile = (nf + kTile - 1) / kTile;
+    const int lane = tid & 31;
     double mx = 0.0;
     for (uint32_t i = gt; i < nf; i += G) mx = fmax(mx, fabs(a.b[i]));
-    double residual = cl_max(c, mx, sh);
+    double residual = pcg_cl_max<kClBS>(pc, a, mx, sh);
     int iters = 0;
     if (residual > a.tol) {
         cl_build_mic0(a, c, l0, l1);
@@ -323,46 +249,61 @@ __global__ void __launch_bounds__(kClBS, 1) k_pcg_cluster(PcgArgs a, double* slo
             a.p[i] = 0.0;
         }
         cluster_sync_all();
-        double zr = cl_apply_mic0(a, c, a.r, a.z, l0, l1);
+        cl_apply_mic0(a, c, a.r, a.z, l0, l1);
+        double sigma = pcg_dot_prod(a, pc, nf, sh);  // dot(z, r)
         for (uint32_t i = gt; i < nf; i += G) a.s[i] = __ldcg(a.z + i);
-        double sigma = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, zr, sh);  // dot(z, r); also orders s
+        cluster_sync_all();  // s complete before the matvec reads neighbours
         for (int it = 0; it < a.max_iters; ++it) {
             iters = it + 1;
-            // apply_a (pressure.rs:400-439): diag*x, then +x,-x,+y,-y,+z,-z; and s*As.
-            double sas = 0.0;
-            for (uint32_t i = gt; i < nf; i += G) {
-                const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
-                int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
-                int nbv[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
-                double sv = __ldcg(a.s + i);
-                double nsv[6];
+            // apply_a (pressure.rs:400-439) and s*As, by tiles of the tree dot
+            for (uint32_t t = (uint32_t)pc.gw; t < ntile; t += (uint32_t)pc.nw) {
+                double acc = 0.0;
+                for (int u = 0; u < kTile / 32; ++u) {
+                    const uint32_t i = t * kTile + lane + 32u * u;
+                    if (i >= nf) break;
+                    const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
+                    int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
+                    int nbv[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
+                    double sv = __ldcg(a.s + i);
+                    double nsv[6];
 #pragma unroll
-                for (int d = 0; d < 6; ++d) nsv[d] = nbv[d] >= 0 ? __ldcg(a.s + nbv[d]) : 0.0;
-                double v = dmul((double)a.diag[i], sv);
-                if (nbv[NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
-                if (nbv[NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
-                if (nbv[NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
-                if (nbv[NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
-                if (nbv[NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
-                if (nbv[NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
-                a.as[i] = v;
-                if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv, v);
-                else sas = dadd(sas, dmul(sv, v));
+                    for (int d = 0; d < 6; ++d) nsv[d] = nbv[d] >= 0 ? __ldcg(a.s + nbv[d]) : 0.0;
+                    double v = dmul((double)a.diag[i], sv);
+                    if (nbv[NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
+                    if (nbv[NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
+                    if (nbv[NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
+                    if (nbv[NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
+                    if (nbv[NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
+                    if (nbv[NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
+                    a.as[i] = v;
+                    if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv, v);
+                    else acc = dadd(acc, dmul(sv, v));
+                }
+                if (!a.exact_dots) {
+                    acc = warp_tree_sum(acc);
+                    if (lane == 0) a.tpart[t] = acc;
+                }
             }
-            double denom = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, sas, sh);  // dot(s, As)
+            double denom;  // dot(s, As)
+            if (a.exact_dots) {
+                denom = pcg_exact_dot(a, pc, sh);
+            } else {
+                cluster_sync_all();
+                denom = pcg_tile_total(a, ntile);
+            }
             if (fabs(denom) < 1e-30) break;
             double alpha = ddiv(sigma, denom);
             double mr = 0.0;
             for (uint32_t i = gt; i < nf; i += G) {
-                a.p[i] = dadd(a.p[i], dmul(alpha, a.s[i]));
-                double rv = dsub(a.r[i], dmul(alpha, a.as[i]));
+                a.p[i] = dadd(a.p[i], dmul(alpha, __ldcg(a.s + i)));
+                double rv = dsub(a.r[i], dmul(alpha, __ldcg(a.as + i)));
                 a.r[i] = rv;
                 mr = fmax(mr, fabs(rv));
             }
-            residual = cl_max(c, mr, sh);  // also orders r before the sweeps
+            residual = pcg_cl_max<kClBS>(pc, a, mr, sh);  // also orders r before the sweeps
             if (residual <= a.tol) break;
-            zr = cl_apply_mic0(a, c, a.r, a.z, l0, l1);
-            double sigma_new = a.exact_dots ? cl_chunk_sums(a, c, sh) : cl_sum(c, zr, sh);  // dot(z, r)
+            cl_apply_mic0(a, c, a.r, a.z, l0, l1);
+            double sigma_new = pcg_dot_prod(a, pc, nf, sh);  // dot(z, r)
             double beta = ddiv(sigma_new, sigma);
             for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(a.z + i), dmul(beta, a.s[i]));
             cluster_sync_all();  // s complete before the next matvec reads neighbours

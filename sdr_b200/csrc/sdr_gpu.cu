@@ -71,22 +71,25 @@ constexpr uint32_t kClusterMinFluidCells = 200000;
 // 16 (one per SM, the largest non-portable cluster) when the device can
 // schedule it for that kernel, else the portable 8.
 template <class Kern>
-int cluster_ctas(Kern kernel, int slot, int threads, int device) {
+int cluster_ctas(Kern kernel, int slot, int threads, int device, size_t dyn_smem = 0) {
     static std::mutex mu;
-    static int ctas[2][64] = {};
+    static int ctas[3][64] = {};
     if (device < 0 || device >= 64) throw Fail{SDR_ERR_CUDA, "device index out of range"};
     std::lock_guard<std::mutex> lk(mu);
     if (!ctas[slot][device]) {
-        int n = 8;
+        int n = dyn_smem ? 4 : 8;  // without an answer: a size every GPC holds
         if (cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(kClMaxCtas);
             cfg.blockDim = dim3(threads);
+            cfg.dynamicSmemBytes = dyn_smem;
             int mx = 0;
-            if (cudaOccupancyMaxPotentialClusterSize(&mx, kernel, &cfg) == cudaSuccess && mx >= kClMaxCtas)
-                n = kClMaxCtas;
+            if (cudaOccupancyMaxPotentialClusterSize(&mx, kernel, &cfg) == cudaSuccess && mx >= 1) {
+                n = 1;
+                while (n * 2 <= mx && n * 2 <= kClMaxCtas) n *= 2;  // largest power of two it allows
+            }
         }
-        cudaGetLastError();  // a refused query leaves the portable size
+        cudaGetLastError();  // a refused query leaves the default
         ctas[slot][device] = n;
     }
     return ctas[slot][device];
@@ -94,11 +97,11 @@ int cluster_ctas(Kern kernel, int slot, int threads, int device) {
 
 // Launch a kernel as exactly one cluster of `ctas` CTAs on `st`.
 template <class Kern, class... Args>
-void launch_one_cluster(Kern kernel, int ctas, int threads, cudaStream_t st, Args... args) {
+void launch_one_cluster_smem(Kern kernel, int ctas, int threads, size_t dyn_smem, cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)ctas);
     cfg.blockDim = dim3((unsigned)threads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = dyn_smem;
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -109,6 +112,11 @@ void launch_one_cluster(Kern kernel, int ctas, int threads, cudaStream_t st, Arg
     cfg.numAttrs = 1;
     CK(cudaLaunchKernelEx(&cfg, kernel, args...));
     g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+template <class Kern, class... Args>
+void launch_one_cluster(Kern kernel, int ctas, int threads, cudaStream_t st, Args... args) {
+    launch_one_cluster_smem(kernel, ctas, threads, 0, st, args...);
 }
 
 // Solver-owned device buffers come from one library memory pool per device,
@@ -236,6 +244,7 @@ struct DevStatus {
     uint32_t ncand;
     uint32_t nmoves;
     uint32_t long_count;
+    uint32_t p2g_queue;     // P2G nodes with particles this substep
     uint32_t total;         // scratch scan total
     uint32_t hist_max;
     unsigned long long fluid_count;
@@ -368,6 +377,11 @@ struct sdr_solver {
     bool kernel_timers = false;  // profiling level 2: section timers inside k_pcg
     bool exact_dots = false;  // reference dot order in the PCG (bit-exact pressure)
     int pcg_kernel = SDR_PCG_AUTO;  // which pressure-solve kernel (SDR_PCG_*)
+    int pcg_ctas = 0;               // CTAs of k_pcg's cluster (0: 1 on a shared GPU, else the device's largest)
+    bool shared_gpu = false;        // SDR_SOLVER_SHARED_GPU
+    double* tpart = nullptr;        // tile sums of the tree-order dots
+    uint32_t* p2g_list = nullptr;   // grid nodes with particles around them (P2G queue)
+    uint32_t last_p2g_queue = 0;    // its length at the last status read
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
     double* cl_slots = nullptr;     // CTA partials of the cluster kernels
     unsigned long long* rclaim = nullptr;  // per cell: claim stamps of the parallel redistribution replay
@@ -455,6 +469,7 @@ struct sdr_solver {
         size_t nc = ncell;
         dalloc(u, nu, st); dalloc(v, nv, st); dalloc(w, nw, st);
         dalloc(su, nu, st); dalloc(sv, nv, st); dalloc(sw, nw, st);
+        dalloc(p2g_list, nnodes(), st);
         dalloc(u2, nu, st); dalloc(v2, nv, st); dalloc(w2, nw, st);
         dalloc(ku, nu, st); dalloc(kv, nv, st); dalloc(kw, nw, st);
         dalloc(ku2, nu, st); dalloc(kv2, nv, st); dalloc(kw2, nw, st);
@@ -484,6 +499,7 @@ struct sdr_solver {
         dalloc(s, nc, st); dalloc(as, nc, st); dalloc(q, nc, st); dalloc(pq, nc, st);
         dalloc(partials, nchunks + 1, st);
         if (!cl_slots) dalloc(cl_slots, 2 * kClMaxCtas, st);
+        dalloc(tpart, ncell / kTile + 2, st);
         dalloc(rclaim, ncell, st);
         CK(cudaMemsetAsync(rclaim, 0, ncell * sizeof(unsigned long long), st));
         dalloc(corder, nc, st);
@@ -512,7 +528,7 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st);
+        dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
         if (hst) hput(hst, 1);
@@ -613,7 +629,13 @@ struct sdr_solver {
         a.gdt[2] = fluid.gravity.z * dt;
         a.add_forces = fused;
         a.enforce = fused;
-        LAUNCH(k_p2g, blocks(nnodes() * kP2GLanes, kBS), kBS, 0, st, a);
+        // empty nodes at once, the rest queued for the eight-lane gather; its grid
+        // follows the last queue length (the loop over the queue covers any length)
+        CK(cudaMemsetAsync(&dst->p2g_queue, 0, 4, st));
+        LAUNCH(k_p2g_nodes, blocks(nnodes(), kBS), kBS, 0, st, a, p2g_list, &dst->p2g_queue);
+        const size_t want = ((size_t)last_p2g_queue + last_p2g_queue / 4 + 64) * kP2GLanes;
+        LAUNCH(k_p2g, (unsigned)std::min<size_t>(blocks(want, kBS), 148 * 16), kBS, 0, st, a, p2g_list,
+               &dst->p2g_queue);
     }
 
     void add_forces(double dt) {  // solver.rs:593-604
@@ -687,6 +709,8 @@ struct sdr_solver {
         a.b = b;
         a.precon = precon; a.p = p; a.r = r; a.z = z; a.s = s; a.as = as; a.q = q; a.pq = pq;
         a.partials = partials;
+        a.tpart = tpart;
+        a.slots = cl_slots;
         a.tol = tol;
         a.max_iters = (int)std::min<uint64_t>(max_iters, (uint64_t)INT32_MAX);
         a.lv_cell = lv_cell;
@@ -701,10 +725,21 @@ struct sdr_solver {
             // One cluster of up to 16 CTAs (one per SM); the levels of each
             // sweep are separated by the hardware cluster barrier.
             a.timing = nullptr;
-            launch_one_cluster(k_pcg_cluster, cluster_ctas(k_pcg_cluster, 0, kClBS, device), kClBS, st, a, cl_slots);
+            launch_one_cluster(k_pcg_cluster, cluster_ctas(k_pcg_cluster, 0, kClBS, device), kClBS, st, a);
             if (profiling) prof.pcg_cluster_launches += 1;
         } else {
-            LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+            // Sweeps on CTA 0, elementwise phases on the whole cluster: one
+            // CTA when the GPU is shared with other scenes (each solve then
+            // holds one SM), else the largest cluster the device schedules.
+            const int most = cluster_ctas(k_pcg, 2, kPcgBS, device, kPcgSmem);
+            const int ctas = pcg_ctas > 0 ? std::min(pcg_ctas, most) : (shared_gpu ? 1 : most);
+            if (ctas == 1) {
+                // a plain launch: the kernel sees a cluster of one CTA, and the
+                // launch overlaps other streams' kernels like any other
+                LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+            } else {
+                launch_one_cluster_smem(k_pcg, ctas, kPcgBS, kPcgSmem, st, a);
+            }
         }
     }
 
@@ -801,8 +836,11 @@ struct sdr_solver {
         ra.bitmap = ptmp;  // free between the sort of one substep and the next
         ra.n_upper = n_upper;
         ra.claim = rclaim;
+        ra.rounds = shared_gpu ? 0 : 1;  // many scenes: spend no SM time on rounds
         ra.slots = cl_slots;
-        const int rp_ctas = cluster_ctas(k_redist_par, 1, kRpBS, device);
+        // On a shared GPU one CTA: a cluster launch waits for a whole GPC of
+        // free SMs, which other scenes' solves rarely leave.
+        const int rp_ctas = shared_gpu ? 1 : cluster_ctas(k_redist_par, 1, kRpBS, device);
         ra.cap = cap_;
         const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
@@ -816,7 +854,8 @@ struct sdr_solver {
                    (uint32_t)cap);
             LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
             // long lists only (the replay kernel hands over through the state; otherwise it returns at once)
-            launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
+            if (rp_ctas == 1) LAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
+            else launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
         }
         LAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
         sorted_valid = false;
@@ -873,6 +912,7 @@ struct sdr_solver {
         last_pcg_iters = (uint64_t)hst->iters;
         last_residual = hst->residual;
         last_nf = hst->nf;
+        last_p2g_queue = hst->p2g_queue;
         read_grid_speed();
         device_ms += elapsed(0, 9);
         particle_substeps += n_before;
@@ -1117,6 +1157,7 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
                                                   std::to_string(prop.major) + std::to_string(prop.minor)};
             CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
             s->create_events();
+            s->shared_gpu = options && (options->flags & SDR_SOLVER_SHARED_GPU);
             if (options && (options->flags & SDR_SOLVER_BLOCKING_SYNC))
                 CK(cudaEventCreateWithFlags(&s->ev_block, cudaEventBlockingSync | cudaEventDisableTiming));
             CK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmem));
@@ -1262,6 +1303,14 @@ int sdr_solver_set_dot_order(sdr_solver* s, int reference_order) {
     return guard([&] {
         require(s, "null solver");
         s->exact_dots = reference_order != 0;
+    });
+}
+
+int sdr_solver_set_pcg_ctas(sdr_solver* s, int ctas) {
+    return guard([&] {
+        require(s, "null solver");
+        require(ctas >= 0 && ctas <= kMaxCtas, "CTAs must be 0 (automatic) or 1..16");
+        s->pcg_ctas = ctas;
     });
 }
 

@@ -109,7 +109,7 @@ SceneResult run_scene(const sdr_scene_desc& d, int32_t device) {
     sdr_solver_options o{};
     o.max_particles = particle_capacity(d);
     o.device = device;
-    o.flags = SDR_SOLVER_BLOCKING_SYNC;
+    o.flags = SDR_SOLVER_BLOCKING_SYNC | SDR_SOLVER_SHARED_GPU;
     int rc = sdr_solver_create(&d.sdf, d.sim_dx, &d.fluid, &d.needle, &o, &s);
     if (rc == SDR_OK && d.has_outlet) rc = sdr_solver_set_outlet(s, &d.outlet);
     if (rc == SDR_OK) rc = sdr_solver_set_solve_params(s, &d.solve);

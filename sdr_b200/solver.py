@@ -167,6 +167,10 @@ class Solver:
         """_lib.PCG_AUTO, PCG_ONE_BLOCK (one SM) or PCG_CLUSTER (up to 16 SMs)."""
         check(_lib.load().sdr_solver_set_pcg_kernel(self._h, int(kernel)))
 
+    def set_pcg_ctas(self, ctas: int) -> None:
+        """CTAs of the one-SM-sweep solve's cluster (0: automatic); results do not depend on it."""
+        check(_lib.load().sdr_solver_set_pcg_ctas(self._h, int(ctas)))
+
     def set_profiling(self, on: bool, kernel_timers: bool = False) -> None:
         """Phase timing with CUDA events; kernel_timers adds the pressure-solve section timers."""
         check(_lib.load().sdr_solver_set_profiling(self._h, (2 if kernel_timers else 1) if on else 0))

@@ -178,6 +178,28 @@ def test_project_wide_levels_bit_exact(kernel):
     assert diff == 0
 
 
+def test_project_tree_dots_same_bits_for_every_kernel():
+    """The default tree-order dots do not depend on where the solve runs:
+    sweeps on one SM with the rest on 1, 2 or 4 CTAs or the device's largest
+    cluster, or everything on the cluster kernel, give the same pressure bits
+    and iteration count."""
+    runs = {}
+    for name, kernel, ctas in [("one_cta", _lib.PCG_ONE_BLOCK, 1), ("two_ctas", _lib.PCG_ONE_BLOCK, 2),
+                               ("four_ctas", _lib.PCG_ONE_BLOCK, 4), ("auto", _lib.PCG_ONE_BLOCK, 0),
+                               ("cluster", _lib.PCG_CLUSTER, 0)]:
+        gpu, orc, fluid, widths = _wide_pair()
+        gpu.set_pcg_kernel(kernel)
+        gpu.set_pcg_ctas(ctas)
+        gpu.run_phase(_lib.PHASE_PROJECT, 1e-4)
+        runs[name] = (gpu.pressure(), gpu.last_pcg_iters)
+    ref_p, ref_it = runs["one_cta"]
+    record("project_tree_kernels", {k: {"iters": it, "bit_mismatch": int(np.sum(p.view(np.uint64) != ref_p.view(np.uint64)))}
+                                    for k, (p, it) in runs.items()})
+    for name, (p, it) in runs.items():
+        assert it == ref_it, name
+        assert np.array_equal(p.view(np.uint64), ref_p.view(np.uint64)), name
+
+
 def test_project_cluster_tree_dots():
     """The cluster kernel with its default tree dots (per-CTA trees added in
     CTA order): pressure within the tree-order tolerance of the reference."""
