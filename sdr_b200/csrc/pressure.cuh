@@ -197,13 +197,12 @@ struct SweepRec {
 
 // Shared-memory plan of k_pcg (dynamic): a ring of kStages staged levels
 // (two f64 operands and one record per cell), two level windows of f64 and of
-// neighbour masks, the level starts and the dot partials.
+// neighbour masks and the level starts.
 constexpr int kStages = 4;          // levels in flight ahead of the sweep
 constexpr int kMaxLevelsSmem = 2048;
-constexpr int kMaxChunksSmem = 2048;
 constexpr int kSweepMax = kPcgBS - 32;  // compute threads; one producer warp stages ahead
 constexpr size_t kPcgSmem = (size_t)kStages * kPcgBS * (8 + 8 + 16) + 2 * kPcgBS * 8 + 2 * kPcgBS * 4 +
-                            (kMaxLevelsSmem + 1) * 4 + kMaxChunksSmem * 8;
+                            (kMaxLevelsSmem + 1) * 4;
 
 struct PcgSmem {
     double* sa;     // [kStages][BS]
@@ -214,7 +213,6 @@ struct PcgSmem {
     int* m0;        // [BS] neighbour-mask window (MIC build)
     int* m1;
     int* lvs;       // level starts (smem copy or global)
-    double* part;   // dot partials
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -498,14 +496,13 @@ __device__ void pcg_build_records(const PcgArgs& a, const PcgSmem& m, uint32_t n
 // Compute threads [0, sw) take one cell each per level from the staged ring;
 // the producer warp [sw, sw+32) stages level L + kStages - 1 while level L is
 // computed. Levels wider than the ring use global memory (uniform branch).
-__device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const double* r, double* z, int sw, int l0,
-                                 int l1, unsigned long long* lt = nullptr) {
+__device__ void pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const double* r, double* z, int sw, int l0,
+                               int l1, unsigned long long* lt = nullptr) {
     const int tid = threadIdx.x;
     const int nbar = sw + 32;
-    double zr = 0.0;
     if (tid >= nbar) {
         __syncthreads();
-        return zr;
+        return;
     }
     const bool producer = tid >= sw;
     const int lane = tid - sw;
@@ -693,7 +690,6 @@ __device__ double pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const doubl
     }
     if (producer) asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
-    return zr;
 }
 
 // pcg (pressure.rs:341-397) as one thread-block cluster of C CTAs (C = 1
@@ -714,7 +710,6 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
         m.sb = (double*)q; q += (size_t)kStages * kPcgBS * 8;
         m.w0 = (double*)q; q += (size_t)kPcgBS * 8;
         m.w1 = (double*)q; q += (size_t)kPcgBS * 8;
-        m.part = (double*)q; q += (size_t)kMaxChunksSmem * 8;
         m.m0 = (int*)q; q += (size_t)kPcgBS * 4;
         m.m1 = (int*)q; q += (size_t)kPcgBS * 4;
         m.lvs = (int*)q;
