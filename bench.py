@@ -66,6 +66,19 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def reduce_over_ranks(dev_ms: float, wall: float, ps: int, device: str):
+    """Whole-job figures of a multi-rank run: the slowest rank's device and
+    wall time (max) and the particle-substeps of all ranks (sum). Every rank
+    takes the same two collectives in the same order."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([dev_ms, wall], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(ps)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), int(c[0])
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -385,12 +398,7 @@ def main():
     diag = solver.profile()
     solver.set_profiling(False)
     if world > 1:
-        t = torch.tensor([dev_ms, wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, wall = float(t[0]), float(t[1])
-        c = torch.tensor([ps], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        ps = int(c[0])
+        dev_ms, wall, ps = reduce_over_ranks(dev_ms, wall, ps, "cuda")
     value = ps / (dev_ms / 1e3)
     e2e = ps / wall
     hbm, peak_kind = peaks()
