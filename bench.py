@@ -66,6 +66,14 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def substep_bytes(particle_substeps: int, substeps: int, cells: int, sdf_nodes: int, cell_iters: int) -> float:
+    """Algorithmic bytes of `substeps` substeps by the per-substep contract
+    B = 112 P + 92 C + 4 S + 83 N_f iters (f32 particle and face state, u8
+    labels, f32 solve vectors, f64 factor): P particles, C grid cells, S SDF
+    nodes, N_f fluid cells; summed over substeps."""
+    return 112.0 * particle_substeps + (92.0 * cells + 4.0 * sdf_nodes) * substeps + 83.0 * cell_iters
+
+
 def reduce_over_ranks(dev_ms: float, wall: float, ps: int, device: str):
     """Whole-job figures of a multi-rank run: the slowest rank's device and
     wall time (max) and the particle-substeps of all ranks (sum). Every rank
@@ -406,6 +414,9 @@ def main():
     pcg_bytes = (PCG_BYTES_PER_CELL_ITER * prof["pcg_cell_iters"] + PCG_BYTES_PER_CELL_SOLVE * prof["fluid_cells"]) / max(prof["pcg_launches"], 1)
     achieved = pcg_bytes / (pcg_launch_ms / 1e3) / 1e9 if pcg_launch_ms > 0 else 0.0
     st = solver.stats()
+    sub_bytes = substep_bytes(prof["particles"], prof["substeps"], int(st.nx * st.ny * st.nz),
+                              int(sdf.data.size), prof["pcg_cell_iters"])
+    sub_gbs = sub_bytes / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else 0.0  # rank 0's substeps, rank 0's time at N = 1
     line = {"metric": "particle-substeps/s", "value": value, "unit": "particle-substeps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
@@ -420,6 +431,11 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_pcg", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
                          "bytes_per_launch": pcg_bytes, "ms_per_launch": pcg_launch_ms},
+            "substep_roofline": ({"bound": "hbm", "achieved": sub_gbs, "peak": hbm, "unit": "GB/s",
+                                  "frac": sub_gbs / hbm, "peak_kind": peak_kind,
+                                  "bytes_per_substep": sub_bytes / max(prof["substeps"], 1),
+                                  "bytes": "112 P + 92 C + 4 S + 83 N_f iters per substep"}
+                                 if world == 1 else None),
             "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
             "pcg_section_cycles": {k: v for k, v in zip(
                 ["mic_build", "sweeps", "unused", "matvec", "dots", "axpy_norm", "direction", "setup_exit",

@@ -42,3 +42,11 @@ def test_two_rank_reduction_matches_bench_contract():
     assert res[0] == res[1] == (150.0, 0.20, 4_000_000)
     dev_ms, wall, ps = res[0]
     assert abs(ps / (dev_ms / 1e3) - 4_000_000 / 0.150) < 1e-6
+
+
+def test_substep_bytes_contract():
+    import bench
+    # one substep: 1000 particles, 10x10x10 cells, 20^3 SDF nodes, 500 fluid cells x 10 iterations
+    b = bench.substep_bytes(1000, 1, 1000, 8000, 5000)
+    assert b == 112 * 1000 + 92 * 1000 + 4 * 8000 + 83 * 5000
+    assert bench.substep_bytes(2000, 2, 1000, 8000, 10000) == 2 * b
