@@ -226,8 +226,8 @@ int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
 enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2 };
 int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel);
 /* CTAs of the SDR_PCG_ONE_BLOCK solve's cluster (CTA 0 runs the sweeps).
- * 0 (default): 1 with SDR_SOLVER_SHARED_GPU, else the largest cluster the
- * device schedules. Results do not depend on it. */
+ * 0 (default): 1 with SDR_SOLVER_SHARED_GPU, else 8 (or the largest cluster
+ * the device schedules, if smaller). Results do not depend on it. */
 int sdr_solver_set_pcg_ctas(sdr_solver* s, int ctas);
 /* Phase-group timing with CUDA events (adds one event record per group):
  * on = 1. on = 2 also turns on the section timers inside the pressure-solve

@@ -732,7 +732,10 @@ struct sdr_solver {
             // CTA when the GPU is shared with other scenes (each solve then
             // holds one SM), else the largest cluster the device schedules.
             const int most = cluster_ctas(k_pcg, 2, kPcgBS, device, kPcgSmem);
-            const int ctas = pcg_ctas > 0 ? std::min(pcg_ctas, most) : (shared_gpu ? 1 : most);
+            // 8 CTAs measured best on the real cavity (1: 2202, 4: 2039, 8: 2024,
+            // 16: 2060 ms of solve over three frames): past 8 the cluster barrier
+            // costs more than the extra bandwidth gives
+            const int ctas = pcg_ctas > 0 ? std::min(pcg_ctas, most) : (shared_gpu ? 1 : std::min(most, 8));
             if (ctas == 1) {
                 // a plain launch: the kernel sees a cluster of one CTA, and the
                 // launch overlaps other streams' kernels like any other
