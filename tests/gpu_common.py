@@ -10,7 +10,9 @@ import oracle
 from sdr_b200 import scene as sc
 from tests.helpers import oracle_solver
 
-OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
+# Folder for the parity statistics of the GPU tests (diagnostic output; not
+# written unless SDR_TEST_RECORD_DIR is set).
+OUT = os.environ.get("SDR_TEST_RECORD_DIR")
 
 SMOKE_TOML = """
 [sim]
@@ -27,7 +29,9 @@ particles_per_cell = 8
 
 
 def record(name: str, data: dict) -> None:
-    """Append parity statistics to gpurun_out/parity.json (diagnostic output)."""
+    """Append parity statistics to parity.json in SDR_TEST_RECORD_DIR, if set."""
+    if not OUT:
+        return
     os.makedirs(OUT, exist_ok=True)
     path = os.path.join(OUT, "parity.json")
     all_ = {}

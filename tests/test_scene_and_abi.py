@@ -76,7 +76,8 @@ def test_readme_pins():
     examples/maxillary_real.toml: fill 44.9 % (README.md:58-61) and the 2.228 ml cavity
     (assets/README.md). examples/scene.toml (README.md:146-151): the injected dose
     (10.0 ml) and the mean membrane load (436 Pa) agree; the peak fill, coverage,
-    drained volume and focal peak differ by 2-15 %."""
+    drained volume and focal peak differ by 2-15 %: those README figures come from an
+    unstated code revision and a chaotic run, so they are recorded, not required."""
     d = json.load(open(os.path.join(ROOT, "tests", "golden", "readme_pins.json")))
     mx = d["maxillary_real"]["summary"]
     assert round(mx["peak_fill_fraction"] * 100, 1) == 44.9
