@@ -86,50 +86,46 @@ __global__ void k_extrap_valid(Grid g, const uint8_t* __restrict__ cells, uint8_
         kw[((size_t)k * g.ny + j) * g.nx + i] = (k > 0 && fl(i, j, k - 1)) || (k < g.nz && fl(i, j, k));
 }
 
-// One snapshot sweep of extrapolate (solver.rs:964-1007) on one component:
-// unknown entries take the mean of their known neighbours, summed in the
-// order -x,+x,-y,+y,-z,+z.
-__device__ __forceinline__ void extrap_one(const float* __restrict__ f, const uint8_t* __restrict__ kn,
-                                           float* __restrict__ f2, uint8_t* __restrict__ kn2, int nx,
+// One snapshot sweep of extrapolate (solver.rs:964-1007) on one component,
+// in place. kn holds 0 for unknown, 1 for known from the start and s + 2 for
+// a face that became known in sweep s; sweep s reads only faces known before
+// it, whose values no longer change, so every face sees the snapshot the
+// reference's copy-then-update sweep gives it. Unknown entries take the mean
+// of their known neighbours, summed in the order -x,+x,-y,+y,-z,+z; everything
+// else is left as it is (the reference copies it unchanged).
+__device__ __forceinline__ void extrap_one(float* __restrict__ f, uint8_t* __restrict__ kn, int sweep, int nx,
                                            int ny, int nz, int i, int j, int k) {
-    size_t c = ((size_t)k * ny + j) * nx + i;
-    if (kn[c]) {
-        f2[c] = f[c];
-        kn2[c] = 1;
-        return;
-    }
+    const size_t c = ((size_t)k * ny + j) * nx + i;
+    if (kn[c]) return;
+    const int before = sweep + 1;  // kn in [1, before]: known before this sweep
+    auto known = [&](size_t q) {
+        const int v = kn[q];
+        return v != 0 && v <= before;
+    };
     float sum = 0.0f;
     int cnt = 0;
-    size_t sy = nx, sz = (size_t)nx * ny;
-    if (i > 0 && kn[c - 1]) { sum += f[c - 1]; ++cnt; }
-    if (i + 1 < nx && kn[c + 1]) { sum += f[c + 1]; ++cnt; }
-    if (j > 0 && kn[c - sy]) { sum += f[c - sy]; ++cnt; }
-    if (j + 1 < ny && kn[c + sy]) { sum += f[c + sy]; ++cnt; }
-    if (k > 0 && kn[c - sz]) { sum += f[c - sz]; ++cnt; }
-    if (k + 1 < nz && kn[c + sz]) { sum += f[c + sz]; ++cnt; }
+    const size_t sy = nx, sz = (size_t)nx * ny;
+    if (i > 0 && known(c - 1)) { sum += f[c - 1]; ++cnt; }
+    if (i + 1 < nx && known(c + 1)) { sum += f[c + 1]; ++cnt; }
+    if (j > 0 && known(c - sy)) { sum += f[c - sy]; ++cnt; }
+    if (j + 1 < ny && known(c + sy)) { sum += f[c + sy]; ++cnt; }
+    if (k > 0 && known(c - sz)) { sum += f[c - sz]; ++cnt; }
+    if (k + 1 < nz && known(c + sz)) { sum += f[c + sz]; ++cnt; }
     if (cnt > 0) {
-        f2[c] = sum / (float)cnt;
-        kn2[c] = 1;
-    } else {
-        f2[c] = f[c];
-        kn2[c] = 0;
+        f[c] = sum / (float)cnt;
+        kn[c] = (uint8_t)(sweep + 2);
     }
 }
 
 struct ExtrapArgs {
     Grid g;
-    const float* u;
-    const float* v;
-    const float* w;
-    const uint8_t* ku;
-    const uint8_t* kv;
-    const uint8_t* kw;
-    float* u2;
-    float* v2;
-    float* w2;
-    uint8_t* ku2;
-    uint8_t* kv2;
-    uint8_t* kw2;
+    float* u;
+    float* v;
+    float* w;
+    uint8_t* ku;
+    uint8_t* kv;
+    uint8_t* kw;
+    int sweep;              // 0..3
     unsigned int* maxbits;  // optional: |u|,|v|,|w| maxima (last sweep)
 };
 
@@ -139,16 +135,16 @@ __global__ void __launch_bounds__(256) k_extrap(ExtrapArgs a) {
     float mu = 0.f, mv = 0.f, mw = 0.f;
     if (node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) {
         if (j < g.ny && k < g.nz) {
-            extrap_one(a.u, a.ku, a.u2, a.ku2, g.nx + 1, g.ny, g.nz, i, j, k);
-            mu = fabsf(a.u2[((size_t)k * g.ny + j) * (g.nx + 1) + i]);
+            extrap_one(a.u, a.ku, a.sweep, g.nx + 1, g.ny, g.nz, i, j, k);
+            if (a.maxbits) mu = fabsf(a.u[((size_t)k * g.ny + j) * (g.nx + 1) + i]);
         }
         if (i < g.nx && k < g.nz) {
-            extrap_one(a.v, a.kv, a.v2, a.kv2, g.nx, g.ny + 1, g.nz, i, j, k);
-            mv = fabsf(a.v2[((size_t)k * (g.ny + 1) + j) * g.nx + i]);
+            extrap_one(a.v, a.kv, a.sweep, g.nx, g.ny + 1, g.nz, i, j, k);
+            if (a.maxbits) mv = fabsf(a.v[((size_t)k * (g.ny + 1) + j) * g.nx + i]);
         }
         if (i < g.nx && j < g.ny) {
-            extrap_one(a.w, a.kw, a.w2, a.kw2, g.nx, g.ny, g.nz + 1, i, j, k);
-            mw = fabsf(a.w2[((size_t)k * g.ny + j) * g.nx + i]);
+            extrap_one(a.w, a.kw, a.sweep, g.nx, g.ny, g.nz + 1, i, j, k);
+            if (a.maxbits) mw = fabsf(a.w[((size_t)k * g.ny + j) * g.nx + i]);
         }
     }
     if (a.maxbits) {

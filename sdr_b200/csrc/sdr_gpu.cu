@@ -330,8 +330,7 @@ struct sdr_solver {
     double* sdf64 = nullptr;
     float* sdf32 = nullptr;
     float *u = nullptr, *v = nullptr, *w = nullptr, *su = nullptr, *sv = nullptr, *sw = nullptr;
-    float *u2 = nullptr, *v2 = nullptr, *w2 = nullptr;
-    uint8_t *ku = nullptr, *kv = nullptr, *kw = nullptr, *ku2 = nullptr, *kv2 = nullptr, *kw2 = nullptr;
+    uint8_t *ku = nullptr, *kv = nullptr, *kw = nullptr;  // extrapolation: when each face became known
     uint8_t *cells = nullptr, *base = nullptr, *cavity = nullptr;
     float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
     int* key_cell = nullptr;
@@ -470,9 +469,7 @@ struct sdr_solver {
         dalloc(u, nu, st); dalloc(v, nv, st); dalloc(w, nw, st);
         dalloc(su, nu, st); dalloc(sv, nv, st); dalloc(sw, nw, st);
         dalloc(p2g_list, nnodes(), st);
-        dalloc(u2, nu, st); dalloc(v2, nv, st); dalloc(w2, nw, st);
         dalloc(ku, nu, st); dalloc(kv, nv, st); dalloc(kw, nw, st);
-        dalloc(ku2, nu, st); dalloc(kv2, nv, st); dalloc(kw2, nw, st);
         CK(cudaMemsetAsync(u, 0, nu * 4, st));
         CK(cudaMemsetAsync(v, 0, nv * 4, st));
         CK(cudaMemsetAsync(w, 0, nw * 4, st));
@@ -518,8 +515,8 @@ struct sdr_solver {
 
     void free_all() {
         dfree(sdf64, st); dfree(sdf32, st);
-        dfree(u, st); dfree(v, st); dfree(w, st); dfree(su, st); dfree(sv, st); dfree(sw, st); dfree(u2, st); dfree(v2, st); dfree(w2, st);
-        dfree(ku, st); dfree(kv, st); dfree(kw, st); dfree(ku2, st); dfree(kv2, st); dfree(kw2, st);
+        dfree(u, st); dfree(v, st); dfree(w, st); dfree(su, st); dfree(sv, st); dfree(sw, st);
+        dfree(ku, st); dfree(kv, st); dfree(kw, st);
         dfree(cells, st); dfree(base, st); dfree(cavity, st);
         dfree(pos, st); dfree(vel, st); dfree(pos2, st); dfree(vel2, st);
         dfree(key_cell, st); dfree(key_sort, st); dfree(perm, st); dfree(ptmp, st); dfree(flag, st); dfree(off, st); dfree(drn, st);
@@ -756,16 +753,10 @@ struct sdr_solver {
         unsigned ngrid = blocks(nnodes(), 256);
         LAUNCH(k_extrap_valid, ngrid, 256, 0, st, g, cells, ku, kv, kw);
         CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
-        float *a_u = u, *a_v = v, *a_w = w, *b_u = u2, *b_v = v2, *b_w = w2;
-        uint8_t *a_ku = ku, *a_kv = kv, *a_kw = kw, *b_ku = ku2, *b_kv = kv2, *b_kw = kw2;
-        for (int it = 0; it < 4; ++it) {
-            ExtrapArgs e{g, a_u, a_v, a_w, a_ku, a_kv, a_kw, b_u, b_v, b_w, b_ku, b_kv, b_kw,
-                         it == 3 ? dst->maxbits : nullptr};
+        for (int it = 0; it < 4; ++it) {  // four sweeps, in place
+            ExtrapArgs e{g, u, v, w, ku, kv, kw, it, it == 3 ? dst->maxbits : nullptr};
             LAUNCH(k_extrap, ngrid, 256, 0, st, e);
-            std::swap(a_u, b_u); std::swap(a_v, b_v); std::swap(a_w, b_w);
-            std::swap(a_ku, b_ku); std::swap(a_kv, b_kv); std::swap(a_kw, b_kw);
         }
-        // four sweeps: the result is back in u, v, w
     }
 
     void face_max() {
