@@ -87,3 +87,32 @@ def test_readme_pins():
     assert abs(s["injected_ml"] - 10.0) < 1e-9
     assert abs(s["mean_membrane_pressure_pa"] - 436) / 436 < 0.01
     assert abs(s["total_drained_ml"] - 8.11) / 8.11 < 0.03
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device():
+    """Null handles and out-of-range values fail cleanly with SDR_ERR_INVALID
+    and a message, before any device work."""
+    import ctypes as C
+
+    from sdr_b200 import _lib
+    L = _lib.load()
+    plane = _lib.SlicePlaneC()
+    w, h = C.c_uint32(), C.c_uint32()
+    cases = [
+        lambda: L.sdr_solver_set_pcg_ctas(None, 4),
+        lambda: L.sdr_solver_set_pcg_kernel(None, 1),
+        lambda: L.sdr_render_slice(None, C.byref(plane), 300, 0.0, None, 0, C.byref(w), C.byref(h)),
+        lambda: L.sdr_render_timeseries(None, 3, 10, 10, None, 0),
+        lambda: L.sdr_write_png(None, None, 1, 1),
+        lambda: L.sdr_slice_plane_xy(0.0, 1.0, None),
+        lambda: L.sdr_slice_plane_gravity(_lib.Vec3(0, -9.81, 0), None),
+        lambda: L.sdr_metrics_write_json(None, b"x.json"),
+        lambda: L.sdr_metrics_write_csv(None, b"x.csv"),
+        lambda: L.sdr_frames_write_json(None, 2, b"x.json"),
+        lambda: L.sdr_summary_write_json(None, b"x.json"),
+    ]
+    for i, call in enumerate(cases):
+        assert call() == _lib.SDR_ERR_INVALID, i
+        assert L.sdr_last_error(), i
+    img = (C.c_uint8 * 12)()
+    assert L.sdr_render_timeseries(None, 0, 10, 10, img, 12) == _lib.SDR_ERR_BUFFER  # needs 300 bytes
