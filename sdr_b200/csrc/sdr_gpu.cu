@@ -630,7 +630,8 @@ struct sdr_solver {
         // follows the last queue length (the loop over the queue covers any length)
         CK(cudaMemsetAsync(&dst->p2g_queue, 0, 4, st));
         LAUNCH(k_p2g_nodes, blocks(nnodes(), kBS), kBS, 0, st, a, p2g_list, &dst->p2g_queue);
-        const size_t want = ((size_t)last_p2g_queue + last_p2g_queue / 4 + 64) * kP2GLanes;
+        const size_t want = last_p2g_queue ? ((size_t)last_p2g_queue + last_p2g_queue / 4 + 64) * kP2GLanes
+                                           : nnodes() * kP2GLanes;  // no history yet: every node
         LAUNCH(k_p2g, (unsigned)std::min<size_t>(blocks(want, kBS), 148 * 16), kBS, 0, st, a, p2g_list,
                &dst->p2g_queue);
     }
@@ -1005,6 +1006,7 @@ struct sdr_solver {
             }
             if (ph == SDR_PHASE_EXTRAPOLATE) read_grid_speed();
             if (ph == SDR_PHASE_REDISTRIBUTE) account_redistribution();
+            if (ph == SDR_PHASE_P2G) last_p2g_queue = hst->p2g_queue;
         }
     }
 };
