@@ -378,6 +378,7 @@ struct sdr_solver {
     int pcg_kernel = SDR_PCG_AUTO;  // which pressure-solve kernel (SDR_PCG_*)
     int pcg_ctas = 0;               // CTAs of k_pcg's cluster (0: 1 on a shared GPU, else the device's largest)
     bool shared_gpu = false;        // SDR_SOLVER_SHARED_GPU
+    int ctas_pcg = 0, ctas_pcgc = 0, ctas_rp = 0;  // largest clusters the device schedules (asked once)
     double* tpart = nullptr;        // tile sums of the tree-order dots
     uint32_t* p2g_list = nullptr;   // grid nodes with particles around them (P2G queue)
     uint32_t last_p2g_queue = 0;    // its length at the last status read
@@ -723,17 +724,21 @@ struct sdr_solver {
             // One cluster of up to 16 CTAs (one per SM); the levels of each
             // sweep are separated by the hardware cluster barrier.
             a.timing = nullptr;
-            launch_one_cluster(k_pcg_cluster, cluster_ctas(k_pcg_cluster, 0, kClBS, device), kClBS, st, a);
+            if (!ctas_pcgc) ctas_pcgc = cluster_ctas(k_pcg_cluster, 0, kClBS, device);
+            launch_one_cluster(k_pcg_cluster, ctas_pcgc, kClBS, st, a);
             if (profiling) prof.pcg_cluster_launches += 1;
         } else {
             // Sweeps on CTA 0, elementwise phases on the whole cluster: one
             // CTA when the GPU is shared with other scenes (each solve then
             // holds one SM), else the largest cluster the device schedules.
-            const int most = cluster_ctas(k_pcg, 2, kPcgBS, device, kPcgSmem);
             // 8 CTAs measured best on the real cavity (1: 2202, 4: 2039, 8: 2024,
             // 16: 2060 ms of solve over three frames): past 8 the cluster barrier
             // costs more than the extra bandwidth gives
-            const int ctas = pcg_ctas > 0 ? std::min(pcg_ctas, most) : (shared_gpu ? 1 : std::min(most, 8));
+            int ctas = 1;
+            if (pcg_ctas > 0 || !shared_gpu) {
+                if (!ctas_pcg) ctas_pcg = cluster_ctas(k_pcg, 2, kPcgBS, device, kPcgSmem);
+                ctas = pcg_ctas > 0 ? std::min(pcg_ctas, ctas_pcg) : std::min(ctas_pcg, 8);
+            }
             if (ctas == 1) {
                 // a plain launch: the kernel sees a cluster of one CTA, and the
                 // launch overlaps other streams' kernels like any other
@@ -835,7 +840,8 @@ struct sdr_solver {
         ra.slots = cl_slots;
         // On a shared GPU one CTA: a cluster launch waits for a whole GPC of
         // free SMs, which other scenes' solves rarely leave.
-        const int rp_ctas = shared_gpu ? 1 : cluster_ctas(k_redist_par, 1, kRpBS, device);
+        if (!shared_gpu && !ctas_rp) ctas_rp = cluster_ctas(k_redist_par, 1, kRpBS, device);
+        const int rp_ctas = shared_gpu ? 1 : ctas_rp;
         ra.cap = cap_;
         const double dirs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
