@@ -98,3 +98,36 @@ def test_png_round_trip(tmp_path):
         assert np.array_equal(_read_png(p), img)
     with pytest.raises(RuntimeError):
         save_png(img, tmp_path / "missing" / "x.png")
+
+
+def test_oracle_renderer_passes_the_reference_render_tests():
+    """The oracle's restatement of render.rs, pinned by the reference's own
+    render tests (render.rs:492-566) on their short_run scene: the slice shows
+    cavity interior and coloured fluid/needle pixels, the gravity projection a
+    silhouette and an amber pool, and the amber render is deterministic."""
+    from sdr_b200 import scene as sc
+    from tests.helpers import oracle_solver
+    toml = ("[sim]\nresolution_mm = 2.5\nduration_s = 0.05\nframes = 5\n"
+            "[needle]\nauto = true\ndiameter_mm = 1.2\nflow_rate_ml_s = 6.0\n"
+            "[fluid]\nparticles_per_cell = 16\n")
+    res = sc.SceneConfig.from_toml_str(toml).resolve()
+    orc = oracle_solver(res)
+    for _ in range(res.frames):
+        orc.step(res.frame_dt)
+    interior = np.array([232, 236, 244], dtype=np.uint8)
+
+    def coloured(img):
+        return bool(((img.max(axis=2).astype(int) - img.min(axis=2).astype(int)) > 60).any())
+
+    xy = SlicePlane.xy(res.needle.tip[2], res.sim_dx).as_dict()
+    img = orc.render_slice(xy, 300, 0.0)
+    assert img.shape[0] > 0 and img.shape[1] > 0
+    assert (img == interior).all(axis=2).any(), "no cavity interior was drawn"
+    assert coloured(img), "no fluid/needle pixels rendered"
+    g = SlicePlane.projected_along_gravity(res.fluid.gravity).as_dict()
+    a = orc.render_slice(g, 300, 0.0)
+    assert (a == interior).all(axis=2).any(), "no cavity silhouette"
+    assert coloured(a)
+    r, gg, b = (a[..., k].astype(int) for k in range(3))
+    assert ((r > gg) & (gg > b) & ((r - b) > 20)).any(), "no amber fluid pool was rendered"
+    assert np.array_equal(a, orc.render_slice(g, 300, 0.0)), "amber render is not deterministic"
