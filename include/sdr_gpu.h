@@ -3,7 +3,7 @@
  *
  * This is the drop-in boundary: every entry point replaces one piece of the
  * reference's Rust API (paths are within the reference project). A Rust
- * `extern "C"` block binds these one to one (see INTEGRATION.md).
+ * `extern "C"` block binds these one to one.
  *
  * Conventions
  *  - Opaque handles, created and destroyed explicitly by the caller.
@@ -34,8 +34,9 @@ enum {
     SDR_ERR_INVALID = 1,        /* bad argument (null pointer, size mismatch, bad params) */
     SDR_ERR_CUDA = 2,           /* a CUDA runtime call failed */
     SDR_ERR_OOM = 3,            /* device allocation failed */
-    SDR_ERR_CAPACITY = 4,       /* particle or work-list capacity exceeded */
-    SDR_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+    SDR_ERR_CAPACITY = 4,       /* particle or work-list capacity exceeded (the redistribution
+                                   candidate list: see sdr_solver_set_candidate_capacity) */
+    SDR_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait or loop gave up */
     SDR_ERR_NO_DEVICE = 6,      /* no CUDA device or the library was built for another arch */
     SDR_ERR_BUFFER = 7,         /* caller buffer too small; required size reported */
     SDR_ERR_IO = 8              /* a file could not be created or written */
@@ -149,6 +150,10 @@ typedef struct {
     uint64_t redist_sweeps;
     uint64_t redist_long_sweeps;
     uint64_t pcg_cluster_launches; /* solves that ran on the cluster kernel */
+    /* bytes the substeps copied host -> device (emitted particles) and device
+     * -> host (the per-substep status block) */
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
 } sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */
@@ -205,6 +210,18 @@ int sdr_solver_step(sdr_solver* s, double dt);
 int sdr_solver_substep(sdr_solver* s, double dt);
 /* Public fields time/steps/last_pcg_iters/last_substeps/drained (solver.rs:155-166). */
 int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* out);
+/* Solver::cfl_dt (src/solver.rs:262-281) for the current state, and the
+ * MacGrid::max_speed (src/grid.rs:202-206) it uses: the face maxima the last
+ * extrapolation sweep reduced on the device, combined on the host in f64.
+ * Either output may be NULL. */
+int sdr_solver_cfl(const sdr_solver* s, double* dt, double* grid_speed);
+/* Entries of the redistribution candidate list (particles of over-cap cells
+ * in one sweep of Solver::redistribute, src/solver.rs:454-557). 0 (default):
+ * the particle capacity, which no sweep can exceed. A smaller list uses less
+ * device memory; a sweep whose candidates do not fit moves nothing and the
+ * substep returns SDR_ERR_CAPACITY (the error is reported once; the solver
+ * stays usable). */
+int sdr_solver_set_candidate_capacity(sdr_solver* s, uint64_t candidates);
 /* Dot-product order inside the pressure solve. 1: the reference's order
  * (fixed 4096-cell chunks summed sequentially, partials in chunk order,
  * src/pressure.rs:588-603) — pressure and iteration counts then equal the
@@ -303,13 +320,21 @@ int sdr_sdf_mesh_grid(const double* tris, size_t ntri, double dx, double padding
  * sign and closest-point distance per node, on the device. */
 int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double dx,
                       const uint64_t dims[3], double* out);
+/* Test hook: the next sdr_sdf_from_mesh call on the calling thread makes one
+ * bounded device wait run out on purpose, so that its error path runs without
+ * any GPU fault. SDR_FAULT_SDF_STAGING: the bulk copy of the first triangle
+ * tile is not issued, the staging wait gives up after its limit (about one
+ * second), the kernel waits for its other copies in flight and reports, and
+ * the call returns SDR_ERR_DEVICE_TIMEOUT. 0 clears a pending fault. */
+enum { SDR_FAULT_NONE = 0, SDR_FAULT_SDF_STAGING = 1 };
+int sdr_debug_inject(int fault);
 /* Largest mesh sdr_sdf_from_mesh_noalloc accepts. */
 #define SDR_NOALLOC_MAX_TRIANGLES 32768
 
 /* The winding-number SDF of sdr_sdf_from_mesh for callers that cannot
  * allocate device memory: hosts that hand out their whole GPU memory budget
- * up front, code running while a stream is being captured (where cudaMalloc is
- * not allowed), or latency-bound loops that cannot afford cudaMalloc's device
+ * up front (a serving process that carves one pool at start-up and must not
+ * grow), or latency-bound loops that cannot afford cudaMalloc's device
  * synchronisation. No counterpart in the reference (it has no device).
  *
  * tris_dev and out_dev are device pointers owned by the caller: ntri triangles
@@ -320,11 +345,15 @@ int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double d
  * It calls no cudaMalloc/cudaFree: its scratch (the triangles padded to whole
  * staging tiles, ~2.4 MB, plus an error word) is a static device array that
  * every GPU loading this library holds until the process exits. Meshes with
- * more than SDR_NOALLOC_MAX_TRIANGLES triangles return SDR_ERR_INVALID. The
- * first call on a device looks up the scratch's device address; make that
- * first call before any stream capture. All calls share the one scratch, so
- * calls that overlap on the GPU (other streams, other host threads) race and
- * must be serialised by the caller. */
+ * more than SDR_NOALLOC_MAX_TRIANGLES triangles, and dims with a zero axis, an
+ * axis above 2^31-1 or more than 2^37 nodes, return SDR_ERR_INVALID before
+ * anything runs. The call is synchronous: it reads the kernel's error word
+ * back and waits for the stream. The first call on a device looks up the
+ * scratch's device address and caches it; do not use the library on a device
+ * after a cudaDeviceReset of it in the same process. All calls share the one
+ * scratch, which keeps the last call's contents, so calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised by the
+ * caller. */
 int sdr_sdf_from_mesh_noalloc(const double* tris_dev, size_t ntri, sdr_vec3 origin, double dx,
                               const uint64_t dims[3], double* out_dev, void* stream);
 
@@ -446,7 +475,9 @@ int sdr_scene_footprint(const sdr_scene_desc* scene, uint64_t* bytes);
 typedef struct sdr_batch sdr_batch;
 int sdr_batch_create(const sdr_scene_desc* scenes, size_t n, int32_t device, sdr_batch** out);
 /* Run every scene of the batch to its frame count with up to `concurrency`
- * scenes in flight (0 = all; 1 = one after another, the plain path). Scene
+ * scenes in flight (0 = all; 1 = one after another, each on a default solver
+ * as sdr_solver_create makes it: the plain path). Concurrent scenes run with
+ * SDR_SOLVER_SHARED_GPU. Scene
  * failures are reported per scene by sdr_batch_result; the call itself fails
  * only for bad arguments. */
 int sdr_batch_run(sdr_batch* b, uint32_t concurrency);

@@ -83,7 +83,8 @@ class Profile(C.Structure):
                 ("pcg_launches", C.c_uint64), ("pcg_cell_iters", C.c_uint64), ("fluid_cells", C.c_uint64),
                 ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16),
                 ("redist_candidates", C.c_uint64), ("redist_sweeps", C.c_uint64),
-                ("redist_long_sweeps", C.c_uint64), ("pcg_cluster_launches", C.c_uint64)]
+                ("redist_long_sweeps", C.c_uint64), ("pcg_cluster_launches", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
     def to_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}
@@ -149,6 +150,7 @@ class ServerStats(C.Structure):
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 FORMAT_VTK, FORMAT_XYZ = 0, 1
+FAULT_NONE, FAULT_SDF_STAGING = 0, 1
 
 P = C.POINTER
 d, u64, i32, vp, sz = C.c_double, C.c_uint64, C.c_int, C.c_void_p, C.c_size_t
@@ -167,6 +169,9 @@ SIGNATURES = {
     "sdr_solver_substep": (i32, [vp, d]),
     "sdr_solver_get_stats": (i32, [vp, P(SolverStats)]),
     "sdr_solver_set_scalars": (i32, [vp, d, d, u64, u64, u64]),
+    "sdr_solver_cfl": (i32, [vp, P(d), P(d)]),
+    "sdr_solver_set_candidate_capacity": (i32, [vp, u64]),
+    "sdr_debug_inject": (i32, [i32]),
     "sdr_solver_set_dot_order": (i32, [vp, i32]),
     "sdr_solver_set_pcg_kernel": (i32, [vp, i32]),
     "sdr_solver_set_pcg_ctas": (i32, [vp, i32]),

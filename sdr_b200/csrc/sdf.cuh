@@ -91,9 +91,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-// Bounded wait on an mbarrier phase; returns false if it gave up.
+// Bounded wait on an mbarrier phase: gives up after about one second of SM
+// clock (2^31 cycles, 1.1 s at 1965 MHz) and returns false.
+constexpr long long kWaitCycles = 1ll << 31;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t spin = 0; spin < (1u << 26); ++spin) {
+    const long long t0 = clock64();
+    for (;;) {
         uint32_t done;
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -101,15 +104,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
+        if (clock64() - t0 > kWaitCycles) return false;
     }
-    return false;
 }
+
+// k_sdf_mesh's test hook: the tile whose bulk copy is not issued (so its
+// staging wait runs out); kNoSkip in normal use.
+constexpr uint32_t kNoSkip = 0xFFFFFFFFu;
 
 // tris: padded to a whole number of tiles (9 f64 per triangle, 16-byte aligned).
 __global__ void __launch_bounds__(kSdfBS) k_sdf_mesh(const double* __restrict__ tris, uint32_t ntri,
                                                      uint32_t ntiles, double ox, double oy, double oz,
                                                      double dx, int nx, int ny, int nz,
-                                                     double* __restrict__ out, uint32_t* __restrict__ err) {
+                                                     double* __restrict__ out, uint32_t* __restrict__ err,
+                                                     uint32_t skip_tile = kNoSkip) {
     __shared__ __align__(128) double st[2][kSdfTile * 9];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int fail;
@@ -127,7 +135,7 @@ __global__ void __launch_bounds__(kSdfBS) k_sdf_mesh(const double* __restrict__ 
     const uint32_t bytes = kSdfTile * 9 * sizeof(double);
     uint32_t issued = 0;  // thread 0 only
     if (threadIdx.x == 0 && ntiles > 0) {
-        bulk_load(st[0], tris, bytes, &bar[0]);
+        if (skip_tile != 0) bulk_load(st[0], tris, bytes, &bar[0]);
         issued = 1;
     }
     double min_d2 = INFINITY, wind = 0.0;
@@ -135,7 +143,7 @@ __global__ void __launch_bounds__(kSdfBS) k_sdf_mesh(const double* __restrict__ 
     for (; t < ntiles; ++t) {
         int b = t & 1;
         if (threadIdx.x == 0 && t + 1 < ntiles) {
-            bulk_load(st[b ^ 1], tris + (size_t)(t + 1) * kSdfTile * 9, bytes, &bar[b ^ 1]);
+            if (skip_tile != t + 1) bulk_load(st[b ^ 1], tris + (size_t)(t + 1) * kSdfTile * 9, bytes, &bar[b ^ 1]);
             issued = t + 2;
         }
         if (!mbar_wait(&bar[b], (t >> 1) & 1)) fail = 1;
@@ -157,7 +165,8 @@ __global__ void __launch_bounds__(kSdfBS) k_sdf_mesh(const double* __restrict__ 
         // A bounded wait gave up: drain the copies still in flight (again
         // bounded) before the block's shared memory goes away, then report.
         if (threadIdx.x == 0) {
-            for (uint32_t q = t; q < issued; ++q) mbar_wait(&bar[q & 1], (q >> 1) & 1);
+            for (uint32_t q = t; q < issued; ++q)
+                if (q != skip_tile) mbar_wait(&bar[q & 1], (q >> 1) & 1);
             atomicOr(err, 1u);
         }
         return;

@@ -40,6 +40,8 @@ namespace {
 
 thread_local std::string g_err;
 std::atomic<uint64_t> g_launches{0};
+// sdr_debug_inject: the fault the next matching call on this thread injects.
+thread_local int g_fault = 0;
 
 struct Fail {
     int code;
@@ -355,6 +357,8 @@ struct sdr_solver {
     int4 *frec = nullptr, *brec = nullptr;
     // redistribution
     uint32_t* cand = nullptr;
+    size_t cand_n = 0;      // entries of `cand`
+    size_t cand_limit = 0;  // sdr_solver_set_candidate_capacity (0: the particle capacity)
     uint32_t* moves = nullptr;
     RedistState* rds = nullptr;
     // emission staging (pinned)
@@ -457,7 +461,8 @@ struct sdr_solver {
         dalloc(flag, ncap + 1, st);
         dalloc(off, ncap + 1, st);
         dalloc(drn, ncap, st);
-        dalloc(cand, ncap, st);
+        cand_n = cand_limit ? std::min(ncap, cand_limit) : ncap;
+        dalloc(cand, cand_n, st);
         dalloc(moves, ncap * 2, st);
         dalloc(lrec, ncap, st);
         dalloc(vrec, ncap, st);
@@ -584,6 +589,7 @@ struct sdr_solver {
         }
         CK(cudaMemcpyAsync(pos + n, h_epos, k * sizeof(float4), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(vel + n, h_evel, k * sizeof(float4), cudaMemcpyHostToDevice, st));
+        if (profiling) prof.h2d_bytes += 2 * k * sizeof(float4);
         // The staging buffers are reused next substep; the status sync at the
         // end of this substep orders the copies before any reuse.
         n += (uint32_t)k;
@@ -832,7 +838,7 @@ struct sdr_solver {
         ra.count = hist_valid;
         ra.cavity = cavity;
         ra.cand = cand;
-        ra.cand_cap = (uint32_t)cap;
+        ra.cand_cap = (uint32_t)cand_n;
         ra.bitmap = ptmp;  // free between the sort of one substep and the next
         ra.n_upper = n_upper;
         ra.claim = rclaim;
@@ -852,7 +858,7 @@ struct sdr_solver {
             CK(cudaMemsetAsync(hist_valid, 0, ncell * 4, st));
             LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), rds, key_cell, hist_valid);
             LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, g, key_cell, hist_valid, cavity, dn(), cap_, rds, cand,
-                   (uint32_t)cap);
+                   (uint32_t)cand_n);
             LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
             // long lists only (the replay kernel hands over through the state; otherwise it returns at once)
             if (rp_ctas == 1) LAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
@@ -864,6 +870,7 @@ struct sdr_solver {
 
     void sync_status() {
         CK(cudaMemcpyAsync(hst, dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+        if (profiling) prof.d2h_bytes += sizeof(DevStatus);
         if (ev_block) {  // the waiting thread sleeps instead of spinning
             CK(cudaEventRecord(ev_block, st));
             CK(cudaEventSynchronize(ev_block));
@@ -874,7 +881,17 @@ struct sdr_solver {
         drained = hst->drained;
         culled = hst->culled;
         redistributed = hst->moves;
-        if (hst->err) throw Fail{SDR_ERR_CAPACITY, "device work list overflow (error bits " + std::to_string(hst->err) + ")"};
+        if (const uint32_t e = hst->err) {
+            // Reported once: the error words start clean for the next call.
+            // The substep that set them did not finish its redistribution.
+            CK(cudaMemsetAsync(&dst->err, 0, sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(&rds->err, 0, sizeof(uint32_t), st));
+            CK(cudaStreamSynchronize(st));
+            if (e & 1u)
+                throw Fail{SDR_ERR_CAPACITY, "redistribution candidate list overflow (error bits " + std::to_string(e) +
+                                                 "); raise it with sdr_solver_set_candidate_capacity"};
+            throw Fail{SDR_ERR_DEVICE_TIMEOUT, "a bounded device loop gave up (error bits " + std::to_string(e) + ")"};
+        }
     }
 
     void read_grid_speed() {
@@ -1061,6 +1078,16 @@ int guard(F&& f) {
 
 void require(bool c, const char* msg) {
     if (!c) throw Fail{SDR_ERR_INVALID, msg};
+}
+
+// Node count of an SDF grid, checked before any copy or launch: every axis
+// 1..2^31-1 nodes (the kernels take int dimensions) and at most 2^37 nodes in
+// all (one thread per node on a one-dimensional grid of 128-thread blocks).
+size_t sdf_node_count(const uint64_t dims[3]) {
+    for (int c = 0; c < 3; ++c) require(dims[c] >= 1 && dims[c] <= (uint64_t)INT32_MAX, "dims must be 1..2^31-1");
+    const unsigned __int128 nn = (unsigned __int128)dims[0] * dims[1] * dims[2];
+    require(nn <= ((unsigned __int128)1 << 37), "SDF grid too large (more than 2^37 nodes)");
+    return (size_t)nn;
 }
 
 struct DeviceScope {
@@ -1298,6 +1325,33 @@ int sdr_solver_get_stats(const sdr_solver* s, sdr_solver_stats* o) {
         o->particle_substeps = s->particle_substeps;
         o->device_ms = s->device_ms;
         o->substeps_total = s->substeps_total;
+    });
+}
+
+int sdr_solver_cfl(const sdr_solver* s, double* dt, double* grid_speed) {
+    return guard([&] {
+        require(s && (dt || grid_speed), "null argument");
+        if (dt) *dt = s->cfl_dt();
+        if (grid_speed) *grid_speed = s->grid_speed;
+    });
+}
+
+int sdr_solver_set_candidate_capacity(sdr_solver* s, uint64_t candidates) {
+    return guard([&] {
+        require(s, "null solver");
+        require(candidates < (uint64_t)UINT32_MAX, "candidate capacity must be below 2^32");
+        DeviceScope ds(s->device);
+        s->cand_limit = (size_t)candidates;
+        s->cand_n = s->cand_limit ? std::min(s->cap, s->cand_limit) : s->cap;
+        dalloc(s->cand, s->cand_n, s->st);
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int sdr_debug_inject(int fault) {
+    return guard([&] {
+        require(fault == 0 || fault == SDR_FAULT_SDF_STAGING, "unknown fault");
+        g_fault = fault;
     });
 }
 
@@ -1885,8 +1939,11 @@ int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double d
                       double* out) {
     return guard([&] {
         require(tris && ntri && dims && out && dx > 0, "bad argument");
+        const size_t nn = sdf_node_count(dims);
+        require(ntri <= (size_t)UINT32_MAX / 2, "too many triangles");
         check_device();
-        size_t nn = dims[0] * dims[1] * dims[2];
+        const uint32_t skip = g_fault == SDR_FAULT_SDF_STAGING ? 0u : kNoSkip;
+        g_fault = 0;
         uint32_t ntiles = (uint32_t)((ntri + kSdfTile - 1) / kSdfTile);
         size_t padded = (size_t)ntiles * kSdfTile * 9;
         double *dt = nullptr, *dout = nullptr;
@@ -1907,7 +1964,7 @@ int sdr_sdf_from_mesh(const double* tris, size_t ntri, sdr_vec3 origin, double d
             CK(cudaMemsetAsync(derr, 0, 4, st));
             CK(cudaMemcpyAsync(dt, tris, ntri * 72, cudaMemcpyHostToDevice, st));
             LAUNCH(k_sdf_mesh, blocks(nn, kSdfBS), kSdfBS, 0, st, dt, (uint32_t)ntri, ntiles, origin.x, origin.y,
-                   origin.z, dx, (int)dims[0], (int)dims[1], (int)dims[2], dout, derr);
+                   origin.z, dx, (int)dims[0], (int)dims[1], (int)dims[2], dout, derr, skip);
             CK(cudaMemcpyAsync(out, dout, nn * 8, cudaMemcpyDeviceToHost, st));
             uint32_t e = 0;
             CK(cudaMemcpyAsync(&e, derr, 4, cudaMemcpyDeviceToHost, st));
@@ -1929,13 +1986,13 @@ int sdr_sdf_from_mesh_noalloc(const double* tris_dev, size_t ntri, sdr_vec3 orig
             throw Fail{SDR_ERR_INVALID, "mesh has " + std::to_string(ntri) + " triangles; the no-allocation scratch holds " +
                                             std::to_string(SDR_NOALLOC_MAX_TRIANGLES)};
         require(((uintptr_t)out_dev & 7) == 0, "out_dev must be 8-byte aligned");
+        const size_t nn = sdf_node_count(dims);
         check_device();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         double* tiles = noalloc_scratch();
         uint32_t* err = reinterpret_cast<uint32_t*>(tiles + kNoAllocTris * 9);
         uint32_t ntiles = (uint32_t)((ntri + kSdfTile - 1) / kSdfTile);
         size_t used = ntri * 9, padded = (size_t)ntiles * kSdfTile * 9;
-        size_t nn = dims[0] * dims[1] * dims[2];
         // The scratch keeps the previous call's contents: overwrite the
         // triangles, zero the padding tail and the error word.
         CK(cudaMemcpyAsync(tiles, tris_dev, used * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1954,8 +2011,8 @@ int sdr_sdf_from_sinus(const sdr_sinus_params* p, sdr_vec3 origin, double dx, co
                        double* out) {
     return guard([&] {
         require(p && dims && out && dx > 0, "bad argument");
+        const size_t nn = sdf_node_count(dims);
         check_device();
-        size_t nn = dims[0] * dims[1] * dims[2];
         double* dout = nullptr;
         cudaStream_t st = nullptr;
         try {

@@ -97,7 +97,9 @@ uint64_t footprint(const sdr_scene_desc& s) {
 }
 
 // One scene end to end: create, frames x (step, record), summary, destroy.
-SceneResult run_scene(const sdr_scene_desc& d, int32_t device) {
+// `shared`: other scenes run beside this one (SDR_SOLVER_SHARED_GPU); a scene
+// alone on the GPU gets the default solver (cluster pressure solve).
+SceneResult run_scene(const sdr_scene_desc& d, int32_t device, bool shared) {
     SceneResult r;
     const auto t0 = Clock::now();
     sdr_solver* s = nullptr;
@@ -109,7 +111,7 @@ SceneResult run_scene(const sdr_scene_desc& d, int32_t device) {
     sdr_solver_options o{};
     o.max_particles = particle_capacity(d);
     o.device = device;
-    o.flags = SDR_SOLVER_BLOCKING_SYNC | SDR_SOLVER_SHARED_GPU;
+    o.flags = SDR_SOLVER_BLOCKING_SYNC | (shared ? SDR_SOLVER_SHARED_GPU : 0);
     int rc = sdr_solver_create(&d.sdf, d.sim_dx, &d.fluid, &d.needle, &o, &s);
     if (rc == SDR_OK && d.has_outlet) rc = sdr_solver_set_outlet(s, &d.outlet);
     if (rc == SDR_OK) rc = sdr_solver_set_solve_params(s, &d.solve);
@@ -215,7 +217,7 @@ struct sdr_server {
             stats.active += 1;
             stats.peak_active = std::max(stats.peak_active, stats.active);
             lk.unlock();
-            SceneResult res = run_scene(r->scene->d, device);
+            SceneResult res = run_scene(r->scene->d, device, true);
             lk.lock();
             r->result = std::move(res);
             r->latency = std::chrono::duration<double>(Clock::now() - r->submitted).count();
@@ -267,7 +269,8 @@ int sdr_batch_run(sdr_batch* b, uint32_t concurrency) {
     const size_t threads = concurrency == 0 ? n : std::min<size_t>(concurrency, n);
     std::atomic<size_t> next{0};
     auto body = [&] {
-        for (size_t i; (i = next.fetch_add(1)) < n;) b->results[i] = run_scene(b->scenes[i]->d, b->device);
+        for (size_t i; (i = next.fetch_add(1)) < n;)
+            b->results[i] = run_scene(b->scenes[i]->d, b->device, threads > 1);
     };
     std::vector<std::thread> pool;
     pool.reserve(threads);

@@ -159,6 +159,19 @@ class Solver:
         check(_lib.load().sdr_solver_get_stats(self._h, C.byref(st)))
         return st
 
+    def cfl(self):
+        """(Solver::cfl_dt, MacGrid::max_speed) of the current state (solver.rs:262-281, grid.rs:202-206)."""
+        dt, gs = C.c_double(), C.c_double()
+        check(_lib.load().sdr_solver_cfl(self._h, C.byref(dt), C.byref(gs)))
+        return dt.value, gs.value
+
+    def cfl_dt(self) -> float:
+        return self.cfl()[0]
+
+    def set_candidate_capacity(self, candidates: int) -> None:
+        """Entries of the redistribution candidate list (0: the particle capacity)."""
+        check(_lib.load().sdr_solver_set_candidate_capacity(self._h, int(candidates)))
+
     def set_dot_order(self, reference_order: bool) -> None:
         """Reference dot order in the PCG (bit-exact pressure) or the faster block tree."""
         check(_lib.load().sdr_solver_set_dot_order(self._h, 1 if reference_order else 0))

@@ -116,3 +116,30 @@ def test_new_entry_points_reject_bad_arguments_without_a_device():
         assert L.sdr_last_error(), i
     img = (C.c_uint8 * 12)()
     assert L.sdr_render_timeseries(None, 0, 10, 10, img, 12) == _lib.SDR_ERR_BUFFER  # needs 300 bytes
+
+
+def test_sdf_entry_points_reject_bad_dims_before_any_device_call():
+    """A zero axis, an axis beyond 2^31-1 or more than 2^37 nodes is refused
+    before any copy or launch (the no-allocation call writes straight into a
+    caller buffer it cannot size). Pointers are never dereferenced here."""
+    import ctypes as C
+
+    from sdr_b200 import _lib
+    lib = _lib.load()
+    fake = C.c_void_p(256)
+    tri = (C.c_double * 9)()
+    for dims in [(0, 4, 4), (4, 4, 0), (2 ** 31, 2, 2), (2 ** 13, 2 ** 13, 2 ** 12)]:
+        d = (C.c_uint64 * 3)(*dims)
+        assert lib.sdr_sdf_from_mesh_noalloc(fake, 1, _lib.Vec3(0, 0, 0), 1.0, d, fake, None) == _lib.SDR_ERR_INVALID
+        assert b"dims" in lib.sdr_last_error() or b"too large" in lib.sdr_last_error()
+        out = (C.c_double * 1)()
+        assert lib.sdr_sdf_from_mesh(tri, 1, _lib.Vec3(0, 0, 0), 1.0, d, out) == _lib.SDR_ERR_INVALID
+
+
+def test_new_solver_entry_points_validate_without_a_device():
+    from sdr_b200 import _lib
+    lib = _lib.load()
+    assert lib.sdr_solver_cfl(None, None, None) == _lib.SDR_ERR_INVALID
+    assert lib.sdr_solver_set_candidate_capacity(None, 10) == _lib.SDR_ERR_INVALID
+    assert lib.sdr_debug_inject(99) == _lib.SDR_ERR_INVALID
+    assert lib.sdr_debug_inject(_lib.FAULT_NONE) == _lib.SDR_OK
