@@ -1,5 +1,5 @@
 """GPU parity of the SDF builders, the cavity volume and the frame metrics,
-plus run-to-run determinism and a whole-run comparison with the oracle."""
+plus run-to-run determinism (whole runs against the oracle: test_gpu_whole_run.py)."""
 import numpy as np
 import pytest
 
@@ -100,49 +100,3 @@ def test_gpu_is_byte_identical_run_to_run():  # solver.rs:1127-1164 on the devic
     for x, y in zip(a, b):
         assert x.shape == y.shape
         assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
-
-
-def _oracle_run(res, round_f32: bool):
-    """The oracle over a whole run; with round_f32 its particle state is rounded
-    to f32 after every substep (the storage precision of the device)."""
-    orc = oracle_solver(res)
-    mo = oracle.Metrics(orc, cavity_volume(res))
-    for f in range(res.frames):
-        remaining, floor = res.frame_dt, res.frame_dt / 512  # solver.rs:248-257
-        while remaining > 1e-12:
-            sub = min(max(orc.cfl_dt(), floor), remaining)
-            orc.substep(sub)
-            remaining -= sub
-            if round_f32:
-                p, v = orc.particles()
-                orc.set_particles(p.astype(np.float32).astype(np.float64), v.astype(np.float32).astype(np.float64))
-        mo.record(orc, f)
-    return mo.summary()
-
-
-def test_whole_run_summary_vs_oracle():
-    """The CI smoke scene (2 mm, 0.5 s, 10 frames) end to end.
-
-    A FLIP jet is chaotic: over ~2500 substeps tiny differences grow, so the
-    whole-run summary is compared against the chaos envelope measured on the
-    oracle itself — the f64 oracle vs the same oracle with its state rounded
-    to f32 every substep. The device must stay within twice that envelope
-    (plus a small absolute floor); emission and mass balance are exact."""
-    from sdr_b200.solver import MetricsCollector, build_scene
-    cfg = sc.SceneConfig.from_toml_str(SMOKE_TOML)
-    res = cfg.resolve()
-    b = build_scene(cfg)
-    mg = MetricsCollector(b.solver, b.cavity_volume)
-    for f in range(res.frames):
-        b.solver.step(res.frame_dt)
-        mg.record(b.solver, f)
-    sg = mg.summary()
-    so = _oracle_run(res, False)
-    sc32 = _oracle_run(res, True)
-    record("whole_run", {"gpu": sg, "orc": so, "orc_f32_state": sc32})
-    assert sg["frames"] == so["frames"]
-    assert abs(sg["injected_ml"] - so["injected_ml"]) < 1e-9
-    assert abs(sg["mass_balance"] - 1.0) < 1e-4
-    for k, floor in (("peak_fill_fraction", 0.005), ("peak_wall_coverage", 0.02), ("total_drained_ml", 0.05)):
-        envelope = abs(sc32[k] - so[k])
-        assert abs(sg[k] - so[k]) <= 2.0 * envelope + floor, (k, sg[k], so[k], sc32[k])

@@ -1,13 +1,19 @@
 """Per-phase parity of the CUDA substep against the CPU oracle (shadow stepping).
 
-Before each phase both solvers hold identical state (the device's f32 values,
-widened to f64 for the oracle); after it the outputs are compared:
+Every phase test runs on each state of tests/gpu_states.py: the CI smoke
+scene, the 0.8 mm parametric jet, the 0.5 mm perturbed-ellipsoid cavity while
+the jet fires and after it has settled, and the 0.2 mm pre-seeded pool of
+9.5 M particles. Before each phase both solvers hold identical state (the
+device's f32 values, widened to f64 for the oracle); after it the outputs are
+compared:
   * integer work (labels, cell keys, the counting-sort permutation, the
-    bounds/compaction map, redistribution moves) — bit-exact;
-  * the pressure solve — bit-exact pressure and iteration count, because the
-    device repeats the reference's f64 arithmetic and dot order;
-  * f32 transfers (P2G, extrapolation, G2P, advection) — relative tolerances
-    stated per assertion, against the oracle's f64 arithmetic.
+    bounds/compaction map, redistribution moves) and the CFL step - bit-exact;
+  * the pressure solve - bit-exact pressure and iteration count with the
+    reference dot order, because the device repeats the reference's f64
+    arithmetic;
+  * f32 transfers (P2G, extrapolation, G2P, advection) - the largest error
+    over every face or particle, within the tolerances stated below, against
+    the oracle's f64 arithmetic.
 """
 import numpy as np
 import pytest
@@ -15,6 +21,7 @@ import pytest
 import oracle
 from sdr_b200 import _lib
 from tests.gpu_common import f32, make_pair, record, rel_err
+from tests.gpu_states import STATES, gpu_to_oracle, make_state, sync_faces
 
 pytestmark = pytest.mark.gpu
 
@@ -26,35 +33,52 @@ VEL_TOL = 2e-5       # particle velocities (relative to max speed)
 POS_TOL = 1e-7       # particle positions, metres (f32 spacing at 2 cm is ~1.9e-9 m)
 
 
-@pytest.fixture(scope="module")
-def pair():
-    gpu, orc, res = make_pair(warm_frames=3)
+@pytest.fixture(scope="module", params=STATES)
+def pair(request):
+    gpu, orc, res = make_state(request.param)
     assert len(gpu) > 100
-    return gpu, orc, res
+    yield gpu, orc, res, request.param
+    gpu.close()
 
 
-def sync_faces(gpu, orc, which=(0, 1, 2, 3, 4, 5)):
-    for w in which:
-        orc.set_face(w, gpu.face(w))
+def test_cfl_step_bit_exact(pair):
+    """cfl_dt (solver.rs:262-281) from MacGrid::max_speed (grid.rs:202-206):
+    the device reduces the face maxima in the last extrapolation sweep and
+    combines them on the host in f64. On the same (f32) faces that is the
+    oracle's dt and grid speed bit for bit; against the oracle's own f64
+    extrapolation the grid speed differs by the f32 rounding of the faces."""
+    gpu, orc, res, name = pair
+    sync_faces(gpu, orc)
+    gpu.run_phase(_lib.PHASE_EXTRAPOLATE)
+    orc.phase(oracle.PHASE_EXTRAPOLATE)
+    own = orc.grid_max_speed()
+    sync_faces(gpu, orc, (0, 1, 2))
+    dt_g, gs_g = gpu.cfl()
+    dt_o, gs_o = orc.cfl_dt(), orc.grid_max_speed()
+    record(f"cfl[{name}]", {"dt_gpu": dt_g, "dt_orc": dt_o, "speed_gpu": gs_g, "speed_orc": gs_o,
+                             "speed_orc_f64_faces": own})
+    assert gs_g == gs_o
+    assert dt_g == dt_o
+    assert abs(gs_g - own) <= 1e-6 * max(own, 1e-30)
 
 
 def test_classify_labels_bit_exact(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     gpu.run_phase(_lib.PHASE_CLASSIFY)
     orc.phase(oracle.PHASE_CLASSIFY)
     g, o = gpu.cells(), orc.cells()
-    record("classify", {"cells": int(g.size), "fluid": int((o == 1).sum()), "mismatch": int((g != o).sum())})
+    record(f"classify[{name}]", {"cells": int(g.size), "fluid": int((o == 1).sum()), "mismatch": int((g != o).sum())})
     assert np.array_equal(g, o)
     assert np.array_equal(gpu.cavity_mask(), orc.cavity_mask())
 
 
 def test_p2g_sort_is_stable_counting_sort(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     gpu.run_phase(_lib.PHASE_P2G)
     keys, perm = gpu.sort()
     # CPU stable counting sort of the same keys
     ref = np.argsort(keys, kind="stable").astype(np.uint32)
-    record("sort", {"n": int(keys.size), "perm_mismatch": int((perm != ref).sum())})
+    record(f"sort[{name}]", {"n": int(keys.size), "perm_mismatch": int((perm != ref).sum())})
     assert np.array_equal(perm, ref)
     # the keys are the f32 cell of each particle (clamped to the grid)
     pos, _ = gpu.particles_f32()
@@ -69,20 +93,20 @@ def test_p2g_sort_is_stable_counting_sort(pair):
 
 
 def test_p2g_faces(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     gpu.run_phase(_lib.PHASE_P2G)
     orc.phase(oracle.PHASE_P2G)
     orc.phase(oracle.PHASE_SAVE_GRID)
     _, vel = gpu.particles()
     vscale = float(np.max(np.abs(vel)))
     errs = {w: float(np.max(np.abs(gpu.face(w) - orc.face(w)))) / vscale for w in range(6)}
-    record("p2g", {"err_over_vmax": errs, "vmax": vscale})
+    record(f"p2g[{name}]", {"err_over_vmax": errs, "vmax": vscale})
     for w in range(6):
         assert errs[w] < P2G_TOL, errs
 
 
 def test_add_forces(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     dt = 1e-4
     sync_faces(gpu, orc)
     gpu.run_phase(_lib.PHASE_ADD_FORCES, dt)
@@ -93,7 +117,7 @@ def test_add_forces(pair):
 
 def test_project_bit_exact_pressure(pair):
     """With the reference dot order the solve is bit-exact: same iterations, same pressure bits."""
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     dt = 1e-4
     gpu.set_dot_order(True)
     gpu.run_phase(_lib.PHASE_CLASSIFY)
@@ -105,7 +129,7 @@ def test_project_bit_exact_pressure(pair):
     it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
     diff = int(np.sum(pg.view(np.uint64) != po.view(np.uint64)))
     errs = {w: rel_err(gpu.face(w), orc.face(w)) for w in range(3)}
-    record("project", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_bit_mismatch": diff,
+    record(f"project[{name}]", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_bit_mismatch": diff,
                        "pressure_rel_err": rel_err(pg, po), "max_p": float(po.max()), "face_rel_err": errs})
     gpu.set_dot_order(False)
     assert it_g == it_o
@@ -220,7 +244,7 @@ PRESSURE_TOL = 1e-8  # block-tree dots: pressure relative to its max, f64
 
 def test_project_tree_dots(pair):
     """The default block-tree dot order: pressure within 1e-8 relative, iterations within one."""
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     dt = 1e-4
     gpu.run_phase(_lib.PHASE_CLASSIFY)
     orc.phase(oracle.PHASE_CLASSIFY)
@@ -230,24 +254,24 @@ def test_project_tree_dots(pair):
     pg, po = gpu.pressure(), orc.pressure()
     it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
     e = rel_err(pg, po)
-    record("project_tree", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_rel_err": e})
+    record(f"project_tree[{name}]", {"iters_gpu": it_g, "iters_orc": it_o, "pressure_rel_err": e})
     assert abs(it_g - it_o) <= 1
     assert e < PRESSURE_TOL
 
 
 def test_extrapolate(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     sync_faces(gpu, orc)
     gpu.run_phase(_lib.PHASE_EXTRAPOLATE)
     orc.phase(oracle.PHASE_EXTRAPOLATE)
     errs = {w: rel_err(gpu.face(w), orc.face(w)) for w in range(3)}
-    record("extrapolate", {"rel_err": errs})
+    record(f"extrapolate[{name}]", {"rel_err": errs})
     for w in range(3):
         assert errs[w] < FACE_TOL
 
 
 def test_g2p(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     sync_faces(gpu, orc)
     pos, vel = gpu.particles()
     orc.set_particles(pos, vel)
@@ -256,12 +280,12 @@ def test_g2p(pair):
     _, vg = gpu.particles()
     _, vo = orc.particles()
     e = rel_err(vg, vo)
-    record("g2p", {"n": int(len(vg)), "vel_rel_err": e})
+    record(f"g2p[{name}]", {"n": int(len(vg)), "vel_rel_err": e})
     assert e < VEL_TOL
 
 
 def test_advect(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     dt = 1e-4
     sync_faces(gpu, orc)
     pos, vel = gpu.particles()
@@ -271,14 +295,13 @@ def test_advect(pair):
     pg, _ = gpu.particles()
     po, _ = orc.particles()
     d = np.max(np.abs(pg - po), axis=1)
-    record("advect", {"n": int(len(d)), "max_abs": float(d.max()), "p99": float(np.quantile(d, 0.99)),
-                      "n_over_tol": int((d > POS_TOL).sum())})
-    assert np.quantile(d, 0.999) < POS_TOL
-    assert (d > 0.5 * res.sim_dx).sum() == 0
+    record(f"advect[{name}]", {"n": int(len(d)), "max_abs": float(d.max()), "p99": float(np.quantile(d, 0.99)),
+                               "n_over_tol": int((d > POS_TOL).sum())})
+    assert d.max() < POS_TOL
 
 
 def test_bounds_compaction_exact(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     pos, vel = gpu.particles()
     orc.set_particles(pos, vel)
     d0g, d0o = gpu.drained, orc.scalars()["drained"]
@@ -286,7 +309,7 @@ def test_bounds_compaction_exact(pair):
     orc.phase(oracle.PHASE_BOUNDS)
     pg, vg = gpu.particles()
     po, vo = orc.particles()
-    record("bounds", {"n_gpu": int(len(pg)), "n_orc": int(len(po)), "drained_gpu": gpu.drained - d0g,
+    record(f"bounds[{name}]", {"n_gpu": int(len(pg)), "n_orc": int(len(po)), "drained_gpu": gpu.drained - d0g,
                       "drained_orc": orc.scalars()["drained"] - d0o})
     assert len(pg) == len(po)
     assert np.array_equal(pg, po)  # same survivors, same order, same (f32) values
@@ -294,7 +317,7 @@ def test_bounds_compaction_exact(pair):
 
 
 def test_redistribute_moves_exact(pair):
-    gpu, orc, res = pair
+    gpu, orc, res, name = pair
     sync_faces(gpu, orc)
     pos, vel = gpu.particles()
     orc.set_particles(pos, vel)
@@ -305,7 +328,7 @@ def test_redistribute_moves_exact(pair):
     moved_g = np.any(pg != pos, axis=1)
     moved_o = np.any(po != pos, axis=1)
     d = np.max(np.abs(pg - po), axis=1)
-    record("redistribute", {"moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
+    record(f"redistribute[{name}]", {"moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
                             "max_abs_pos": float(d.max()) if len(d) else 0.0,
                             "vel_rel_err": rel_err(vg, vo)})
     assert np.array_equal(moved_g, moved_o)
@@ -354,22 +377,40 @@ def test_redistribute_long_candidate_list_exact():
     assert d.max() < POS_TOL
 
 
-def test_full_substep_shadow():
-    """One full substep from identical state: counts, labels and particle state."""
-    gpu, orc, res = make_pair(warm_frames=4)
+SUB_POS_TOL = 1e-7      # one whole substep: particle positions, metres (max over particles)
+SUB_VEL_TOL = 2e-5      # velocities, relative to the largest speed (max over particles)
+SUB_PRESSURE_TOL = 1e-6  # pressure, relative to its largest value: the f32 faces of P2G move the RHS
+
+
+def test_full_substep_shadow(pair):
+    """One full substep from identical state: particle count, labels and
+    drained count exactly; every particle's position and velocity and the
+    pressure of every cell within the stated bounds."""
+    gpu, orc, res, name = pair
+    gpu_to_oracle(gpu, orc)
+    sync_faces(gpu, orc)
     dt = orc.cfl_dt()
     gpu.substep(dt)
     orc.substep(dt)
     pg, vg = gpu.particles()
     po, vo = orc.particles()
+    pr_g, pr_o = gpu.pressure(), orc.pressure()
     rec = {"n_gpu": int(len(pg)), "n_orc": int(len(po)), "iters_gpu": gpu.last_pcg_iters,
-           "iters_orc": orc.scalars()["last_pcg_iters"], "dt": dt}
+           "iters_orc": orc.scalars()["last_pcg_iters"], "dt": dt, "drained_gpu": gpu.drained,
+           "drained_orc": orc.scalars()["drained"]}
     if len(pg) == len(po):
         d = np.max(np.abs(pg - po), axis=1)
-        rec.update(pos_max=float(d.max()), pos_p999=float(np.quantile(d, 0.999)), vel_rel=rel_err(vg, vo),
-                   pressure_rel=rel_err(gpu.pressure(), orc.pressure()))
-    record("full_substep", rec)
+        vscale = max(float(np.max(np.abs(vo))), 1e-30)
+        dv = np.max(np.abs(vg - vo), axis=1) / vscale
+        dp = np.abs(pr_g - pr_o) / max(float(np.max(np.abs(pr_o))), 1e-30)
+        rec.update(pos_max=float(d.max()), pos_p99=float(np.quantile(d, 0.99)),
+                   vel_rel_max=float(dv.max()), vel_rel_p99=float(np.quantile(dv, 0.99)),
+                   pressure_rel_max=float(dp.max()), pressure_rel_p99=float(np.quantile(dp, 0.99)),
+                   vmax=vscale, pmax=float(np.max(np.abs(pr_o))))
+    record(f"full_substep[{name}]", rec)
     assert len(pg) == len(po)
+    assert gpu.drained == orc.scalars()["drained"]
     assert np.array_equal(gpu.cells(), orc.cells())
-    assert np.quantile(d, 0.99) < 1e-6
-    assert rec["pressure_rel"] < 1e-3
+    assert rec["pos_max"] < SUB_POS_TOL
+    assert rec["vel_rel_max"] < SUB_VEL_TOL
+    assert rec["pressure_rel_max"] < SUB_PRESSURE_TOL

@@ -1,12 +1,15 @@
 """The no-allocation SDF entry point against the allocating one.
 
 sdr_sdf_from_mesh_noalloc serves callers that cannot allocate device memory
-(a fixed device-memory budget handed out up front, work issued during stream
-capture, loops that cannot take cudaMalloc's synchronisation): it reads and
-writes caller-owned device buffers and keeps its scratch in a static device
-array. Both entry points run the same kernel, so their outputs must agree bit
-for bit, on every call (the scratch keeps the previous call's contents).
-This file is collected last so a failure here comes after every other test.
+(a process that carves its whole device-memory budget into a pool at start-up
+and must not grow it, loops that cannot take cudaMalloc's synchronisation): it
+reads and writes caller-owned device buffers and keeps its scratch in a static
+device array. Both entry points run the same kernel, so their outputs must
+agree bit for bit on every call, including a smaller mesh after a larger one
+(the scratch keeps the previous call's contents, and the padding of the last
+staging tile must be cleared again). Free device memory does not change
+across the calls. This file is collected last so a failure here comes after
+every other test.
 """
 import ctypes as C
 
@@ -24,23 +27,37 @@ def test_noalloc_sdf_matches_allocating_entry_point():
     from sdr_b200.solver import sdf_from_mesh
 
     lib = _lib.load()
-    cav = perturbed_ellipsoid(11, subdiv=3)
     dx, pad = 1.0e-3, 3.0e-3
-    ref = sdf_from_mesh(cav.tris, dx, pad)  # the allocating entry point
-    nz, ny, nx = ref.data.shape
-    dims = (C.c_uint64 * 3)(nx, ny, nz)
-    origin = _lib.Vec3(*ref.origin)
-    tris_dev = torch.tensor(np.ascontiguousarray(cav.tris), dtype=torch.float64, device="cuda")
-    out_dev = torch.empty(nx * ny * nz, dtype=torch.float64, device="cuda")
+    # a mesh of whole staging tiles (1280 triangles), then a smaller ragged one (320)
+    meshes = [perturbed_ellipsoid(11, subdiv=3), perturbed_ellipsoid(12, subdiv=2)]
+    assert len(meshes[0].tris) % 128 == 0 and len(meshes[1].tris) % 128 != 0
+    refs = [sdf_from_mesh(m.tris, dx, pad) for m in meshes]  # the allocating entry point
     stream = torch.cuda.current_stream().cuda_stream
-    for call in range(2):
+    bufs = []
+    for m, ref in zip(meshes, refs):
+        nz, ny, nx = ref.data.shape
+        bufs.append((torch.tensor(np.ascontiguousarray(m.tris), dtype=torch.float64, device="cuda"),
+                     torch.empty(nx * ny * nz, dtype=torch.float64, device="cuda")))
+    torch.cuda.synchronize()
+    free0 = alloc0 = None
+    # call 0 does the first-call set-up (the scratch address lookup); free
+    # memory is taken after it and must not move over the calls that follow
+    for call, k in enumerate([0, 0, 1, 0, 1]):
+        ref, (tris_dev, out_dev) = refs[k], bufs[k]
+        nz, ny, nx = ref.data.shape
+        dims = (C.c_uint64 * 3)(nx, ny, nz)
         out_dev.fill_(float("nan"))
         torch.cuda.synchronize()
-        rc = lib.sdr_sdf_from_mesh_noalloc(C.c_void_p(tris_dev.data_ptr()), len(cav.tris), origin, dx, dims,
-                                           C.c_void_p(out_dev.data_ptr()), C.c_void_p(stream))
+        rc = lib.sdr_sdf_from_mesh_noalloc(C.c_void_p(tris_dev.data_ptr()), len(meshes[k].tris), _lib.Vec3(*ref.origin),
+                                           dx, dims, C.c_void_p(out_dev.data_ptr()), C.c_void_p(stream))
         _lib.check(rc)
         got = out_dev.cpu().numpy().reshape(nz, ny, nx)
-        assert np.array_equal(got.view(np.uint64), ref.data.view(np.uint64)), f"call {call} differs"
+        assert np.array_equal(got.view(np.uint64), ref.data.view(np.uint64)), f"call {call} (mesh {k}) differs"
+        if call == 0:
+            free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+        else:
+            assert torch.cuda.mem_get_info()[0] == free0, f"call {call} changed free device memory"
+            assert torch.cuda.memory_allocated() == alloc0
 
 
 def test_noalloc_rejects_meshes_beyond_the_scratch():
