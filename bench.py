@@ -1,41 +1,50 @@
 #!/usr/bin/env python
 """Benchmark: particle-substeps/s of the FLIP/PIC substep on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sdr|reference] [--workload real_cavity]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sdr|reference]
 
-A step is one output frame (Solver::step(frame_dt), all its CFL substeps) of
-the workload. W frames warm up, K frames are timed. ``value`` is device time
-(CUDA events on the solver stream, summed over the timed frames, max over
-ranks); ``e2e`` is the same frames timed on the host around the public call
-plus the per-frame read-back of particle positions (host buffers). Between
-timed frames a 256 MiB buffer is written to flush L2.
+Headline (``value``): the largest single-GPU workload, ``pool_0p2mm`` - the
+`sdr init` parametric sinus at 0.2 mm (207 x 217 x 161 = 7.23 M cells, 6 ml/s
+jet, PCG capped at 400 iterations) holding a pre-seeded pool of 9.5 M
+particles at rest (the deepest cavity cells filled at 8 particles per cell
+with hash_jitter offsets). A step is one Solver::substep at the jet's CFL step
+(dx / jet speed). W warm-up substeps run from the pre-seeded state, then the
+state is put back (particles and scalars) and K substeps are timed from it, so
+the timed window is the same for every run and for the reference arm. The
+state (1.5 GB on the device) is far larger than the 126 MB L2, so no flush is
+needed between steps.
 
-Multi-GPU runs are independent scene replicas (one per rank, different cavity
-seeds): no collective on the data path; a barrier and a max-reduce of the
-timings use torch.distributed.
+``value`` is device time: CUDA events on the solver stream around every
+substep, summed, max over ranks. ``e2e`` times the same substeps on the host
+around the public call (sdr_solver_substep: the emitted particles' host ->
+device upload and the device -> host status read of every substep inside).
 
 ``--impl reference`` times the CPU restatement of the reference solver
-(oracle/, the reference Rust cannot be built here) on the host cores: W
-frames from t = 0 to reach the timed window, then K bounded samples.
+(oracle/; the reference is Rust and cannot be built here) on all host threads,
+from the identical pre-seeded state at the same dt: a bounded sample of the
+first ``--ref-substeps`` substeps of the window (one oracle substep takes
+~14 s on 16 threads).
 
-``batched`` and ``served`` (one GPU): a bounded sample of the batched scene
-family (seeded perturbed-ellipsoid cavities, grids log-uniform in 32^3..96^3
-cells, random needle tilt, flow and dose). Each of ``--batch-scenes`` scenes
-runs one frame of ``--batch-cfl`` jet-CFL steps (frame_dt = n * dx / jet
-speed), so that per-scene work varies with the grid alone instead of being
-dominated by the finest, fastest jets. The scenes run one after another
-through the public calls (the plain path), all at once (sdr_batch_run), and as
-Poisson arrivals into the request server (sdr_server_*, 150 GB admission
-budget) with p50/p99 time-to-summary.
+Extra records on one GPU:
+``parametric_0p8mm`` the parametric sinus at 0.8 mm, 4 ml/s, the whole 0.5 s
+                   (15 frames) timed frame by frame after a warm-up run, with
+                   the per-frame read-back of positions; the oracle continues
+                   from the mid-run state for a bounded sample.
+``cavity_0p5mm``   the perturbed-ellipsoid cavity (2.2 ml, 20,480 triangles,
+                   winding-number SDF at 0.5 mm), 1 ml at 4 ml/s, the whole
+                   0.6 s (18 frames), timed the same way.
+``batched``/``served`` a bounded sample of the batched scene family (seeded
+                   perturbed-ellipsoid cavities, grids log-uniform in
+                   32^3..96^3 cells, needle tilt, flow and dose drawn per
+                   scene): one after another on default solvers (the plain
+                   path), all at once (sdr_batch_run), and as Poisson
+                   arrivals into the request server with p50/p99
+                   time-to-summary.
+``render``         preview images (600 px) of the cavity run's final state
+                   beside the oracle drawing the same state.
 
-``render``: preview images (render_slice, 600 px) of the final state, the
-slice through the needle tip and the gravity projection, timed through the
-public call, beside the oracle drawing the same state.
-
-``large`` (one GPU): the 0.2 mm parametric cavity (207 x 217 x 161 cells)
-with a pre-seeded pool of 9.5 M particles at rest, ``--large-substeps``
-substeps at the fixed jet CFL step after ``--large-warmup``, device-timed;
-the oracle times one substep of the identical state.
+Multi-GPU runs are independent replicas (one pool per rank): no collective on
+the data path; a barrier and a max-reduce of the timings use torch.distributed.
 """
 from __future__ import annotations
 
@@ -54,11 +63,15 @@ sys.path.insert(0, ROOT)
 # queues than the default 8 (read when the CUDA context is created).
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
-# Algorithmic bytes of the pressure solve (the dominant kernel, k_pcg), f64
-# vectors in wavefront order: per fluid cell and PCG iteration, and per fluid
-# cell once per solve (factorisation, first preconditioner application, setup).
+# Algorithmic bytes of the pressure solve (the dominant kernel), f64 vectors in
+# wavefront order: per fluid cell and PCG iteration (matvec 41, dot 20, p/r
+# update 48, forward sweep 44, backward sweep 36, second dot 20, direction 24)
+# and per fluid cell once per solve (factorisation, first preconditioner
+# application, setup).
 PCG_BYTES_PER_CELL_ITER = 233
 PCG_BYTES_PER_CELL_SOLVE = 190
+POOL_TARGET = 30_000_000   # particles asked for; the cavity holds 9.5 M at 8 per cell
+POOL_CAPACITY = 12_000_000
 
 
 def dist_env():
@@ -93,6 +106,15 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    this kernel on this workload from the committed ncu summaries, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    return json.load(open(p)).get(f"{kernel}@{workload}")
 
 
 class Clocks:
@@ -130,6 +152,23 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# ---------------------------------------------------------------- the pool workload
+def pool_config(w, grid, particles: int, dt: float) -> dict:
+    """The headline's config, identical in both arms."""
+    return {"workload": "pool_0p2mm", "cavity": "parametric sinus (sdr init defaults)", "dx_mm": 0.2,
+            "grid": [int(v) for v in grid], "particles": int(particles),
+            "state": "pre-seeded pool at rest, 8 particles per cell (hash_jitter offsets), deepest cavity cells first",
+            "flow_ml_s": 6.0, "dt_s": dt, "dt_rule": "jet CFL step dx / jet speed",
+            "pcg_iters_cap": int(w.res.solve.max_iters), "pcg_tol": float(w.res.solve.tol),
+            "window": "substeps 1..K from the pre-seeded state",
+            "l2": "state 1.5 GB, larger than the 126 MB L2 (no flush)"}
+
+
+def jet_dt(needle, dx: float) -> float:
+    import math
+    return dx / (needle.flow_rate / (math.pi * needle.radius ** 2))
+
+
 def oracle_for(w, sdf):
     import oracle
     from tests.helpers import oracle_solver
@@ -137,60 +176,231 @@ def oracle_for(w, sdf):
     return oracle_solver(w.res, osdf)
 
 
-def cpu_sample(orc, budget_s: float, max_substeps: int):
-    """Run the oracle for a bounded sample; returns (particle_substeps, seconds, substeps)."""
-    t0 = time.perf_counter()
-    ps = sub = 0
-    while sub < max_substeps and time.perf_counter() - t0 < budget_s:
-        dt = orc.cfl_dt()
-        ps += len(orc) + 0
-        orc.substep(dt)
-        sub += 1
-    return ps, time.perf_counter() - t0, sub
-
-
 def run_reference(args):
-    """CPU restatement of the reference (all host threads), same workload and metric."""
+    """The oracle on the host cores: the pre-seeded pool, the same dt, the first
+    --ref-substeps substeps of the GPU arm's window."""
+    import numpy as np
+
     import oracle
     from sdr_b200 import workloads
-    from sdr_b200.solver import Sdf
-    w = workloads.WORKLOADS[args.workload]()
-    # The reference arm builds its SDF with the oracle's own winding-number/implicit code.
-    if w.res.sinus is not None:
-        osdf = oracle.sdf_from_sinus(w.res.sinus, w.res.sdf_origin, w.res.sdf_dx, w.res.sdf_dims)
-    else:
-        osdf = oracle.sdf_from_mesh(w.tris, w.res.sdf_dx, w.res.mesh_padding)
+    from tests.helpers import oracle_solver
+    w = workloads.large_parametric()
+    res = w.res
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    from tests.helpers import oracle_solver
-    orc = oracle_solver(w.res, osdf)
-    for _ in range(args.warmup):
-        orc.step(w.res.frame_dt)
-    ps_tot = 0
-    t_tot = 0.0
-    subs = 0
-    for _ in range(args.steps):
-        ps, t, sub = cpu_sample(orc, budget_s=args.ref_budget, max_substeps=args.ref_substeps)
-        ps_tot += ps
-        t_tot += t
-        subs += sub
-    v = ps_tot / t_tot if t_tot > 0 else 0.0
-    sample = (f"{args.warmup} frames from t=0 (untimed), then {args.steps} samples of up to "
-              f"{args.ref_substeps} substeps ({subs} substeps, {ps_tot} particle-substeps)")
+    osdf = oracle.sdf_from_sinus(res.sinus, res.sdf_origin, res.sdf_dx, res.sdf_dims)
+    orc = oracle_solver(res, osdf)
+    (nx, ny, nz), origin, dx = orc.grid
+    pos, vel = workloads.preseed_pool_on((nx, ny, nz), origin, dx, res.fluid.gravity, orc.cavity_mask(),
+                                         POOL_TARGET)
+    pos = pos.astype(np.float32).astype(np.float64)
+    orc.set_particles(pos, vel)
+    dt = jet_dt(res.needle, dx)
+    n_sub = max(1, min(args.steps, args.ref_substeps))
+    ps, t = 0, 0.0
+    for _ in range(n_sub):
+        ps += len(orc)
+        t0 = time.perf_counter()
+        orc.substep(dt)
+        t += time.perf_counter() - t0
+    v = ps / t
+    sample = (f"the first {n_sub} substeps of the timed window from the identical pre-seeded state "
+              f"({ps} particle-substeps, {t:.1f} s); C++ restatement of the reference solver (the Rust "
+              "reference cannot be built here), f64, rayon-parallel parts on all host threads")
     line = {"metric": "particle-substeps/s", "value": v, "unit": "particle-substeps/s", "impl": "reference",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / max(args.steps, 1),
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / n_sub,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": w.name, **(w.describe or {})},
+            "data": "synthetic", "config": pool_config(w, (nx, ny, nz), len(pos), dt),
             "cpu_baseline": {"value": v, "unit": "particle-substeps/s", "cores": threads, "kind": "port",
-                             "sample": sample + "; C++ restatement of the reference solver (Rust not buildable)"},
+                             "sample": sample},
             "e2e": {"value": v, "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
+def pool_line(args, rank, world, local):
+    """The headline measurement (see the module docstring)."""
+    import numpy as np
+    import torch
+
+    from sdr_b200 import _lib, workloads
+    w = workloads.large_parametric()
+    t0 = time.perf_counter()
+    solver, sdf, vol = workloads.build_gpu(w, max_particles=POOL_CAPACITY)
+    pos, vel = workloads.preseed_pool(solver, POOL_TARGET)
+    pos = pos.astype(np.float32).astype(np.float64)  # the stored (f32) state, shared with the oracle
+    setup_s = time.perf_counter() - t0
+    dt = jet_dt(solver.needle, solver.dx)
+    st_init = solver.stats()
+
+    def reset():
+        solver.set_particles(pos, vel)
+        solver.set_scalars(st_init.time, st_init.emit_accum, st_init.steps, st_init.drained, st_init.rng_state)
+
+    solver.set_profiling(True)
+    reset()
+    for _ in range(args.warmup):
+        solver.substep(dt)
+    reset()
+    solver.reset_profile()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    launches0 = _lib.load().sdr_kernel_launch_count()
+    clk = Clocks(local)
+    st0 = solver.stats()
+    wall = 0.0
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        solver.substep(dt)  # public call: emission upload and status read inside
+        wall += time.perf_counter() - t1
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clk.stop()
+    st1 = solver.stats()
+    launches = _lib.load().sdr_kernel_launch_count() - launches0
+    prof = solver.profile()
+    dev_ms = st1.device_ms - st0.device_ms
+    local_dev_ms = dev_ms
+    ps = st1.particle_substeps - st0.particle_substeps
+    if world > 1:
+        dev_ms, wall, ps = reduce_over_ranks(dev_ms, wall, ps, "cuda")
+    value = ps / (dev_ms / 1e3)
+    e2e = ps / wall
+    hbm, peak_kind = peaks()
+    n_pcg = max(prof["pcg_launches"], 1)
+    if prof.get("pcg_tile_launches", 0) == prof["pcg_launches"]:
+        kernel = "k_pcg_tiles"
+    elif prof["pcg_cluster_launches"] == prof["pcg_launches"]:
+        kernel = "k_pcg_cluster"
+    else:
+        kernel = "k_pcg"
+    pcg_launch_ms = prof["pcg_ms"] / n_pcg
+    pcg_bytes = (PCG_BYTES_PER_CELL_ITER * prof["pcg_cell_iters"] + PCG_BYTES_PER_CELL_SOLVE * prof["fluid_cells"]) / n_pcg
+    achieved = pcg_bytes / (pcg_launch_ms / 1e3) / 1e9 if pcg_launch_ms > 0 else 0.0
+    traffic = measured_traffic(kernel, "pool_0p2mm")
+    sub_bytes = substep_bytes(prof["particles"], prof["substeps"], int(st1.nx * st1.ny * st1.nz),
+                              int(sdf.data.size), prof["pcg_cell_iters"])
+    sub_gbs = sub_bytes / (local_dev_ms / 1e3) / 1e9 if local_dev_ms > 0 else 0.0  # this rank's substeps
+    line = {"metric": "particle-substeps/s", "value": value, "unit": "particle-substeps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "config": pool_config(w, (st1.nx, st1.ny, st1.nz), len(pos), dt),
+            "e2e": {"value": e2e, "unit": "particle-substeps/s",
+                    "h2d_bytes_per_step": int(prof["h2d_bytes"] / args.steps),
+                    "d2h_bytes_per_step": int(prof["d2h_bytes"] / args.steps)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "traffic": traffic["bytes_per_launch"] if traffic else None,
+                         "traffic_source": traffic["source"] if traffic else None,
+                         "bytes_per_launch": pcg_bytes, "ms_per_launch": pcg_launch_ms,
+                         "bytes": f"{PCG_BYTES_PER_CELL_ITER} B per fluid cell per iteration + "
+                                  f"{PCG_BYTES_PER_CELL_SOLVE} B per fluid cell per solve"},
+            "substep_roofline": {"bound": "hbm", "achieved": sub_gbs, "peak": hbm, "unit": "GB/s",
+                                 "frac": sub_gbs / hbm, "peak_kind": peak_kind,
+                                 "bytes_per_substep": sub_bytes / max(prof["substeps"], 1),
+                                 "bytes": "112 P + 92 C + 4 S + 83 N_f iters per substep"},
+            "phase_ms_per_substep": {k: round(v / max(prof["substeps"], 1), 3) for k, v in prof.items()
+                                     if k.endswith("_ms")},
+            "pcg": {"launches": prof["pcg_launches"], "kernel": kernel,
+                    "mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
+                    "mean_fluid_cells": prof["fluid_cells"] / n_pcg},
+            "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
+                               "long_sweeps": prof["redist_long_sweeps"]},
+            "setup_s": setup_s}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        orc = oracle_for(w, sdf)
+        orc.set_particles(pos, vel)
+        t1 = time.perf_counter()
+        orc.substep(dt)
+        ct = time.perf_counter() - t1
+        line["cpu_baseline"] = {"value": len(pos) / ct, "unit": "particle-substeps/s", "cores": threads,
+                                "kind": "port", "sample": f"substep 1 of the timed window from the identical "
+                                                          f"pre-seeded state ({ct:.1f} s); C++ restatement of the "
+                                                          "reference solver, f64, on all host threads"}
+        del orc
+    solver.close()
+    return line
+
+
+# ---------------------------------------------------------------- frame-based runs
+def frame_record(w, key: str, cpu: bool, cpu_budget: float):
+    """A whole run of a scene (every frame) timed frame by frame after a
+    warm-up run of two frames on another solver; between frames a 256 MiB
+    buffer is written to flush L2 (these states are smaller than L2)."""
+    import torch
+
+    from sdr_b200 import workloads
+    warm, _, _ = workloads.build_gpu(w)
+    for _ in range(2):
+        warm.step(w.res.frame_dt)
+    warm.close()
+    solver, sdf, vol = workloads.build_gpu(w)
+    solver.set_profiling(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    dev_ms = wall = 0.0
+    ps = 0
+    mid = None
+    for f in range(w.res.frames):
+        flush.zero_()
+        torch.cuda.synchronize()
+        st0 = solver.stats()
+        t0 = time.perf_counter()
+        solver.step(w.res.frame_dt)
+        pos, _ = solver.particles_f32()  # the per-frame read-back of cmd_simulate's output
+        wall += time.perf_counter() - t0
+        st1 = solver.stats()
+        dev_ms += st1.device_ms - st0.device_ms
+        ps += st1.particle_substeps - st0.particle_substeps
+        if f == w.res.frames // 2 and cpu:
+            p, v = solver.particles()
+            mid = (p, v, st1)
+    prof = solver.profile()
+    st = solver.stats()
+    out = {"workload": key, **(w.describe or {}), "grid": [st.nx, st.ny, st.nz], "frames": w.res.frames,
+           "substeps": int(prof["substeps"]), "particles_end": int(st.particles),
+           "particle_substeps_per_s": ps / (dev_ms / 1e3), "e2e_particle_substeps_per_s": ps / wall,
+           "device_s": dev_ms / 1e3, "wall_s": wall,
+           "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
+           "pcg": {"mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
+                   "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1)},
+           "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"]},
+           "mass": {"emitted": st.emitted, "resident": st.particles, "drained": st.drained, "culled": st.culled}}
+    if cpu and mid is not None:
+        import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        orc = oracle_for(w, sdf)
+        p, v, s = mid
+        orc.set_particles(p, v)
+        orc.set_scalars(s.time, s.emit_accum, s.steps, s.drained, s.rng_state)
+        t0 = time.perf_counter()
+        cps = csub = 0
+        while time.perf_counter() - t0 < cpu_budget:
+            dt = orc.cfl_dt()
+            cps += len(orc)
+            orc.substep(dt)
+            csub += 1
+        ct = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cps / ct, "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+                               "sample": f"{csub} substeps from the mid-run state (frame {w.res.frames // 2}), "
+                                         f"{ct:.1f} s"}
+        out["speedup_vs_cpu"] = out["particle_substeps_per_s"] / out["cpu_baseline"]["value"]
+        out["e2e_speedup_vs_cpu"] = out["e2e_particle_substeps_per_s"] / out["cpu_baseline"]["value"]
+    return {key: out}, solver, sdf
+
+
 def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
-    """Plain (one scene after another), batched and served runs of the same scenes."""
+    """Plain (one scene after another, default solvers), batched and served runs of the same scenes."""
     import math
     import random
+
     from sdr_b200 import _lib, workloads
     from sdr_b200.serving import Server, run_batch
     t0 = time.perf_counter()
@@ -236,6 +446,7 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
         "batched": {"scenes": n_scenes, "cfl_steps_per_scene": cfl_steps, "sample": sample,
                     "plain_scenes_per_s": n_scenes / t_plain, "batched_scenes_per_s": n_scenes / t_mix,
                     "speedup": t_plain / t_mix, "plain_s": t_plain, "batched_s": t_mix,
+                    "plain_solver": "default (sdr_solver_create flags 0)",
                     "particle_substeps_per_s": ps / t_mix, "substeps": subs, "results_identical": same},
         "served": {"arrivals": "poisson", "rate_per_s": rate, "scenes_per_s": n_scenes / t_srv,
                    "p50_time_to_summary_s": pct(0.5), "p99_time_to_summary_s": pct(0.99),
@@ -273,79 +484,19 @@ def render_bench(solver, w, sdf, cpu: bool, px: int = 600, reps: int = 5) -> dic
     return {"render": out}
 
 
-def large_bench(n_sub: int, warm: int, cpu: bool) -> dict:
-    """The 0.2 mm parametric cavity (207 x 217 x 161 cells) with a pre-seeded
-    pool: the deepest cavity cells filled at 8 particles per cell with
-    hash_jitter offsets, at rest (9.5 M particles, the cavity holds fewer than
-    the 30 M asked for), then substeps at the fixed jet CFL step. Inputs are far
-    larger than L2. The oracle times one substep of the identical state."""
-    import numpy as np
-    from sdr_b200 import workloads
-    w = workloads.large_parametric()
-    t0 = time.perf_counter()
-    solver, sdf, vol = workloads.build_gpu(w, max_particles=12_000_000)
-    pos, vel = workloads.preseed_pool(solver, 30_000_000)
-    pos = pos.astype(np.float32).astype(np.float64)  # the stored (f32) state, shared with the oracle
-    solver.set_particles(pos, vel)
-    setup_s = time.perf_counter() - t0
-    jet = solver.needle.flow_rate / (np.pi * solver.needle.radius ** 2)
-    dt = solver.dx / jet
-    solver.set_profiling(True)
-    for _ in range(warm):
-        solver.substep(dt)
-    solver.reset_profile()
-    st0 = solver.stats()
-    t0 = time.perf_counter()
-    for _ in range(n_sub):
-        solver.substep(dt)
-    wall = time.perf_counter() - t0
-    st1 = solver.stats()
-    prof = solver.profile()
-    dev_ms = st1.device_ms - st0.device_ms
-    ps = st1.particle_substeps - st0.particle_substeps
-    out = {"workload": "large_parametric, pre-seeded pool", "grid": [st1.nx, st1.ny, st1.nz],
-           "particles": int(len(pos)), "dt_s": dt, "warmup_substeps": warm, "substeps": n_sub,
-           "particle_substeps_per_s": ps / (dev_ms / 1e3), "wall_particle_substeps_per_s": ps / wall,
-           "ms_per_substep": dev_ms / n_sub, "setup_s": setup_s,
-           "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
-           "pcg": {"mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
-                   "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1),
-                   "cluster_launches": prof["pcg_cluster_launches"]},
-           "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
-                              "long_sweeps": prof["redist_long_sweeps"]}}
-    solver.close()
-    if cpu:
-        import oracle
-        orc = oracle_for(w, sdf)
-        orc.set_particles(pos, vel)
-        threads = os.cpu_count() or 1
-        oracle.set_threads(threads)
-        t0 = time.perf_counter()
-        orc.substep(dt)
-        ct = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": len(pos) / ct, "unit": "particle-substeps/s", "cores": threads,
-                               "kind": "port", "sample": f"one substep of the pre-seeded state ({ct:.1f} s); "
-                                                         "C++ restatement of the reference solver, f64"}
-    return {"large": out}
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sdr", choices=["sdr", "reference"])
-    ap.add_argument("--workload", default="real_cavity")
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of oracle time for cpu_baseline")
-    ap.add_argument("--ref-budget", type=float, default=20.0)
-    ap.add_argument("--ref-substeps", type=int, default=20)
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of oracle time per extra record")
+    ap.add_argument("--ref-substeps", type=int, default=4, help="substeps the reference arm times")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="headline only")
     ap.add_argument("--batch-scenes", type=int, default=48)
     ap.add_argument("--batch-cfl", type=int, default=150)
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--no-large", action="store_true")
-    ap.add_argument("--large-substeps", type=int, default=5)
-    ap.add_argument("--large-warmup", type=int, default=3)
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -354,120 +505,26 @@ def main():
             run_reference(args)
         return
 
-    import numpy as np
     import torch
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from sdr_b200 import _lib, workloads
-
-    w = workloads.WORKLOADS[args.workload]() if args.workload != "real_cavity" else workloads.real_cavity(seed=2 + rank)
-    solver, sdf, vol = workloads.build_gpu(w)
-    solver.set_profiling(True)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
-        solver.step(w.res.frame_dt)
-    solver.reset_profile()
-    launches0 = _lib.load().sdr_kernel_launch_count()
-    clk = Clocks(local)
-    dev_ms = 0.0
-    wall = 0.0
-    ps = 0
-    h2d = 0
-    d2h = 0
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        st0 = solver.stats()
-        t0 = time.perf_counter()
-        solver.step(w.res.frame_dt)          # public API: host emission uploads inside
-        pos, _ = solver.particles_f32()      # per-frame result read-back (positions)
-        t1 = time.perf_counter()
-        st1 = solver.stats()
-        dev_ms += st1.device_ms - st0.device_ms
-        wall += t1 - t0
-        ps += st1.particle_substeps - st0.particle_substeps
-        h2d += (st1.emitted - st0.emitted) * 32 + (st1.substeps_total - st0.substeps_total) * 4
-        d2h += pos.nbytes * 2 + (st1.substeps_total - st0.substeps_total) * 96
-    torch.cuda.synchronize()
-    clocks = clk.stop()
-    launches = _lib.load().sdr_kernel_launch_count() - launches0
-    prof = solver.profile()
-    # One more frame, not timed, with the section timers inside the pressure
-    # solve switched on (they sit on its critical path, so the timed frames
-    # run without them): the per-section cycle split of k_pcg.
-    solver.reset_profile()
-    solver.set_profiling(True, kernel_timers=True)
-    solver.step(w.res.frame_dt)
-    diag = solver.profile()
-    solver.set_profiling(False)
-    if world > 1:
-        dev_ms, wall, ps = reduce_over_ranks(dev_ms, wall, ps, "cuda")
-    value = ps / (dev_ms / 1e3)
-    e2e = ps / wall
-    hbm, peak_kind = peaks()
-    pcg_launch_ms = prof["pcg_ms"] / max(prof["pcg_launches"], 1)
-    pcg_bytes = (PCG_BYTES_PER_CELL_ITER * prof["pcg_cell_iters"] + PCG_BYTES_PER_CELL_SOLVE * prof["fluid_cells"]) / max(prof["pcg_launches"], 1)
-    achieved = pcg_bytes / (pcg_launch_ms / 1e3) / 1e9 if pcg_launch_ms > 0 else 0.0
-    st = solver.stats()
-    sub_bytes = substep_bytes(prof["particles"], prof["substeps"], int(st.nx * st.ny * st.nz),
-                              int(sdf.data.size), prof["pcg_cell_iters"])
-    sub_gbs = sub_bytes / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else 0.0  # rank 0's substeps, rank 0's time at N = 1
-    line = {"metric": "particle-substeps/s", "value": value, "unit": "particle-substeps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": w.name, **(w.describe or {}), "grid": [st.nx, st.ny, st.nz],
-                       "particles_end": int(st.particles), "substeps": int(prof["substeps"]),
-                       "l2": "256 MiB buffer written between timed frames", "replicas": world},
-            "e2e": {"value": e2e, "unit": "particle-substeps/s", "h2d_bytes_per_step": int(h2d / args.steps),
-                    "d2h_bytes_per_step": int(d2h / args.steps)},
-            "gpu_launches": int(launches),
-            "clocks": clocks,
-            "roofline": {"bound": "hbm", "kernel": "k_pcg", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
-                         "bytes_per_launch": pcg_bytes, "ms_per_launch": pcg_launch_ms},
-            "substep_roofline": ({"bound": "hbm", "achieved": sub_gbs, "peak": hbm, "unit": "GB/s",
-                                  "frac": sub_gbs / hbm, "peak_kind": peak_kind,
-                                  "bytes_per_substep": sub_bytes / max(prof["substeps"], 1),
-                                  "bytes": "112 P + 92 C + 4 S + 83 N_f iters per substep"}
-                                 if world == 1 else None),
-            "phase_ms": {k: round(v, 3) for k, v in prof.items() if k.endswith("_ms")},
-            "pcg_section_cycles": {k: v for k, v in zip(
-                ["mic_build", "sweeps", "unused", "matvec", "dots", "axpy_norm", "direction", "setup_exit",
-                 "lvl_stage_wait", "lvl_compute", "lvl_barrier", "lvl_count", "sum_sweep_width", "sum_level_range",
-                 "solves"], diag["pcg_section_cycles"]) if k not in ("unused", "lvl_stage_wait")},
-            "pcg_section_cycles_frame": "one untimed frame after the timed ones, in-kernel section timers on",
-            "pcg": {"launches": prof["pcg_launches"], "mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
-                    "mean_fluid_cells": prof["fluid_cells"] / max(prof["pcg_launches"], 1)},
-            "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
-                               "long_sweeps": prof["redist_long_sweeps"]}}
-    if rank == 0 and not args.no_cpu:
-        orc = oracle_for(w, sdf)
-        pos, vel = solver.particles()
-        orc.set_particles(pos, vel)
-        s = solver.stats()
-        orc.set_scalars(s.time, s.emit_accum, s.steps, s.drained, s.rng_state)
-        import oracle
-        threads = os.cpu_count() or 1
-        oracle.set_threads(threads)
-        cps, ct, csub = cpu_sample(orc, budget_s=args.cpu_budget, max_substeps=10 ** 9)
-        line["cpu_baseline"] = {"value": cps / ct, "unit": "particle-substeps/s", "cores": threads, "kind": "port",
-                                "sample": f"{csub} substeps from the GPU state one frame after the timed frames "
-                                          f"({cps} particle-substeps, {ct:.1f} s); C++ restatement of the "
-                                          "reference solver, f64, rayon-parallel parts on all host threads"}
-    if rank == 0 and world == 1:
-        line.update(render_bench(solver, w, sdf, cpu=not args.no_cpu))
-    if rank == 0 and world == 1 and not args.no_batch and args.batch_scenes > 0:
-        solver.close()
-        line.update(batch_bench(args.batch_scenes, args.batch_cfl))
-    if rank == 0 and world == 1 and not args.no_large:
-        solver.close()  # idempotent
-        line.update(large_bench(args.large_substeps, args.large_warmup, cpu=not args.no_cpu))
+    line = pool_line(args, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_extra:
+        from sdr_b200 import workloads
+        cpu = not args.no_cpu
+        rec, s, sdf = frame_record(workloads.plain_parametric(), "parametric_0p8mm", cpu, args.cpu_budget)
+        s.close()
+        line.update(rec)
+        w = workloads.real_cavity(seed=2)
+        rec, s, sdf = frame_record(w, "cavity_0p5mm", cpu, args.cpu_budget)
+        line.update(rec)
+        line.update(render_bench(s, w, sdf, cpu=cpu))
+        s.close()
+        if not args.no_batch and args.batch_scenes > 0:
+            line.update(batch_bench(args.batch_scenes, args.batch_cfl))
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

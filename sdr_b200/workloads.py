@@ -130,10 +130,18 @@ def preseed_pool(solver, target: int, ppc: int = 8):
     at rest, until ``target`` particles or the cavity is full. Returns (pos, vel)
     in f64 for ``Solver.set_particles``."""
     st = solver.stats()
-    nx, ny, nz, dx = int(st.nx), int(st.ny), int(st.nz), float(st.dx)
-    org = np.array([st.origin.x, st.origin.y, st.origin.z])
-    g = np.array(solver.fluid.gravity, dtype=np.float64)
-    cav = np.flatnonzero(solver.cavity_mask().reshape(-1))
+    return preseed_pool_on((int(st.nx), int(st.ny), int(st.nz)), (st.origin.x, st.origin.y, st.origin.z),
+                           float(st.dx), solver.fluid.gravity, solver.cavity_mask(), target, ppc)
+
+
+def preseed_pool_on(dims, origin, dx: float, gravity, cavity_mask: np.ndarray, target: int, ppc: int = 8):
+    """preseed_pool from the grid, gravity and static cavity mask alone (the
+    same particles for any solver holding that grid)."""
+    nx, ny, nz = (int(v) for v in dims)
+    dx = float(dx)
+    org = np.array(origin, dtype=np.float64)
+    g = np.array(gravity, dtype=np.float64)
+    cav = np.flatnonzero(np.asarray(cavity_mask).reshape(-1))
     i = cav % nx
     j = (cav // nx) % ny
     k = cav // (nx * ny)
