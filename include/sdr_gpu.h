@@ -154,6 +154,7 @@ typedef struct {
      * -> host (the per-substep status block) */
     uint64_t h2d_bytes;
     uint64_t d2h_bytes;
+    uint64_t pcg_tile_launches; /* solves that ran on the whole-GPU tiled kernel */
 } sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */
@@ -238,9 +239,14 @@ int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
  * the sweeps spread over all of them (large fluid regions). Both run the same
  * per-cell arithmetic (pressure.rs:341-609) and the same dot orders, so they
  * give the same pressure bits (with the reference dot order, the
- * reference's). SDR_PCG_AUTO (default): the cluster from 200,000 fluid cells
- * in the previous solve. */
-enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2 };
+ * reference's). SDR_PCG_TILES: the whole GPU in one cooperative launch; the
+ * grid's (j, k) lines cut into tiles of 16 x 16, one CTA per tile walking the
+ * levels of its cells, tiles handing boundary values to their neighbours
+ * through progress counters (large fluid regions on a GPU of their own; the
+ * cluster kernel if the device cannot launch it). SDR_PCG_AUTO (default):
+ * from 200,000 fluid cells in the previous solve the tiled solve, or the
+ * cluster with SDR_SOLVER_SHARED_GPU; below that one block. */
+enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2, SDR_PCG_TILES = 3 };
 int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel);
 /* CTAs of the SDR_PCG_ONE_BLOCK solve's cluster (CTA 0 runs the sweeps).
  * 0 (default): 1 with SDR_SOLVER_SHARED_GPU, else 8 (or the largest cluster

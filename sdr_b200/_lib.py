@@ -63,7 +63,7 @@ class SolverOptions(C.Structure):
 
 SOLVER_BLOCKING_SYNC = 1
 SOLVER_SHARED_GPU = 2
-PCG_AUTO, PCG_ONE_BLOCK, PCG_CLUSTER = 0, 1, 2
+PCG_AUTO, PCG_ONE_BLOCK, PCG_CLUSTER, PCG_TILES = 0, 1, 2, 3
 
 
 class SolverStats(C.Structure):
@@ -84,7 +84,7 @@ class Profile(C.Structure):
                 ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16),
                 ("redist_candidates", C.c_uint64), ("redist_sweeps", C.c_uint64),
                 ("redist_long_sweeps", C.c_uint64), ("pcg_cluster_launches", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("pcg_tile_launches", C.c_uint64)]
 
     def to_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}

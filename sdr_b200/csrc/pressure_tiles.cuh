@@ -1,0 +1,687 @@
+// pcg (src/pressure.rs:341-397) over the whole GPU, for large fluid regions.
+//
+// The MIC(0) factor (pressure.rs:442-513) and its two triangular sweeps
+// (pressure.rs:517-570) are recurrences along i+j+k. Here the grid's (j, k)
+// lines are cut into tiles of kTwJ x kTwK lines, one CTA per tile and one
+// thread per line. A tile walks the levels L = i+j+k of its cells in order;
+// within a level every line has at most one cell (i = L - j - k), whose -x
+// predecessor is the thread's own previous cell (a register) and whose -y and
+// -z predecessors are the neighbouring lines' cells of level L-1 (shared
+// memory, double-buffered by level), or, on the tile's low faces, cells of
+// the neighbouring tiles. So a level costs one barrier of the tile's threads,
+// and tiles synchronise only with their two upstream neighbours through
+// per-tile progress counters: a tile runs as soon as its neighbours are one
+// level ahead, and a sweep takes about (levels x the level step) + (tile hops
+// x the hand-off latency) instead of one grid-wide barrier per level. The
+// backward sweep mirrors it (tiles wait on their +y / +z neighbours, levels in
+// decreasing order).
+//
+// Per cell the arithmetic is that of k_pcg / k_pcg_cluster (the same operands
+// in the same order), so the factor and both sweeps give the same bits, and so
+// does the solve: the matvec, the updates and the dots run in the wavefront
+// order and tiling of the other kernels, spread over the grid. The sweeps work
+// in cell order (a line's fluid cells are contiguous there); the residual is
+// copied into cell order by the update phase and z is read back through the
+// cell-order map.
+//
+// Synchronisation: one cooperative launch (every CTA resident). Phases are
+// separated by a grid barrier (an arrival counter and a generation word,
+// release/acquire at GPU scope). In a sweep the 8 compute warps of a CTA share
+// a named barrier per level; a ninth warp publishes the tile's progress
+// (release), polls the neighbours' (acquire), and copies the neighbours'
+// boundary values of completed levels into a shared-memory ring, so compute
+// threads never wait on a global load. Every wait gives up after about a
+// second (2^31 SM cycles) or as soon as another CTA has given up, sets an
+// error bit and lets the kernel wind down.
+#pragma once
+#include "pressure.cuh"
+
+namespace sdr {
+
+constexpr int kTwJ = 16;                     // lines per tile along y
+constexpr int kTwK = 16;                     // lines per tile along z
+constexpr int kTwLines = kTwJ * kTwK;        // compute threads: one per line
+constexpr int kTwBS = kTwLines + 32;         // plus the progress warp
+constexpr int kTwWarps = kTwBS / 32;
+constexpr int kTwRing = 32;                  // levels of neighbour boundary values staged ahead
+constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
+constexpr unsigned long long kTwDone = (1ull << 21) - 1;  // progress count of a finished sweep
+constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
+
+struct TwArgs {
+    PcgArgs a;                   // wavefront-order vectors, tables and dots (as k_pcg)
+    int nx, ny, nz;
+    int tj, tk, ntiles;          // tiles along y and z
+    const uint32_t* coff;        // dense cell -> cell-order index of its fluid cell (exclusive scan, ncell + 1)
+    uint8_t* mask_c;             // cell order: fluid-neighbour bits (NB_*)
+    uint8_t* diag_c;             // cell order: non-solid neighbour count
+    int16_t* ic;                 // cell order: i
+    double* pc_c;                // cell order: MIC(0) factor
+    double* r_c;                 // cell order: residual
+    double* q_c;                 // cell order: forward sweep result
+    double* z_c;                 // cell order: backward sweep result
+    double* exf;                 // forward exchange planes: per tile [kTwK][nx] (+y face) then [kTwJ][nx] (+z face)
+    double* exb;                 // backward exchange planes: the -y and -z faces
+    uint8_t* exm;                // mask planes of the factorisation (+y, +z faces)
+    int* tlo;                    // per tile: first and last level of its fluid cells
+    int* thi;
+    unsigned long long* flags;   // per tile: (epoch << 21) | levels completed in sweep order
+    unsigned long long epoch0;   // first sweep epoch of this solve
+    unsigned* bar;               // grid barrier: [0] arrivals, [1] generation
+    double* gslots;              // 2 x gridDim CTA partials of grid maxima
+    uint32_t* err;               // error bits
+};
+
+// ---------------------------------------------------------------- memory-order helpers
+__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acqrel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_cta_sh(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.cta.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(smem_addr(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cta_sh(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.cta.shared::cta.u64 [%0], %1;" ::"r"(smem_addr(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+__device__ __forceinline__ bool tw_failed(const TwArgs& t) { return *(volatile uint32_t*)t.err != 0u; }
+// Barrier of the compute warps (named barrier 1).
+__device__ __forceinline__ void tw_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kTwLines) : "memory"); }
+
+struct TwShared {
+    double v[2][kTwLines];            // this tile's values of the last two levels, by line
+    uint8_t m[2][kTwLines];           // the factorisation's neighbour masks, by line
+    double ring[2][kTwRing][16];      // upstream neighbours' boundary values by level ([0] y face, [1] z face)
+    uint8_t ringm[2][kTwRing][16];    // their masks (factorisation)
+    unsigned long long mine;          // levels this tile has completed (sweep order), for the progress warp
+    unsigned long long avail[2];      // levels whose y / z neighbour values are in the ring
+    unsigned long long done;          // the tile's sweep is over
+    int ok;
+    double red[kTwWarps];
+};
+
+// Grid barrier; false if the wait gave up or another CTA has (the error bit is set).
+__device__ bool tw_grid_sync(const TwArgs& t, TwShared& sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned gen = ld_acquire_gpu_u32(t.bar + 1);
+        const unsigned arrived = atom_add_acqrel_gpu(t.bar, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            t.bar[0] = 0u;  // ordered before the release of the next generation
+            st_release_gpu_u32(t.bar + 1, gen + 1u);
+        } else {
+            const long long t0 = clock64();
+            while (ld_acquire_gpu_u32(t.bar + 1) == gen) {
+                if (tw_failed(t)) {
+                    ok = 0;
+                    break;
+                }
+                if (clock64() - t0 > kTwWaitCycles) {
+                    atomicOr(t.err, kTwErrWait);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        if (ok && tw_failed(t)) ok = 0;  // another CTA gave up: wind down
+        sh.ok = ok;
+    }
+    __syncthreads();
+    return sh.ok != 0;
+}
+
+__device__ __forceinline__ double tw_block_max(double v, TwShared& sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sh.red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = sh.red[0];
+    for (int w = 1; w < kTwWarps; ++w) m = fmax(m, sh.red[w]);
+    __syncthreads();
+    return m;
+}
+
+// Maximum over the grid (order-free): CTA maxima through a double-buffered slot array.
+__device__ bool tw_grid_max(const TwArgs& t, TwShared& sh, double v, int& parity, double& out) {
+    const double bm = tw_block_max(v, sh);
+    double* sl = t.gslots + (size_t)parity * gridDim.x;
+    parity ^= 1;
+    if (threadIdx.x == 0) sl[blockIdx.x] = bm;
+    if (!tw_grid_sync(t, sh)) return false;
+    if (threadIdx.x < 32) {
+        double m = 0.0;
+        for (unsigned q = threadIdx.x; q < gridDim.x; q += 32) m = fmax(m, __ldcg(sl + q));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) sh.red[0] = m;
+    }
+    __syncthreads();
+    out = sh.red[0];
+    __syncthreads();
+    return true;
+}
+
+// Total of the tree-order tile sums (the lane pattern and xor tree of
+// pcg_tile_total), formed by warp 0 and handed to the CTA.
+__device__ double tw_tile_total(const TwArgs& t, uint32_t ntile, TwShared& sh) {
+    if (threadIdx.x < 32) {
+        const double s = pcg_tile_total(t.a, ntile);
+        if (threadIdx.x == 0) sh.red[0] = s;
+    }
+    __syncthreads();
+    const double r = sh.red[0];
+    __syncthreads();
+    return r;
+}
+
+// The reference's chunked dot (pressure.rs:588-603) over `prod` in cell
+// order: one warp per 4096-cell chunk across the grid, then the chunk sums in
+// chunk order (as pcg_exact_dot).
+__device__ bool tw_exact_dot(const TwArgs& t, TwShared& sh, double& out) {
+    const PcgArgs& a = t.a;
+    if (!tw_grid_sync(t, sh)) return false;  // products complete
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * kTwWarps + (threadIdx.x >> 5), nw = gridDim.x * kTwWarps;
+    for (int ch = gw; ch < a.nchunks; ch += nw) {
+        int q = a.chunk_start[ch];
+        const int e = a.chunk_start[ch + 1];
+        double acc = 0.0;
+        for (; q < e; q += 512) {
+            double v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int idx = q + u * 32 + lane;
+                v[u] = idx < e ? __ldcg(a.prod + idx) : 0.0;
+            }
+            const int cnt = min(512, e - q);
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+#pragma unroll 8
+                for (int src = 0; src < 32; ++src) {
+                    const double x = __shfl_sync(0xffffffffu, v[u], src);
+                    if (u * 32 + src < cnt) acc = dadd(acc, x);
+                }
+            }
+        }
+        if (lane == 0) a.partials[ch] = acc;
+    }
+    if (!tw_grid_sync(t, sh)) return false;
+    if (threadIdx.x == 0) {
+        double s = -0.0;
+        for (int ch = 0; ch < a.nchunks; ++ch) s = dadd(s, __ldcg(a.partials + ch));
+        sh.red[0] = s;
+    }
+    __syncthreads();
+    out = sh.red[0];
+    __syncthreads();
+    return true;
+}
+
+// ---------------------------------------------------------------- the tile sweeps
+enum { TW_BUILD = 0, TW_FORWARD = 1, TW_BACKWARD = 2 };
+
+// The progress warp of one tile's sweep. Lane 0 publishes the tile's
+// progress to global memory (release); lanes 1 and 2 poll the two upstream
+// neighbours' progress (acquire); then lanes 0-15 copy the y neighbour's
+// boundary values of every newly completed level into the shared ring and
+// lanes 16-31 the z neighbour's, as far as the ring has room, and publish how
+// many levels are staged.
+template <int MODE>
+__device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nby, int nbz, unsigned long long epoch,
+                                 int s_first, int s_last, int nlevels) {
+    constexpr bool fwd = MODE != TW_BACKWARD;
+    const int lane = threadIdx.x & 31;
+    const int J = tile % t.tj, K = tile / t.tj;
+    const int j0 = J * kTwJ, k0 = K * kTwK, nx = t.nx;
+    const size_t plane = (size_t)(kTwJ + kTwK) * nx;
+    const double* ex = fwd ? t.exf : t.exb;
+    // this lane's boundary line: lanes 0-15 the y face (line (jb, k0 + lane)),
+    // lanes 16-31 the z face (line (j0 + lane - 16, kb))
+    const int face = lane >> 4, l = lane & 15;
+    const int nb = face == 0 ? nby : nbz;
+    const int jl = face == 0 ? (fwd ? j0 : j0 + kTwJ - 1) : j0 + l;
+    const int kl = face == 0 ? k0 + l : (fwd ? k0 : k0 + kTwK - 1);
+    const bool line_ok = nb >= 0 && jl < t.ny && kl < t.nz;
+    const size_t row = (size_t)(face == 0 ? 0 : kTwK * nx) + (size_t)l * nx;
+    const double* src = nb >= 0 ? ex + (size_t)nb * plane + row : nullptr;
+    const uint8_t* srcm = nb >= 0 ? t.exm + (size_t)nb * plane + row : nullptr;
+    const unsigned long long base = epoch << 21;
+    unsigned long long published = ~0ull;
+    int copied = s_first;  // next level (sweep order) to stage, for this lane's face
+    const long long t0 = clock64();
+    for (;;) {
+        const unsigned long long done = ld_acquire_cta_sh(&sh.done);
+        const unsigned long long mine = ld_acquire_cta_sh(&sh.mine);
+        if (lane == 0 && mine != published) {
+            st_release_gpu(t.flags + tile, base | mine);
+            published = mine;
+        }
+        if (done) break;
+        // neighbours' progress: levels before `prog` are complete
+        unsigned long long pv = 0ull;
+        if (lane == 1 && nby >= 0) pv = ld_acquire_gpu(t.flags + nby);
+        if (lane == 2 && nbz >= 0) pv = ld_acquire_gpu(t.flags + nbz);
+        const unsigned long long py = __shfl_sync(0xffffffffu, pv, 1), pz = __shfl_sync(0xffffffffu, pv, 2);
+        const unsigned long long p = face == 0 ? py : pz;
+        const long long prog = nb < 0 ? (long long)s_last + 1 : (p < base ? 0ll : (long long)(p - base));
+        // stage the levels s with s <= prog (the neighbour's level s - 1 is complete), ring room permitting
+        const int lim = (int)min(min((long long)s_last, prog), (long long)mine + kTwRing - 1);
+        if (line_ok) {
+            // eight levels at a time: their loads are independent (consecutive i of one line)
+            for (int sq0 = copied; sq0 <= lim; sq0 += 8) {
+                double v[8];
+                uint8_t vm[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int sq = sq0 + u;
+                    const int L = fwd ? sq : nlevels - 1 - sq;
+                    const int i = L - jl - kl;
+                    const bool in = sq <= lim && i >= 0 && i < nx;
+                    v[u] = in ? __ldcg(src + i) : 0.0;
+                    vm[u] = (MODE == TW_BUILD && in) ? __ldcg(srcm + i) : (uint8_t)0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int sq = sq0 + u;
+                    if (sq <= lim) {
+                        sh.ring[face][sq % kTwRing][l] = v[u];
+                        if (MODE == TW_BUILD) sh.ringm[face][sq % kTwRing][l] = vm[u];
+                    }
+                }
+            }
+        }
+        // every lane of a face has staged up to its `lim`: publish it (lanes 0 and 16)
+        const int lim_y = __shfl_sync(0xffffffffu, lim, 0), lim_z = __shfl_sync(0xffffffffu, lim, 16);
+        __syncwarp();
+        if (lane == 0 && lim_y + 1 > copied) st_release_cta_sh(&sh.avail[0], (unsigned long long)(lim_y + 1));
+        if (lane == 16 && lim_z + 1 > copied) st_release_cta_sh(&sh.avail[1], (unsigned long long)(lim_z + 1));
+        copied = max(copied, lim + 1);
+        const bool give_up = __shfl_sync(0xffffffffu, (int)(tw_failed(t) || clock64() - t0 > kTwWaitCycles), 0);
+        if (give_up) {
+            if (lane == 0) {
+                atomicOr(t.err, kTwErrWait);
+                st_release_gpu(t.flags + tile, base | kTwDone);  // release whoever waits on this tile
+                st_release_cta_sh(&sh.avail[0], ~0ull >> 1);      // and this tile's compute warps
+                st_release_cta_sh(&sh.avail[1], ~0ull >> 1);
+            }
+            break;
+        }
+    }
+}
+
+// Compute-thread wait until the ring holds neighbour values for level s.
+__device__ __forceinline__ void tw_wait(const TwArgs& t, TwShared& sh, int which, unsigned long long s) {
+    if (ld_acquire_cta_sh(&sh.avail[which]) > s) return;
+    const long long t0 = clock64();
+    for (unsigned spin = 0; ld_acquire_cta_sh(&sh.avail[which]) <= s; ++spin) {
+        if ((spin & 255u) == 255u && (tw_failed(t) || clock64() - t0 > kTwWaitCycles)) {
+            atomicOr(t.err, kTwErrWait);
+            return;
+        }
+    }
+}
+
+// Operands of one cell in sweep order: its level, neighbour mask and the
+// values the sweep reads (diag for the factor; r and the factor forward; q
+// and the factor backward).
+template <int MODE>
+__device__ __forceinline__ void tw_load(const TwArgs& t, int c, int jk, int& L, uint8_t& m, double& ra, double& rb) {
+    L = (int)t.ic[c] + jk;
+    m = t.mask_c[c];
+    if (MODE == TW_BUILD) {
+        ra = (double)t.diag_c[c];
+        rb = 0.0;
+    } else if (MODE == TW_FORWARD) {
+        ra = __ldcg(t.r_c + c);  // written by other CTAs in the update phase
+        rb = t.pc_c[c];
+    } else {
+        ra = t.q_c[c];
+        rb = t.pc_c[c];
+    }
+}
+
+// One tile's sweep. BUILD: the MIC(0) factor into pc_c (forward order).
+// FORWARD: q = L^-1 r_c. BACKWARD: z = L^-T q, plus the z*r products in cell
+// order for the reference dot order.
+template <int MODE>
+__device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long long epoch, int nlevels) {
+    const PcgArgs& a = t.a;
+    const int tid = threadIdx.x;
+    const int J = tile % t.tj, K = tile / t.tj;
+    constexpr bool fwd = MODE != TW_BACKWARD;
+    // upstream neighbours of this sweep
+    const int nby = fwd ? (J > 0 ? tile - 1 : -1) : (J + 1 < t.tj ? tile + 1 : -1);
+    const int nbz = fwd ? (K > 0 ? tile - t.tj : -1) : (K + 1 < t.tk ? tile + t.tj : -1);
+    const int lo = __ldcg(t.tlo + tile), hi = __ldcg(t.thi + tile);
+    const int s_first = hi < lo ? nlevels : (fwd ? lo : nlevels - 1 - hi);
+    const int s_last = hi < lo ? nlevels - 1 : (fwd ? hi : nlevels - 1 - lo);
+    if (tid == 0) {
+        sh.mine = (unsigned long long)s_first;
+        sh.avail[0] = sh.avail[1] = (unsigned long long)s_first;
+        sh.done = 0ull;
+    }
+    __syncthreads();
+    if (tid >= kTwLines) {
+        tw_progress_warp<MODE>(t, sh, tile, nby, nbz, epoch, s_first, s_last, nlevels);
+        __syncthreads();
+        return;
+    }
+    const int lj = tid % kTwJ, lk = tid / kTwJ;
+    const int j = J * kTwJ + lj, k = K * kTwK + lk;
+    const int nx = t.nx;
+    uint32_t beg = 0, end = 0;
+    if (j < t.ny && k < t.nz) {
+        const size_t d = ((size_t)k * t.ny + j) * (size_t)nx;
+        beg = __ldcg(t.coff + d);
+        end = __ldcg(t.coff + d + nx);
+    }
+    const int jk = j + k;
+    const size_t plane = (size_t)(kTwJ + kTwK) * nx;
+    double* ex_own = (fwd ? t.exf : t.exb) + (size_t)tile * plane;
+    uint8_t* exm_own = t.exm + (size_t)tile * plane;
+    // this line's next two cells in sweep order: the operands of the cell
+    // after next load while the next levels run
+    const int step = fwd ? 1 : -1;
+    int cur = fwd ? (int)beg : (int)end - 1;
+    const int stop = fwd ? (int)end : (int)beg - 1;
+    int L0 = -1, L1 = -1;
+    uint8_t m0 = 0, m1 = 0;
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+    if (cur != stop) tw_load<MODE>(t, cur, jk, L0, m0, a0, b0);
+    if (cur != stop && cur + step != stop) tw_load<MODE>(t, cur + step, jk, L1, m1, a1, b1);
+    double carry = 0.0;   // the value of this line's previous cell (the -x / +x predecessor)
+    uint8_t carry_m = 0;  // its neighbour mask (factorisation)
+    const double TAU = 0.97, SIGMA = 0.25;
+    const bool yb = fwd ? lj == 0 : lj == kTwJ - 1;  // this line reads the y neighbour tile
+    const bool zb = fwd ? lk == 0 : lk == kTwK - 1;
+    for (int s = s_first; s <= s_last; ++s) {
+        const int L = fwd ? s : nlevels - 1 - s;
+        if (tid == 0 && nby >= 0) tw_wait(t, sh, 0, (unsigned long long)s);
+        if (tid == 32 && nbz >= 0) tw_wait(t, sh, 1, (unsigned long long)s);
+        tw_bar();
+        if (tid == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);  // levels before s are complete
+        const int wp = (s - 1) & 1, wc = s & 1, rs = s % kTwRing;
+        if (L != L0) continue;
+        const int i = L - jk;
+        const uint8_t m = m0;
+        if (MODE == TW_BUILD) {
+            double axi = 0, pxi = 0, axi_y = 0, axi_z = 0;
+            double ayj = 0, pyj = 0, ayj_x = 0, ayj_z = 0;
+            double azk = 0, pzk = 0, azk_x = 0, azk_y = 0;
+            if (m >> NB_MX & 1) {
+                axi = -1.0;
+                pxi = carry;
+                axi_y = (carry_m >> NB_PY & 1) ? -1.0 : 0.0;
+                axi_z = (carry_m >> NB_PZ & 1) ? -1.0 : 0.0;
+            }
+            if (m >> NB_MY & 1) {
+                const uint8_t mk = yb ? sh.ringm[0][rs][lk] : sh.m[wp][tid - 1];
+                pyj = yb ? sh.ring[0][rs][lk] : sh.v[wp][tid - 1];
+                ayj = -1.0;
+                ayj_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
+                ayj_z = (mk >> NB_PZ & 1) ? -1.0 : 0.0;
+            }
+            if (m >> NB_MZ & 1) {
+                const uint8_t mk = zb ? sh.ringm[1][rs][lj] : sh.m[wp][tid - kTwJ];
+                pzk = zb ? sh.ring[1][rs][lj] : sh.v[wp][tid - kTwJ];
+                azk = -1.0;
+                azk_x = (mk >> NB_PX & 1) ? -1.0 : 0.0;
+                azk_y = (mk >> NB_PY & 1) ? -1.0 : 0.0;
+            }
+            const double tx = dmul(axi, pxi), ty = dmul(ayj, pyj), tz = dmul(azk, pzk);
+            const double diag = a0;
+            const double mx = dmul(dmul(dmul(axi, dadd(axi_y, axi_z)), pxi), pxi);
+            const double my = dmul(dmul(dmul(ayj, dadd(ayj_x, ayj_z)), pyj), pyj);
+            const double mz = dmul(dmul(dmul(azk, dadd(azk_x, azk_y)), pzk), pzk);
+            double e = dsub(dsub(dsub(dsub(diag, dmul(tx, tx)), dmul(ty, ty)), dmul(tz, tz)),
+                            dmul(TAU, dadd(dadd(mx, my), mz)));
+            if (e < dmul(SIGMA, diag)) e = diag;
+            const double pc = e > 0.0 ? ddiv(1.0, __dsqrt_rn(e)) : 0.0;
+            t.pc_c[cur] = pc;
+            sh.v[wc][tid] = pc;
+            sh.m[wc][tid] = m;
+            carry = pc;
+            carry_m = m;
+            if (lj == kTwJ - 1) {
+                ex_own[(size_t)lk * nx + i] = pc;
+                exm_own[(size_t)lk * nx + i] = m;
+            }
+            if (lk == kTwK - 1) {
+                ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = pc;
+                exm_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = m;
+            }
+        } else if (MODE == TW_FORWARD) {
+            // t = r + pq[-x] + pq[-y] + pq[-z]; q = t * pc (pcg_apply_mic0, forward)
+            double tt = a0;
+            if (m >> NB_MX & 1) tt = dadd(tt, carry);
+            if (m >> NB_MY & 1) tt = dadd(tt, yb ? sh.ring[0][rs][lk] : sh.v[wp][tid - 1]);
+            if (m >> NB_MZ & 1) tt = dadd(tt, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid - kTwJ]);
+            const double qv = dmul(tt, b0);
+            const double pqv = dmul(b0, qv);
+            t.q_c[cur] = qv;
+            sh.v[wc][tid] = pqv;
+            carry = pqv;
+            if (lj == kTwJ - 1) ex_own[(size_t)lk * nx + i] = pqv;
+            if (lk == kTwK - 1) ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = pqv;
+        } else {
+            // t = q + pc z[+x] + pc z[+y] + pc z[+z]; z = t * pc (pcg_apply_mic0, backward)
+            const double pc = b0;
+            double tt = a0;
+            if (m >> NB_PX & 1) tt = dadd(tt, dmul(pc, carry));
+            if (m >> NB_PY & 1) tt = dadd(tt, dmul(pc, yb ? sh.ring[0][rs][lk] : sh.v[wp][tid + 1]));
+            if (m >> NB_PZ & 1) tt = dadd(tt, dmul(pc, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid + kTwJ]));
+            const double zv = dmul(tt, pc);
+            t.z_c[cur] = zv;
+            if (a.exact_dots) a.prod[cur] = dmul(zv, __ldcg(t.r_c + cur));
+            sh.v[wc][tid] = zv;
+            carry = zv;
+            if (lj == 0) ex_own[(size_t)lk * nx + i] = zv;
+            if (lk == 0) ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = zv;
+        }
+        // shift the cursor; the cell after next starts loading now
+        cur += step;
+        L0 = L1;
+        m0 = m1;
+        a0 = a1;
+        b0 = b1;
+        L1 = -1;
+        const int nxt = cur + step;
+        if (cur != stop && nxt != stop) {
+            tw_load<MODE>(t, nxt, jk, L1, m1, a1, b1);
+            const int ahead = nxt + 8 * step;
+            if (MODE != TW_BUILD && (fwd ? ahead < (int)end : ahead >= (int)beg)) {
+                prefetch_l1(t.pc_c + ahead);
+                if (MODE == TW_BACKWARD) prefetch_l1(t.q_c + ahead);
+            }
+        }
+    }
+    tw_bar();
+    if (tid == 0) {
+        st_release_cta_sh(&sh.mine, kTwDone);
+        st_release_cta_sh(&sh.done, 1ull);
+    }
+    __syncthreads();  // the progress warp has published the final count and left
+}
+
+// Every tile of this CTA: tiles blockIdx.x, blockIdx.x + gridDim.x, ... in
+// increasing order forward (each tile after its -y and -z neighbours) and in
+// decreasing order backward, so waits always point to tiles earlier in some
+// CTA's order and the earliest unfinished tile can always run.
+template <int MODE>
+__device__ bool tw_sweep_all(const TwArgs& t, TwShared& sh, unsigned long long epoch, int nlevels) {
+    const int G = (int)gridDim.x, b = (int)blockIdx.x;
+    if (MODE == TW_BACKWARD) {
+        if (b < t.ntiles)
+            for (int tile = b + ((t.ntiles - 1 - b) / G) * G; tile >= 0; tile -= G) tw_sweep<MODE>(t, sh, tile, epoch, nlevels);
+    } else {
+        for (int tile = b; tile < t.ntiles; tile += G) tw_sweep<MODE>(t, sh, tile, epoch, nlevels);
+    }
+    return !tw_failed(t);
+}
+
+// ---------------------------------------------------------------- the solve
+// Launched cooperatively (every CTA resident at once).
+__global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
+    __shared__ TwShared sh;
+    const PcgArgs& a = t.a;
+    const uint32_t nf = *a.nf;
+    const uint32_t ntile = (nf + kTile - 1) / kTile;
+    const uint32_t G = gridDim.x * kTwBS, gt = blockIdx.x * kTwBS + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * kTwWarps + (threadIdx.x >> 5), nw = gridDim.x * kTwWarps;
+    const int nlevels = a.nlevels;
+    int parity = 0;
+    unsigned long long epoch = t.epoch0;
+    double residual = 0.0, sigma = 0.0;
+    int iters = 0;
+    double mx = 0.0;
+    for (uint32_t i = gt; i < nf; i += G) mx = fmax(mx, fabs(a.b[i]));
+    for (uint32_t q = gt; q < (uint32_t)t.ntiles; q += G) {
+        t.tlo[q] = INT32_MAX;
+        t.thi[q] = -1;
+    }
+    if (!tw_grid_max(t, sh, mx, parity, residual)) goto out;
+    if (residual > a.tol) {
+        // cell-order tables, r and p, and the tiles' level ranges
+        for (uint32_t i = gt; i < nf; i += G) {
+            const int c = a.cinv[i];
+            const uint32_t cell = a.lv_cell[i];
+            const int ii = (int)(cell % (uint32_t)t.nx), jj = (int)((cell / (uint32_t)t.nx) % (uint32_t)t.ny),
+                      kk = (int)(cell / ((uint32_t)t.nx * (uint32_t)t.ny));
+            t.mask_c[c] = a.nmask[i];
+            t.diag_c[c] = a.diag[i];
+            t.ic[c] = (int16_t)ii;
+            const double bv = a.b[i];
+            t.r_c[c] = bv;
+            a.r[i] = bv;
+            a.p[i] = 0.0;
+            const int tile = jj / kTwJ + (kk / kTwK) * t.tj;
+            atomicMin(t.tlo + tile, ii + jj + kk);
+            atomicMax(t.thi + tile, ii + jj + kk);
+        }
+        if (!tw_grid_sync(t, sh)) goto out;
+        if (!tw_sweep_all<TW_BUILD>(t, sh, epoch++, nlevels)) goto out;
+        if (!tw_grid_sync(t, sh)) goto out;  // the factor's exchange planes are reused by the sweeps
+        if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
+        if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
+        // dot(z, r)
+        if (a.exact_dots) {
+            if (!tw_exact_dot(t, sh, sigma)) goto out;
+        } else {
+            if (!tw_grid_sync(t, sh)) goto out;
+            for (uint32_t tl = (uint32_t)gw; tl < ntile; tl += (uint32_t)nw) {
+                double acc = 0.0;
+                const uint32_t e = min((tl + 1) * kTile, nf);
+                for (uint32_t i = tl * kTile + lane; i < e; i += 32)
+                    acc = dadd(acc, dmul(__ldcg(t.z_c + a.cinv[i]), __ldcg(a.r + i)));
+                acc = warp_tree_sum(acc);
+                if (lane == 0) a.tpart[tl] = acc;
+            }
+            if (!tw_grid_sync(t, sh)) goto out;
+            sigma = tw_tile_total(t, ntile, sh);
+        }
+        for (uint32_t i = gt; i < nf; i += G) a.s[i] = __ldcg(t.z_c + a.cinv[i]);
+        if (!tw_grid_sync(t, sh)) goto out;
+        for (int it = 0; it < a.max_iters; ++it) {
+            iters = it + 1;
+            // apply_a (pressure.rs:400-439) and s*As, by the tiles of the tree dot
+            for (uint32_t tl = (uint32_t)gw; tl < ntile; tl += (uint32_t)nw) {
+                double acc = 0.0;
+                for (int u = 0; u < kTile / 32; ++u) {
+                    const uint32_t i = tl * kTile + lane + 32u * u;
+                    if (i >= nf) break;
+                    const int2* nb2 = reinterpret_cast<const int2*>(a.nbr + (size_t)i * 6);
+                    const int2 x0 = nb2[0], x1 = nb2[1], x2 = nb2[2];
+                    const int nbv[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
+                    const double sv = __ldcg(a.s + i);
+                    double nsv[6];
+#pragma unroll
+                    for (int d = 0; d < 6; ++d) nsv[d] = nbv[d] >= 0 ? __ldcg(a.s + nbv[d]) : 0.0;
+                    double v = dmul((double)a.diag[i], sv);
+                    if (nbv[NB_PX] >= 0) v = dsub(v, nsv[NB_PX]);
+                    if (nbv[NB_MX] >= 0) v = dsub(v, nsv[NB_MX]);
+                    if (nbv[NB_PY] >= 0) v = dsub(v, nsv[NB_PY]);
+                    if (nbv[NB_MY] >= 0) v = dsub(v, nsv[NB_MY]);
+                    if (nbv[NB_PZ] >= 0) v = dsub(v, nsv[NB_PZ]);
+                    if (nbv[NB_MZ] >= 0) v = dsub(v, nsv[NB_MZ]);
+                    a.as[i] = v;
+                    if (a.exact_dots) a.prod[a.cinv[i]] = dmul(sv, v);
+                    else acc = dadd(acc, dmul(sv, v));
+                }
+                if (!a.exact_dots) {
+                    acc = warp_tree_sum(acc);
+                    if (lane == 0) a.tpart[tl] = acc;
+                }
+            }
+            double denom;  // dot(s, As)
+            if (a.exact_dots) {
+                if (!tw_exact_dot(t, sh, denom)) goto out;
+            } else {
+                if (!tw_grid_sync(t, sh)) goto out;
+                denom = tw_tile_total(t, ntile, sh);
+            }
+            if (fabs(denom) < 1e-30) break;
+            const double alpha = ddiv(sigma, denom);
+            double mr = 0.0;
+            for (uint32_t i = gt; i < nf; i += G) {
+                a.p[i] = dadd(a.p[i], dmul(alpha, __ldcg(a.s + i)));
+                const double rv = dsub(a.r[i], dmul(alpha, __ldcg(a.as + i)));
+                a.r[i] = rv;
+                t.r_c[a.cinv[i]] = rv;
+                mr = fmax(mr, fabs(rv));
+            }
+            if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and r_c
+            if (residual <= a.tol) break;
+            if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
+            if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
+            double sigma_new;  // dot(z, r)
+            if (a.exact_dots) {
+                if (!tw_exact_dot(t, sh, sigma_new)) goto out;
+            } else {
+                if (!tw_grid_sync(t, sh)) goto out;
+                for (uint32_t tl = (uint32_t)gw; tl < ntile; tl += (uint32_t)nw) {
+                    double acc = 0.0;
+                    const uint32_t e = min((tl + 1) * kTile, nf);
+                    for (uint32_t i = tl * kTile + lane; i < e; i += 32)
+                        acc = dadd(acc, dmul(__ldcg(t.z_c + a.cinv[i]), __ldcg(a.r + i)));
+                    acc = warp_tree_sum(acc);
+                    if (lane == 0) a.tpart[tl] = acc;
+                }
+                if (!tw_grid_sync(t, sh)) goto out;
+                sigma_new = tw_tile_total(t, ntile, sh);
+            }
+            const double beta = ddiv(sigma_new, sigma);
+            for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(t.z_c + a.cinv[i]), dmul(beta, a.s[i]));
+            if (!tw_grid_sync(t, sh)) goto out;  // s complete before the next matvec reads neighbours
+            sigma = sigma_new;
+        }
+        for (uint32_t i = gt; i < nf; i += G) a.p_dense[a.lv_cell[i]] = a.p[i];
+    }
+out:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *a.out_iters = iters;
+        *a.out_residual = residual;
+    }
+}
+
+}  // namespace sdr

@@ -30,6 +30,7 @@
 #include "particles.cuh"
 #include "pressure.cuh"
 #include "pressure_cluster.cuh"
+#include "pressure_tiles.cuh"
 #include "render.cuh"
 #include "scan.cuh"
 #include "sdf.cuh"
@@ -388,6 +389,16 @@ struct sdr_solver {
     uint32_t last_p2g_queue = 0;    // its length at the last status read
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
     double* cl_slots = nullptr;     // CTA partials of the cluster kernels
+    // whole-GPU tiled solve (k_pcg_tiles), allocated on first use
+    uint8_t *tw_mask = nullptr, *tw_diag = nullptr, *tw_exm = nullptr;
+    int16_t* tw_ic = nullptr;
+    double *tw_pc = nullptr, *tw_r = nullptr, *tw_q = nullptr, *tw_z = nullptr, *tw_exf = nullptr, *tw_exb = nullptr,
+           *tw_slots = nullptr;
+    int *tw_lo = nullptr, *tw_hi = nullptr;
+    unsigned long long* tw_flags = nullptr;
+    unsigned* tw_bar = nullptr;
+    int tw_tj = 0, tw_tk = 0, tw_grid = 0;  // tiles along y and z; CTAs of the cooperative launch (0: not set up)
+    unsigned long long tw_epoch = 1;        // next sweep epoch
     unsigned long long* rclaim = nullptr;  // per cell: claim stamps of the parallel redistribution replay
     sdr_profile prof{};
     uint64_t particle_substeps = 0, substeps_total = 0;
@@ -511,8 +522,9 @@ struct sdr_solver {
         dalloc(frec, nc, st);
         dalloc(brec, nc, st);
         dalloc(chunk_start, nchunks + 1, st);
-        dalloc(cflag, nc, st);
-        dalloc(coff, nc, st);
+        dalloc(cflag, nc + 1, st);
+        dalloc(coff, nc + 1, st);
+        CK(cudaMemsetAsync(cflag + nc, 0, 4, st));  // coff[nc] = the fluid count (line ends of the tiled solve)
         dalloc(p_dense, nc, st);
         CK(cudaMemsetAsync(p_dense, 0, nc * 8, st));
         dalloc(mcell, blocks(nc, kMetBS), st);
@@ -531,6 +543,9 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
+        dfree(tw_mask, st); dfree(tw_diag, st); dfree(tw_exm, st); dfree(tw_ic, st); dfree(tw_pc, st); dfree(tw_r, st);
+        dfree(tw_q, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
+        dfree(tw_hi, st); dfree(tw_flags, st); dfree(tw_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
@@ -687,7 +702,7 @@ struct sdr_solver {
         t.vs_cap = 0.25 * t.vs_unit;
         LAUNCH(k_tables, blocks(ncell, 256), 256, 0, st, t);
         LAUNCH(k_fluid_flags, blocks(ncell, 256), 256, 0, st, cells, ncell, cflag);
-        scan(cflag, coff, ncell, nullptr);
+        scan(cflag, coff, ncell + 1, nullptr);
         LAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, cinv, chunk_start,
                nchunks, &dst->nf);
         CK(cudaMemsetAsync(p_dense, 0, ncell * 8, st));
@@ -724,7 +739,13 @@ struct sdr_solver {
         a.out_residual = &dst->residual;
         a.timing = kernel_timers ? dst->pcg_cycles : nullptr;
         a.exact_dots = exact_dots ? 1 : 0;
-        const bool cluster = pcg_kernel == SDR_PCG_CLUSTER ||
+        const bool large = pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells && !shared_gpu;
+        if ((pcg_kernel == SDR_PCG_TILES || large) && tiles_ready()) {
+            launch_tiles(a);
+            if (profiling) prof.pcg_tile_launches += 1;
+            return;
+        }
+        const bool cluster = pcg_kernel == SDR_PCG_CLUSTER || pcg_kernel == SDR_PCG_TILES || large ||
                              (pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells);
         if (cluster) {
             // One cluster of up to 16 CTAs (one per SM); the levels of each
@@ -753,6 +774,61 @@ struct sdr_solver {
                 launch_one_cluster_smem(k_pcg, ctas, kPcgBS, kPcgSmem, st, a);
             }
         }
+    }
+
+    // The whole-GPU tiled solve needs a cooperative launch with every CTA
+    // resident; its buffers are allocated on first use. False if the device
+    // cannot run it (then the cluster kernel solves).
+    bool tiles_ready() {
+        if (tw_grid < 0) return false;
+        if (tw_grid > 0) return true;
+        int coop = 0, nsm = 0, occ = 0;
+        CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_tiles, kTwBS, 0) != cudaSuccess) {
+            cudaGetLastError();
+            occ = 0;
+        }
+        if (!coop || occ < 1 || g.nx > INT16_MAX) {  // the sweeps keep i in 16 bits
+            tw_grid = -1;
+            return false;
+        }
+        tw_grid = nsm * std::min(occ, 2);
+        tw_tj = (g.ny + kTwJ - 1) / kTwJ;
+        tw_tk = (g.nz + kTwK - 1) / kTwK;
+        const size_t nt = (size_t)tw_tj * tw_tk, plane = (size_t)(kTwJ + kTwK) * g.nx;
+        dalloc(tw_mask, ncell, st); dalloc(tw_diag, ncell, st); dalloc(tw_ic, ncell, st);
+        dalloc(tw_pc, ncell, st); dalloc(tw_r, ncell, st); dalloc(tw_q, ncell, st); dalloc(tw_z, ncell, st);
+        dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st); dalloc(tw_exm, nt * plane, st);
+        dalloc(tw_lo, nt, st); dalloc(tw_hi, nt, st);
+        dalloc(tw_flags, nt, st);
+        CK(cudaMemsetAsync(tw_flags, 0, nt * sizeof(unsigned long long), st));
+        dalloc(tw_bar, 2, st);
+        dalloc(tw_slots, 2 * (size_t)tw_grid, st);
+        return true;
+    }
+
+    void launch_tiles(const PcgArgs& a) {
+        TwArgs t{};
+        t.a = a;
+        t.a.timing = nullptr;
+        t.nx = g.nx; t.ny = g.ny; t.nz = g.nz;
+        t.tj = tw_tj; t.tk = tw_tk; t.ntiles = tw_tj * tw_tk;
+        t.coff = coff;
+        t.mask_c = tw_mask; t.diag_c = tw_diag; t.ic = tw_ic;
+        t.pc_c = tw_pc; t.r_c = tw_r; t.q_c = tw_q; t.z_c = tw_z;
+        t.exf = tw_exf; t.exb = tw_exb; t.exm = tw_exm;
+        t.tlo = tw_lo; t.thi = tw_hi;
+        t.flags = tw_flags;
+        t.epoch0 = tw_epoch;
+        tw_epoch += 2 * (unsigned long long)std::min<uint64_t>(max_iters, (uint64_t)INT32_MAX) + 8;
+        t.bar = tw_bar;
+        t.gslots = tw_slots;
+        t.err = &dst->err;
+        CK(cudaMemsetAsync(tw_bar, 0, 2 * sizeof(unsigned), st));  // a wound-down launch may leave arrivals
+        void* args[] = {&t};
+        CK(cudaLaunchCooperativeKernel((const void*)k_pcg_tiles, dim3((unsigned)tw_grid), dim3(kTwBS), args, 0, st));
+        g_launches.fetch_add(1, std::memory_order_relaxed);
     }
 
     void project_gradient(double dt) {
@@ -1373,7 +1449,7 @@ int sdr_solver_set_pcg_ctas(sdr_solver* s, int ctas) {
 int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel) {
     return guard([&] {
         require(s, "null solver");
-        if (kernel != SDR_PCG_AUTO && kernel != SDR_PCG_ONE_BLOCK && kernel != SDR_PCG_CLUSTER)
+        if (kernel != SDR_PCG_AUTO && kernel != SDR_PCG_ONE_BLOCK && kernel != SDR_PCG_CLUSTER && kernel != SDR_PCG_TILES)
             throw Fail{SDR_ERR_INVALID, "unknown pressure-solve kernel " + std::to_string(kernel)};
         s->pcg_kernel = kernel;
     });

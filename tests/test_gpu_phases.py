@@ -176,12 +176,15 @@ def _wide_pair():
     return gpu, orc, fluid, widths
 
 
-@pytest.mark.parametrize("kernel", [_lib.PCG_ONE_BLOCK, _lib.PCG_CLUSTER], ids=["one_block", "cluster"])
+@pytest.mark.parametrize("kernel", [_lib.PCG_ONE_BLOCK, _lib.PCG_CLUSTER, _lib.PCG_TILES],
+                         ids=["one_block", "cluster", "tiles"])
 def test_project_wide_levels_bit_exact(kernel):
     """Wide wavefront levels: the one-block kernel takes its global-memory path
     for them (and the window path around them); the cluster kernel spreads
-    every level over its CTAs. With the reference dot order both give the
-    reference's pressure and iteration count bit for bit."""
+    every level over its CTAs; the tiled kernel walks 16 x 16-line tiles over
+    the whole GPU, handing boundary values between tiles. With the reference
+    dot order all three give the reference's pressure and iteration count bit
+    for bit."""
     gpu, orc, fluid, widths = _wide_pair()
     gpu.set_dot_order(True)
     gpu.set_pcg_kernel(kernel)
@@ -192,11 +195,13 @@ def test_project_wide_levels_bit_exact(kernel):
     pg, po = gpu.pressure(), orc.pressure()
     it_g, it_o = gpu.last_pcg_iters, orc.scalars()["last_pcg_iters"]
     diff = int(np.sum(pg.view(np.uint64) != po.view(np.uint64)))
-    name = "project_wide" if kernel == _lib.PCG_ONE_BLOCK else "project_wide_cluster"
+    name = {_lib.PCG_ONE_BLOCK: "project_wide", _lib.PCG_CLUSTER: "project_wide_cluster",
+            _lib.PCG_TILES: "project_wide_tiles"}[kernel]
     record(name, {"fluid_cells": int(fluid.sum()), "max_level_width": int(widths.max()),
                   "levels_over_736": int((widths > 736).sum()), "iters_gpu": it_g, "iters_orc": it_o,
                   "pressure_bit_mismatch": diff, "pcg_ms": prof["pcg_ms"]})
     assert prof["pcg_cluster_launches"] == (1 if kernel == _lib.PCG_CLUSTER else 0)
+    assert prof["pcg_tile_launches"] == (1 if kernel == _lib.PCG_TILES else 0)
     assert widths.max() > 768
     assert it_g == it_o
     assert diff == 0
@@ -205,12 +210,12 @@ def test_project_wide_levels_bit_exact(kernel):
 def test_project_tree_dots_same_bits_for_every_kernel():
     """The default tree-order dots do not depend on where the solve runs:
     sweeps on one SM with the rest on 1, 2 or 4 CTAs or the device's largest
-    cluster, or everything on the cluster kernel, give the same pressure bits
-    and iteration count."""
+    cluster, everything on the cluster kernel, or the tiled solve over the
+    whole GPU, give the same pressure bits and iteration count."""
     runs = {}
     for name, kernel, ctas in [("one_cta", _lib.PCG_ONE_BLOCK, 1), ("two_ctas", _lib.PCG_ONE_BLOCK, 2),
                                ("four_ctas", _lib.PCG_ONE_BLOCK, 4), ("auto", _lib.PCG_ONE_BLOCK, 0),
-                               ("cluster", _lib.PCG_CLUSTER, 0)]:
+                               ("cluster", _lib.PCG_CLUSTER, 0), ("tiles", _lib.PCG_TILES, 0)]:
         gpu, orc, fluid, widths = _wide_pair()
         gpu.set_pcg_kernel(kernel)
         gpu.set_pcg_ctas(ctas)
