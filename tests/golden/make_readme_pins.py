@@ -1,7 +1,7 @@
 """Regenerate readme_pins.json: the oracle run on the reference's two README scenes.
 
-Reads the reference checkout (default /root/reference, or $SDR_REFERENCE) at
-generation time only; the committed JSON is what the tests read. The pinned
+Reads the reference checkout named by $SDR_REFERENCE (required) at generation
+time only; the committed JSON is what the tests read. The pinned
 README figures (uselessgoddess/sdr README.md:58-61 and 146-151):
   examples/scene.toml          peak fill 19.9 %, peak coverage 59.1 %,
                                peak membrane 1099.3 mmHg (146558 Pa),
@@ -23,10 +23,12 @@ import oracle  # noqa: E402
 from sdr_b200 import scene as sc  # noqa: E402
 from tests.helpers import cavity_volume, oracle_sdf, oracle_solver  # noqa: E402
 
-REF = os.environ.get("SDR_REFERENCE", "/root/reference")
+REF = os.environ.get("SDR_REFERENCE")
 
 
 def run(name: str, threads: int):
+    if not REF:
+        raise SystemExit("set SDR_REFERENCE to the reference checkout (the directory holding examples/)")
     oracle.set_threads(threads)
     path = os.path.join(REF, "examples", f"{name}.toml")
     cfg = sc.SceneConfig.from_toml_file(path)
