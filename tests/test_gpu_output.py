@@ -58,3 +58,39 @@ def test_metrics_files_from_a_run(tmp_path):
     frames = json.loads((tmp_path / "metrics.json").read_text())
     assert [f["frame"] for f in frames] == [0, 1, 2] and frames[2]["particles"] == m.history[2]["particles"]
     assert json.loads((tmp_path / "summary.json").read_text()) == m.summary()
+
+
+def _read_vtk_points(path):
+    """POINTS block of a legacy ASCII VTK file (read_points_vtk, output.rs:57-96)."""
+    import numpy as np
+    lines = open(path).read().split("\n")
+    i = next(k for k, l in enumerate(lines) if l.startswith("POINTS"))
+    n = int(lines[i].split()[1])
+    vals = " ".join(lines[i + 1:]).split()[: 3 * n]
+    return np.array([float(v) for v in vals]).reshape(n, 3)
+
+
+def test_frame_files_hold_the_solver_state(tmp_path):
+    """The background writer's frames against the solver's own particle
+    state, read back independently: VTK text parses back to the stored f32
+    positions bit for bit (shortest round-trip digits, output.rs:23-48), XYZ
+    bytes are those f32 values (output.rs:98-110)."""
+    import numpy as np
+    from sdr_b200.solver import build_scene
+    b = build_scene(sc.SceneConfig.from_toml_str(SMOKE_TOML))
+    for fmt in ("vtk", "xyz"):
+        d = tmp_path / fmt
+        d.mkdir()
+        with FrameWriter(d, "particles", fmt) as w:
+            b.solver.step(b.frame_dt)
+            w.submit(b.solver, 7)
+            w.flush()
+        pos32, _ = b.solver.particles_f32()
+        path = frame_path(d, "particles", 7, fmt)
+        if fmt == "vtk":
+            back = _read_vtk_points(path)
+            assert back.shape == pos32.shape and len(back) > 0
+            assert np.array_equal(back, pos32.astype(np.float64))
+        else:
+            raw = np.fromfile(path, dtype="<f4").reshape(-1, 3)
+            assert np.array_equal(raw.view(np.uint32), np.ascontiguousarray(pos32, dtype=np.float32).view(np.uint32))
