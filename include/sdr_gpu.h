@@ -487,6 +487,20 @@ int sdr_batch_create(const sdr_scene_desc* scenes, size_t n, int32_t device, sdr
  * failures are reported per scene by sdr_batch_result; the call itself fails
  * only for bad arguments. */
 int sdr_batch_run(sdr_batch* b, uint32_t concurrency);
+/* The batch's scenes packed together (no counterpart in the reference, which
+ * runs one scene per process): every packed step advances each live scene by
+ * one substep at its own CFL step, and each operation of the substep is ONE
+ * launch for all of them - a ragged offset table gives every scene its share
+ * of the launch's blocks, and a persistent grid walks them running the
+ * operation's kernel body with that scene's arguments (each scene's pressure
+ * solve is one block, which runs to that scene's own convergence). Scenes
+ * leave as they finish their frames. Every scene computes exactly what it
+ * computes alone, so results equal sdr_batch_run's bit for bit. Scene times
+ * (sdr_batch_result's seconds) run from the start of the call to the scene's
+ * last frame. */
+int sdr_batch_run_packed(sdr_batch* b);
+/* Launches and packed steps of the last sdr_batch_run_packed. */
+int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps);
 /* status: SDR_OK or the scene's error code (message in `error`, may be NULL). */
 int sdr_batch_result(const sdr_batch* b, size_t i, int32_t* status, sdr_summary* summary,
                      sdr_solver_stats* stats_or_null, double* seconds_or_null, char* error, size_t error_cap);
@@ -503,6 +517,11 @@ typedef struct {
     uint64_t bytes_in_use, peak_bytes;
 } sdr_server_stats;
 int sdr_server_create(int32_t device, uint64_t budget_bytes, uint32_t max_active, sdr_server** out);
+/* The same request loop with every admitted scene in one packed engine
+ * (sdr_batch_run_packed): requests join the packed steps as slots and budget
+ * free up and leave when their summary is ready - continuous batching on one
+ * host thread and one stream. */
+int sdr_server_create_packed(int32_t device, uint64_t budget_bytes, uint32_t max_active, sdr_server** out);
 int sdr_server_submit(sdr_server* s, const sdr_scene_desc* scene, uint64_t* ticket);
 /* state: SDR_REQ_*. When done: the summary and the seconds from submission to
  * summary (time-to-summary); when failed: the message in `error` (may be NULL). */

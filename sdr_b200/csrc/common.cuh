@@ -16,6 +16,13 @@ enum : uint8_t { SOLID = 0, FLUID = 1, AIR = 2 };
 
 constexpr int kInvalid = -1;
 
+// The block a kernel body runs as: its index and the block count of its
+// launch. A plain launch passes (blockIdx.x, gridDim.x); a packed launch of
+// many scenes passes the block's place within its own scene's share.
+struct VB {
+    uint32_t bid, nb;
+};
+
 // Uncontracted f64 arithmetic (the reference's Rust emits no FMA).
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }

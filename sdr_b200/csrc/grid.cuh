@@ -49,10 +49,10 @@ __device__ __forceinline__ double sdf_sample_d(const SdfD& s, double px, double 
 
 // cavity_mask (solver.rs:194-199) and the static half of classify
 // (solver.rs:344-361): outlet cells are Air, non-cavity Solid, the rest Air.
-__global__ void k_cavity_and_base(Grid g, SdfD s, int has_outlet, Aabb outlet,
+__device__ __forceinline__ void k_cavity_and_base_body(VB vb_, Grid g, SdfD s, int has_outlet, Aabb outlet,
                                   uint8_t* __restrict__ cavity, uint8_t* __restrict__ base,
                                   int recompute_cavity) {
-    size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t c = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     size_t n = (size_t)g.nx * g.ny * g.nz;
     if (c >= n) return;
     int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / ((size_t)g.nx * g.ny);
@@ -69,12 +69,15 @@ __global__ void k_cavity_and_base(Grid g, SdfD s, int has_outlet, Aabb outlet,
     bool out = has_outlet && aabb_contains(outlet, cx, cy, cz);
     base[c] = out ? AIR : (!cav ? SOLID : AIR);
 }
+__global__ void k_cavity_and_base(Grid g, SdfD s, int has_outlet, Aabb outlet,
+                                  uint8_t* __restrict__ cavity, uint8_t* __restrict__ base,
+                                  int recompute_cavity) { k_cavity_and_base_body(VB{blockIdx.x, gridDim.x}, g, s, has_outlet, outlet, cavity, base, recompute_cavity); }
 
 // Validity for extrapolation: the face borders a Fluid cell (solver.rs:612-642).
-__global__ void k_extrap_valid(Grid g, const uint8_t* __restrict__ cells, uint8_t* __restrict__ ku,
+__device__ __forceinline__ void k_extrap_valid_body(VB vb_, Grid g, const uint8_t* __restrict__ cells, uint8_t* __restrict__ ku,
                                uint8_t* __restrict__ kv, uint8_t* __restrict__ kw) {
     int i, j, k;
-    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!node_of(g, (size_t)vb_.bid * blockDim.x + threadIdx.x, i, j, k)) return;
     auto fl = [&](int a, int b, int c) {
         return cells[((size_t)c * g.ny + b) * g.nx + a] == FLUID;
     };
@@ -85,6 +88,8 @@ __global__ void k_extrap_valid(Grid g, const uint8_t* __restrict__ cells, uint8_
     if (i < g.nx && j < g.ny)
         kw[((size_t)k * g.ny + j) * g.nx + i] = (k > 0 && fl(i, j, k - 1)) || (k < g.nz && fl(i, j, k));
 }
+__global__ void k_extrap_valid(Grid g, const uint8_t* __restrict__ cells, uint8_t* __restrict__ ku,
+                               uint8_t* __restrict__ kv, uint8_t* __restrict__ kw) { k_extrap_valid_body(VB{blockIdx.x, gridDim.x}, g, cells, ku, kv, kw); }
 
 // One snapshot sweep of extrapolate (solver.rs:964-1007) on one component,
 // in place. kn holds 0 for unknown, 1 for known from the start and s + 2 for
@@ -129,11 +134,11 @@ struct ExtrapArgs {
     unsigned int* maxbits;  // optional: |u|,|v|,|w| maxima (last sweep)
 };
 
-__global__ void __launch_bounds__(256) k_extrap(ExtrapArgs a) {
+__device__ __forceinline__ void k_extrap_body(VB vb_, ExtrapArgs a) {
     const Grid& g = a.g;
     int i, j, k;
     float mu = 0.f, mv = 0.f, mw = 0.f;
-    if (node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) {
+    if (node_of(g, (size_t)vb_.bid * blockDim.x + threadIdx.x, i, j, k)) {
         if (j < g.ny && k < g.nz) {
             extrap_one(a.u, a.ku, a.sweep, g.nx + 1, g.ny, g.nz, i, j, k);
             if (a.maxbits) mu = fabsf(a.u[((size_t)k * g.ny + j) * (g.nx + 1) + i]);
@@ -161,14 +166,16 @@ __global__ void __launch_bounds__(256) k_extrap(ExtrapArgs a) {
         }
     }
 }
+__global__ void __launch_bounds__(256) k_extrap(ExtrapArgs a) { k_extrap_body(VB{blockIdx.x, gridDim.x}, a); }
 
 // Face maxima alone (used when extrapolation did not run, e.g. phase mode).
-__global__ void k_face_max(const float* __restrict__ f, size_t n, unsigned int* __restrict__ out) {
+__device__ __forceinline__ void k_face_max_body(VB vb_, const float* __restrict__ f, size_t n, unsigned int* __restrict__ out) {
     float m = 0.f;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    for (size_t q = (size_t)vb_.bid * blockDim.x + threadIdx.x; q < n; q += (size_t)vb_.nb * blockDim.x)
         m = fmaxf(m, fabsf(f[q]));
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
+__global__ void k_face_max(const float* __restrict__ f, size_t n, unsigned int* __restrict__ out) { k_face_max_body(VB{blockIdx.x, gridDim.x}, f, n, out); }
 
 }  // namespace sdr

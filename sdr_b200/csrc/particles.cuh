@@ -12,23 +12,25 @@ constexpr int kBS = 256;
 
 // ------------------------------------------------------------------ classify
 // Solver::classify (solver.rs:342-371) first half: static labels per cell.
-__global__ void k_base_labels(const uint8_t* __restrict__ base, uint8_t* __restrict__ cells,
+__device__ __forceinline__ void k_base_labels_body(VB vb_, const uint8_t* __restrict__ base, uint8_t* __restrict__ cells,
                               size_t n) {
-    size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t c = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     if (c < n) cells[c] = base[c];
 }
+__global__ void k_base_labels(const uint8_t* __restrict__ base, uint8_t* __restrict__ cells,
+                              size_t n) { k_base_labels_body(VB{blockIdx.x, gridDim.x}, base, cells, n); }
 
 // Per particle: the f64 cell key of Solver::cell_of (labels, histograms) and
 // the clamped cell the P2G gather bins by (from the same f64 grid coordinate
 // the gather's weights use, so every contribution lands in the gathered stencil).
 // With mark_fluid, also the second half of classify: Air cells holding a
 // particle that is not in the outlet become Fluid (solver.rs:362-370).
-__global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t n,
+__device__ __forceinline__ void k_classify_keys_body(VB vb_, Grid g, const float4* __restrict__ pos, uint32_t n,
                                 int has_outlet, Aabb outlet, int mark_fluid,
                                 uint8_t* __restrict__ cells, int* __restrict__ key_cell,
                                 uint32_t* __restrict__ key_sort, uint32_t* __restrict__ hist_valid,
                                 uint32_t* __restrict__ hist_sort) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     if (p >= n) return;
     float4 q = pos[p];
     int c = cell_of(g, q.x, q.y, q.z);
@@ -48,25 +50,32 @@ __global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t
     key_sort[p] = ks;
     atomicAdd(&hist_sort[ks], 1u);
 }
+__global__ void k_classify_keys(Grid g, const float4* __restrict__ pos, uint32_t n,
+                                int has_outlet, Aabb outlet, int mark_fluid,
+                                uint8_t* __restrict__ cells, int* __restrict__ key_cell,
+                                uint32_t* __restrict__ key_sort, uint32_t* __restrict__ hist_valid,
+                                uint32_t* __restrict__ hist_sort) { k_classify_keys_body(VB{blockIdx.x, gridDim.x}, g, pos, n, has_outlet, outlet, mark_fluid, cells, key_cell, key_sort, hist_valid, hist_sort); }
 
 // ------------------------------------------------------------------ counting sort
 // Slot assignment within each cell segment (start from the exclusive scan).
-__global__ void k_sort_scatter(const uint32_t* __restrict__ key, uint32_t n,
+__device__ __forceinline__ void k_sort_scatter_body(VB vb_, const uint32_t* __restrict__ key, uint32_t n,
                                uint32_t* __restrict__ fill, uint32_t* __restrict__ perm) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     if (p >= n) return;
     uint32_t s = atomicAdd(&fill[key[p]], 1u);
     perm[s] = p;
 }
+__global__ void k_sort_scatter(const uint32_t* __restrict__ key, uint32_t n,
+                               uint32_t* __restrict__ fill, uint32_t* __restrict__ perm) { k_sort_scatter_body(VB{blockIdx.x, gridDim.x}, key, n, fill, perm); }
 
 // Make each segment ascending in particle index, so the permutation equals a
 // stable counting sort (bit-exact vs a CPU stable sort of the same keys) and
 // the gather's summation order is fixed. Short segments: insertion sort by
 // one thread; long ones are queued for k_sort_long.
-__global__ void k_sort_segments(const uint32_t* __restrict__ start, uint32_t ncell,
+__device__ __forceinline__ void k_sort_segments_body(VB vb_, const uint32_t* __restrict__ start, uint32_t ncell,
                                 uint32_t* __restrict__ perm, uint32_t* __restrict__ long_list,
                                 uint32_t* __restrict__ long_count) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = vb_.bid * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     uint32_t a = start[c], b = start[c + 1];
     uint32_t len = b - a;
@@ -86,13 +95,16 @@ __global__ void k_sort_segments(const uint32_t* __restrict__ start, uint32_t nce
         perm[y] = v;
     }
 }
+__global__ void k_sort_segments(const uint32_t* __restrict__ start, uint32_t ncell,
+                                uint32_t* __restrict__ perm, uint32_t* __restrict__ long_list,
+                                uint32_t* __restrict__ long_count) { k_sort_segments_body(VB{blockIdx.x, gridDim.x}, start, ncell, perm, long_list, long_count); }
 
 // Rank sort of long segments (indices are distinct): one block per segment.
-__global__ void k_sort_long(const uint32_t* __restrict__ start, const uint32_t* __restrict__ long_list,
+__device__ __forceinline__ void k_sort_long_body(VB vb_, const uint32_t* __restrict__ start, const uint32_t* __restrict__ long_list,
                             const uint32_t* __restrict__ long_count, uint32_t* __restrict__ perm,
                             uint32_t* __restrict__ tmp) {
     uint32_t nl = *long_count;
-    for (uint32_t q = blockIdx.x; q < nl; q += gridDim.x) {
+    for (uint32_t q = vb_.bid; q < nl; q += vb_.nb) {
         uint32_t c = long_list[q];
         uint32_t a = start[c], b = start[c + 1];
         for (uint32_t x = a + threadIdx.x; x < b; x += blockDim.x) {
@@ -106,14 +118,17 @@ __global__ void k_sort_long(const uint32_t* __restrict__ start, const uint32_t* 
         __syncthreads();
     }
 }
+__global__ void k_sort_long(const uint32_t* __restrict__ start, const uint32_t* __restrict__ long_list,
+                            const uint32_t* __restrict__ long_count, uint32_t* __restrict__ perm,
+                            uint32_t* __restrict__ tmp) { k_sort_long_body(VB{blockIdx.x, gridDim.x}, start, long_list, long_count, perm, tmp); }
 
 // ------------------------------------------------------------------ P2G gather
 // Sorted particle records for the gather: the f64 grid coordinate
 // (p - origin)/dx of Solver's u/v/w_coords (grid.rs:161-175) and the f32 velocity.
-__global__ void k_sorted_records(Grid g, const float4* __restrict__ pos, const float4* __restrict__ vel,
+__device__ __forceinline__ void k_sorted_records_body(VB vb_, Grid g, const float4* __restrict__ pos, const float4* __restrict__ vel,
                                  const uint32_t* __restrict__ perm, uint32_t n, double4* __restrict__ lrec,
                                  float4* __restrict__ vrec) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t s = vb_.bid * blockDim.x + threadIdx.x;
     if (s >= n) return;
     uint32_t p = perm[s];
     float4 q = pos[p];
@@ -121,6 +136,9 @@ __global__ void k_sorted_records(Grid g, const float4* __restrict__ pos, const f
                            ddiv(dsub((double)q.z, g.oz), g.dx), 0.0);
     vrec[s] = vel[p];
 }
+__global__ void k_sorted_records(Grid g, const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                 const uint32_t* __restrict__ perm, uint32_t n, double4* __restrict__ lrec,
+                                 float4* __restrict__ vrec) { k_sorted_records_body(VB{blockIdx.x, gridDim.x}, g, pos, vel, perm, n, lrec, vrec); }
 
 struct P2GArgs {
     Grid g;
@@ -211,10 +229,10 @@ __device__ __forceinline__ void p2g_store(const P2GArgs& a, int i, int j, int k,
 // (the node owns the u, v and w faces with that index). A node with no
 // particle in the 27 cells around it gets its faces at once (all sums +0);
 // the others are queued for k_p2g.
-__global__ void __launch_bounds__(kBS) k_p2g_nodes(P2GArgs a, uint32_t* __restrict__ list,
+__device__ __forceinline__ void k_p2g_nodes_body(VB vb_, P2GArgs a, uint32_t* __restrict__ list,
                                                    uint32_t* __restrict__ count) {
     const Grid& g = a.g;
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t t = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     int i, j, k;
     if (!node_of(g, t, i, j, k)) return;
     uint32_t cnt = 0;
@@ -227,6 +245,8 @@ __global__ void __launch_bounds__(kBS) k_p2g_nodes(P2GArgs a, uint32_t* __restri
     if (cnt) list[atomicAdd(count, 1u)] = (uint32_t)t;
     else p2g_store(a, i, j, k, j < g.ny && k < g.nz, i < g.nx && k < g.nz, i < g.nx && j < g.ny, 0, 0, 0, 0, 0, 0);
 }
+__global__ void __launch_bounds__(kBS) k_p2g_nodes(P2GArgs a, uint32_t* __restrict__ list,
+                                                   uint32_t* __restrict__ count) { k_p2g_nodes_body(VB{blockIdx.x, gridDim.x}, a, list, count); }
 
 // P2G gather of the queued nodes, eight lanes each. The lanes split the
 // particles of the 27 cells around the node — for each (k, j) the three cells
@@ -239,12 +259,12 @@ __global__ void __launch_bounds__(kBS) k_p2g_nodes(P2GArgs a, uint32_t* __restri
 // for hundreds of sequential particles. The loop over the queue takes the
 // same trips in every thread, so the shuffles always see whole warps.
 constexpr int kP2GLanes = 8;
-__global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a, const uint32_t* __restrict__ list,
+__device__ __forceinline__ void k_p2g_body(VB vb_, P2GArgs a, const uint32_t* __restrict__ list,
                                              const uint32_t* __restrict__ count) {
     const Grid& g = a.g;
     const uint32_t nq = *count;
-    const uint32_t groups = (uint32_t)(gridDim.x * blockDim.x / kP2GLanes);
-    const uint32_t gid = (uint32_t)((blockIdx.x * blockDim.x + threadIdx.x) / kP2GLanes);
+    const uint32_t groups = (uint32_t)(vb_.nb * blockDim.x / kP2GLanes);
+    const uint32_t gid = (uint32_t)((vb_.bid * blockDim.x + threadIdx.x) / kP2GLanes);
     const int lane = (int)(threadIdx.x % kP2GLanes);
     for (uint32_t base = 0; base < nq; base += groups) {
         const uint32_t h = base + gid;
@@ -302,19 +322,22 @@ __global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a, const uint32_t* __restri
         if (node && lane == 0) p2g_store(a, i, j, k, hu, hv, hw, su, wu, sv, wv, sw, ww);
     }
 }
+__global__ void __launch_bounds__(kBS) k_p2g(P2GArgs a, const uint32_t* __restrict__ list,
+                                             const uint32_t* __restrict__ count) { k_p2g_body(VB{blockIdx.x, gridDim.x}, a, list, count); }
 
 // Solver::add_forces (solver.rs:593-604) on its own (phase mode).
-__global__ void k_add_forces(float* __restrict__ f, size_t n, double gdt) {
-    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_add_forces_body(VB vb_, float* __restrict__ f, size_t n, double gdt) {
+    size_t q = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     if (q < n) f[q] = (float)dadd((double)f[q], gdt);
 }
+__global__ void k_add_forces(float* __restrict__ f, size_t n, double gdt) { k_add_forces_body(VB{blockIdx.x, gridDim.x}, f, n, gdt); }
 
 // enforce_solid_faces (pressure.rs:243-281) on its own (phase mode): one
 // thread per node, owning the u/v/w faces with that index.
-__global__ void k_enforce_solid(Grid g, const uint8_t* __restrict__ cells, float* __restrict__ u,
+__device__ __forceinline__ void k_enforce_solid_body(VB vb_, Grid g, const uint8_t* __restrict__ cells, float* __restrict__ u,
                                 float* __restrict__ v, float* __restrict__ w) {
     int i, j, k;
-    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!node_of(g, (size_t)vb_.bid * blockDim.x + threadIdx.x, i, j, k)) return;
     if (j < g.ny && k < g.nz && (solid_at(g, cells, i - 1, j, k) || solid_at(g, cells, i, j, k)))
         u[((size_t)k * g.ny + j) * (g.nx + 1) + i] = 0.0f;
     if (i < g.nx && k < g.nz && (solid_at(g, cells, i, j - 1, k) || solid_at(g, cells, i, j, k)))
@@ -322,6 +345,8 @@ __global__ void k_enforce_solid(Grid g, const uint8_t* __restrict__ cells, float
     if (i < g.nx && j < g.ny && (solid_at(g, cells, i, j, k - 1) || solid_at(g, cells, i, j, k)))
         w[((size_t)k * g.ny + j) * g.nx + i] = 0.0f;
 }
+__global__ void k_enforce_solid(Grid g, const uint8_t* __restrict__ cells, float* __restrict__ u,
+                                float* __restrict__ v, float* __restrict__ w) { k_enforce_solid_body(VB{blockIdx.x, gridDim.x}, g, cells, u, v, w); }
 
 // ------------------------------------------------------------------ G2P + advect
 struct MoveArgs {
@@ -366,8 +391,8 @@ __device__ __forceinline__ void bounds_flags(const MoveArgs& a, float3 p, uint32
 // and the bounds predicate. Both read the pre-advection position and the same
 // grid, so velocity_at(p0) is shared. Particles are visited in sorted-cell
 // order so neighbouring threads read neighbouring faces.
-__global__ void __launch_bounds__(kBS) k_g2p_advect(MoveArgs a) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_g2p_advect_body(VB vb_, MoveArgs a) {
+    uint32_t t = vb_.bid * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
     uint32_t p = a.order ? a.order[t] : t;
     const Grid& g = a.g;
@@ -408,10 +433,11 @@ __global__ void __launch_bounds__(kBS) k_g2p_advect(MoveArgs a) {
         a.drained[p] = d;
     }
 }
+__global__ void __launch_bounds__(kBS) k_g2p_advect(MoveArgs a) { k_g2p_advect_body(VB{blockIdx.x, gridDim.x}, a); }
 
 // Bounds flags alone (phase mode, after an external position change).
-__global__ void k_bounds_flags(MoveArgs a) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_bounds_flags_body(VB vb_, MoveArgs a) {
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     float4 q = a.pos[p];
     uint32_t k, d;
@@ -419,15 +445,16 @@ __global__ void k_bounds_flags(MoveArgs a) {
     a.keep[p] = k;
     a.drained[p] = d;
 }
+__global__ void k_bounds_flags(MoveArgs a) { k_bounds_flags_body(VB{blockIdx.x, gridDim.x}, a); }
 
 // Stable scatter of kept particles (ParticleSet::retain, particles.rs:38-49)
 // plus the drained/culled tallies.
-__global__ void k_compact(const float4* __restrict__ pos, const float4* __restrict__ vel,
+__device__ __forceinline__ void k_compact_body(VB vb_, const float4* __restrict__ pos, const float4* __restrict__ vel,
                           const uint32_t* __restrict__ keep, const uint32_t* __restrict__ drained,
                           const uint32_t* __restrict__ off, uint32_t n, float4* __restrict__ pos2,
                           float4* __restrict__ vel2, unsigned long long* __restrict__ counters) {
     __shared__ uint32_t sh[33];
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     uint32_t d = 0, c = 0;
     if (p < n) {
         if (keep[p]) {
@@ -446,6 +473,10 @@ __global__ void k_compact(const float4* __restrict__ pos, const float4* __restri
         if (sc) atomicAdd(&counters[1], (unsigned long long)sc);
     }
 }
+__global__ void k_compact(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                          const uint32_t* __restrict__ keep, const uint32_t* __restrict__ drained,
+                          const uint32_t* __restrict__ off, uint32_t n, float4* __restrict__ pos2,
+                          float4* __restrict__ vel2, unsigned long long* __restrict__ counters) { k_compact_body(VB{blockIdx.x, gridDim.x}, pos, vel, keep, drained, off, n, pos2, vel2, counters); }
 
 // ------------------------------------------------------------------ redistribute
 // Solver::redistribute (solver.rs:454-557). Facts the GPU form relies on:
@@ -474,17 +505,20 @@ struct RedistState {
     uint32_t pad;
 };
 
-__global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
+__device__ __forceinline__ void k_redist_hist_n_body(VB vb_, Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
                                 const RedistState* __restrict__ rs, int* __restrict__ key_cell,
                                 uint32_t* __restrict__ count) {
     if (!rs->active) return;
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     if (p >= *n_dev) return;
     float4 q = pos[p];
     int c = cell_of(g, q.x, q.y, q.z);
     key_cell[p] = c;
     if (c >= 0) atomicAdd(&count[c], 1u);
 }
+__global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
+                                const RedistState* __restrict__ rs, int* __restrict__ key_cell,
+                                uint32_t* __restrict__ count) { k_redist_hist_n_body(VB{blockIdx.x, gridDim.x}, g, pos, n_dev, rs, key_cell, count); }
 
 // Particles in over-cap cells, appended in arbitrary order (sorted later).
 // A particle is left out when no face neighbour of its cell is an in-cavity
@@ -492,12 +526,12 @@ __global__ void k_redist_hist_n(Grid g, const float4* __restrict__ pos, const ui
 // receives while below the cap and a source never drains below it, so such a
 // cell never gains a receiver and the reference loop (solver.rs:476-555)
 // leaves every one of its particles where it is. The moves are unchanged.
-__global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
+__device__ __forceinline__ void k_redist_append_body(VB vb_, Grid g, const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
                                 const uint8_t* __restrict__ cavity, const uint32_t* __restrict__ n_dev,
                                 uint32_t cap, RedistState* __restrict__ rs, uint32_t* __restrict__ cand,
                                 uint32_t cand_cap) {
     if (!rs->active) return;
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t p = vb_.bid * blockDim.x + threadIdx.x;
     if (p >= *n_dev) return;
     int c = key_cell[p];
     if (c < 0 || count[c] <= cap) return;
@@ -512,6 +546,10 @@ __global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const 
     uint32_t s = atomicAdd(&rs->ncand, 1u);
     if (s < cand_cap) cand[s] = p;
 }
+__global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const uint32_t* __restrict__ count,
+                                const uint8_t* __restrict__ cavity, const uint32_t* __restrict__ n_dev,
+                                uint32_t cap, RedistState* __restrict__ rs, uint32_t* __restrict__ cand,
+                                uint32_t cand_cap) { k_redist_append_body(VB{blockIdx.x, gridDim.x}, g, key_cell, count, cavity, n_dev, cap, rs, cand, cand_cap); }
 
 constexpr int kRedistTable = 4096;   // shared-memory hash slots (power of two)
 constexpr int kRedistBS = 1024;
@@ -566,7 +604,7 @@ __device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761
 // loop (solver.rs:476-555) on thread 0, then apply the moves (solver.rs:545-554)
 // with all threads. If the table overflows or the list is too long for shared
 // memory, thread 0 replays against the global counts (same result, slower).
-__global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
+__device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     extern __shared__ __align__(16) unsigned char rsm[];
     unsigned long long* tclaim = (unsigned long long*)rsm;  // kRedistTable: claim stamps of the rounds
     int* tkey = (int*)(tclaim + kRedistTable);              // kRedistTable
@@ -851,6 +889,7 @@ __global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) {
     const uint32_t nm = s_nm;
     for (uint32_t mv = threadIdx.x; mv < nm; mv += blockDim.x) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
 }
+__global__ void __launch_bounds__(kRedistBS, 1) k_redist_replay(RedistArgs a) { k_redist_replay_body(VB{blockIdx.x, gridDim.x}, a); }
 
 constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable * 4 * 2 +
                                (size_t)kRedistSmemCand * 4 + (size_t)kRedistSmemCand * 7 * 2 + kRedistTable;
@@ -887,7 +926,7 @@ __device__ __forceinline__ double rp_cluster_sum(double v, double* slots, int& p
     return s;
 }
 
-__global__ void __launch_bounds__(kRpBS, 1) k_redist_par(RedistArgs a) {
+__device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
     __shared__ double sh[40];
     RedistState* rs = a.rs;
     if (!rs->active || !rs->par) return;  // written by earlier launches: the same in every CTA
@@ -1011,5 +1050,6 @@ __global__ void __launch_bounds__(kRpBS, 1) k_redist_par(RedistArgs a) {
         if (nm == 0) rs->active = 0;
     }
 }
+__global__ void __launch_bounds__(kRpBS, 1) k_redist_par(RedistArgs a) { k_redist_par_body(VB{blockIdx.x, gridDim.x}, a); }
 
 }  // namespace sdr

@@ -27,9 +27,9 @@ constexpr int kPcgWin = 6144;  // smem window (doubles) per level buffer
 enum { NB_MX = 0, NB_PX = 1, NB_MY = 2, NB_PY = 3, NB_MZ = 4, NB_PZ = 5 };
 
 // Count fluid cells on each (level, k) line: cells (i, j, k) with i + j + k = L.
-__global__ void k_lines_count(Grid g, const uint8_t* __restrict__ cells, int nlevels,
+__device__ __forceinline__ void k_lines_count_body(VB vb_, Grid g, const uint8_t* __restrict__ cells, int nlevels,
                               uint32_t* __restrict__ cnt) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int t = vb_.bid * blockDim.x + threadIdx.x;
     if (t >= nlevels * g.nz) return;
     int L = t / g.nz, k = t % g.nz;
     int r = L - k;  // i + j = r
@@ -41,12 +41,14 @@ __global__ void k_lines_count(Grid g, const uint8_t* __restrict__ cells, int nle
     }
     cnt[t] = n;
 }
+__global__ void k_lines_count(Grid g, const uint8_t* __restrict__ cells, int nlevels,
+                              uint32_t* __restrict__ cnt) { k_lines_count_body(VB{blockIdx.x, gridDim.x}, g, cells, nlevels, cnt); }
 
 // Assign wavefront positions: pos = line base + rank along j.
-__global__ void k_lines_assign(Grid g, const uint8_t* __restrict__ cells, int nlevels,
+__device__ __forceinline__ void k_lines_assign_body(VB vb_, Grid g, const uint8_t* __restrict__ cells, int nlevels,
                                const uint32_t* __restrict__ base, int* __restrict__ pos_of_cell,
                                uint32_t* __restrict__ lv_cell) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int t = vb_.bid * blockDim.x + threadIdx.x;
     if (t >= nlevels * g.nz) return;
     int L = t / g.nz, k = t % g.nz;
     int r = L - k;
@@ -62,14 +64,19 @@ __global__ void k_lines_assign(Grid g, const uint8_t* __restrict__ cells, int nl
         }
     }
 }
+__global__ void k_lines_assign(Grid g, const uint8_t* __restrict__ cells, int nlevels,
+                               const uint32_t* __restrict__ base, int* __restrict__ pos_of_cell,
+                               uint32_t* __restrict__ lv_cell) { k_lines_assign_body(VB{blockIdx.x, gridDim.x}, g, cells, nlevels, base, pos_of_cell, lv_cell); }
 
 // Level starts from the (level, k) line bases; nf is the device fluid count.
-__global__ void k_level_starts_dev(const uint32_t* __restrict__ base, int nlevels, int nz,
+__device__ __forceinline__ void k_level_starts_dev_body(VB vb_, const uint32_t* __restrict__ base, int nlevels, int nz,
                                    const uint32_t* __restrict__ nf, int* __restrict__ level_start) {
-    int L = blockIdx.x * blockDim.x + threadIdx.x;
+    int L = vb_.bid * blockDim.x + threadIdx.x;
     if (L < nlevels) level_start[L] = (int)base[L * nz];
     if (L == nlevels) level_start[L] = (int)*nf;
 }
+__global__ void k_level_starts_dev(const uint32_t* __restrict__ base, int nlevels, int nz,
+                                   const uint32_t* __restrict__ nf, int* __restrict__ level_start) { k_level_starts_dev_body(VB{blockIdx.x, gridDim.x}, base, nlevels, nz, nf, level_start); }
 
 struct TableArgs {
     Grid g;
@@ -92,8 +99,8 @@ struct TableArgs {
 };
 
 // Per fluid cell: neighbour table, diag, and the RHS b = -(rho dx/dt)(div - s).
-__global__ void k_tables(TableArgs a) {
-    uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_tables_body(VB vb_, TableArgs a) {
+    uint32_t pos = vb_.bid * blockDim.x + threadIdx.x;
     if (pos >= *a.nf) return;
     const Grid& g = a.g;
     uint32_t c = a.lv_cell[pos];
@@ -132,17 +139,19 @@ __global__ void k_tables(TableArgs a) {
     }
     a.b[pos] = dmul(-a.inv_scale, dsub(div, s));
 }
+__global__ void k_tables(TableArgs a) { k_tables_body(VB{blockIdx.x, gridDim.x}, a); }
 
 // Fluid cells in cell-index order -> wavefront position, for the chunked dot.
-__global__ void k_fluid_flags(const uint8_t* __restrict__ cells, size_t n, uint32_t* __restrict__ flag) {
-    size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_fluid_flags_body(VB vb_, const uint8_t* __restrict__ cells, size_t n, uint32_t* __restrict__ flag) {
+    size_t c = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     if (c < n) flag[c] = cells[c] == FLUID;
 }
+__global__ void k_fluid_flags(const uint8_t* __restrict__ cells, size_t n, uint32_t* __restrict__ flag) { k_fluid_flags_body(VB{blockIdx.x, gridDim.x}, cells, n, flag); }
 
-__global__ void k_corder(const uint8_t* __restrict__ cells, size_t n, const uint32_t* __restrict__ off,
+__device__ __forceinline__ void k_corder_body(VB vb_, const uint8_t* __restrict__ cells, size_t n, const uint32_t* __restrict__ off,
                          const int* __restrict__ pos_of_cell, int* __restrict__ corder, int* __restrict__ cinv,
                          int* __restrict__ chunk_start, int nchunks, const uint32_t* __restrict__ nf) {
-    size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t c = (size_t)vb_.bid * blockDim.x + threadIdx.x;
     if (c < n && cells[c] == FLUID) {
         corder[off[c]] = pos_of_cell[c];
         cinv[pos_of_cell[c]] = (int)off[c];
@@ -150,6 +159,9 @@ __global__ void k_corder(const uint8_t* __restrict__ cells, size_t n, const uint
     if (c < n && c % kDotChunk == 0) chunk_start[c / kDotChunk] = (int)off[c];
     if (c == 0) chunk_start[nchunks] = (int)*nf;
 }
+__global__ void k_corder(const uint8_t* __restrict__ cells, size_t n, const uint32_t* __restrict__ off,
+                         const int* __restrict__ pos_of_cell, int* __restrict__ corder, int* __restrict__ cinv,
+                         int* __restrict__ chunk_start, int nchunks, const uint32_t* __restrict__ nf) { k_corder_body(VB{blockIdx.x, gridDim.x}, cells, n, off, pos_of_cell, corder, cinv, chunk_start, nchunks, nf); }
 
 struct PcgArgs {
     const uint32_t* nf;  // device fluid count
@@ -699,7 +711,7 @@ __device__ void pcg_apply_mic0(const PcgArgs& a, const PcgSmem& m, const double*
 // the matvec, the updates of p, r and s, the norms and the dots are spread
 // over all CTAs, whose extra bandwidth they are bound by. Phases are ordered
 // by cluster barriers.
-__global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
+__device__ __forceinline__ void k_pcg_body(VB vb_, PcgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[40];
     PcgSmem m;
@@ -864,14 +876,15 @@ __global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) {
         }
     }
 }
+__global__ void __launch_bounds__(kPcgBS, 1) k_pcg(PcgArgs a) { k_pcg_body(VB{blockIdx.x, gridDim.x}, a); }
 
 // apply_pressure_gradient (pressure.rs:285-332): one thread per node owning
 // its u/v/w faces; f64 update rounded back to the f32 face.
-__global__ void k_gradient(Grid g, const uint8_t* __restrict__ cells, const double* __restrict__ p,
+__device__ __forceinline__ void k_gradient_body(VB vb_, Grid g, const uint8_t* __restrict__ cells, const double* __restrict__ p,
                            double coef, float* __restrict__ u, float* __restrict__ v,
                            float* __restrict__ w) {
     int i, j, k;
-    if (!node_of(g, (size_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!node_of(g, (size_t)vb_.bid * blockDim.x + threadIdx.x, i, j, k)) return;
     size_t c = ((size_t)k * g.ny + j) * g.nx + i;
     if (j < g.ny && k < g.nz && i >= 1 && i < g.nx) {
         uint8_t l = cells[c - 1], r = cells[c];
@@ -895,5 +908,8 @@ __global__ void k_gradient(Grid g, const uint8_t* __restrict__ cells, const doub
         }
     }
 }
+__global__ void k_gradient(Grid g, const uint8_t* __restrict__ cells, const double* __restrict__ p,
+                           double coef, float* __restrict__ u, float* __restrict__ v,
+                           float* __restrict__ w) { k_gradient_body(VB{blockIdx.x, gridDim.x}, g, cells, p, coef, u, v, w); }
 
 }  // namespace sdr

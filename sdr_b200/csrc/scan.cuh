@@ -37,21 +37,23 @@ __device__ __forceinline__ uint32_t block_exscan_u32(uint32_t v, uint32_t& excl,
     return total;
 }
 
-__global__ void __launch_bounds__(kScanBS) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t n,
+__device__ __forceinline__ void k_scan_tiles_body(VB vb_, const uint32_t* __restrict__ in, uint32_t n,
                                                        uint32_t* __restrict__ tile_sums) {
     __shared__ uint32_t sh[33];
-    size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanIPT;
+    size_t base = (size_t)vb_.bid * kScanTile + (size_t)threadIdx.x * kScanIPT;
     uint32_t s = 0;
 #pragma unroll
     for (int q = 0; q < kScanIPT; ++q)
         if (base + q < n) s += in[base + q];
     uint32_t ex;
     uint32_t tot = block_exscan_u32(s, ex, sh);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+    if (threadIdx.x == 0) tile_sums[vb_.bid] = tot;
 }
+__global__ void __launch_bounds__(kScanBS) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t n,
+                                                       uint32_t* __restrict__ tile_sums) { k_scan_tiles_body(VB{blockIdx.x, gridDim.x}, in, n, tile_sums); }
 
 // One block scans all tile sums (exclusive) in order; writes the grand total.
-__global__ void __launch_bounds__(kScanBS) k_scan_sums(uint32_t* __restrict__ sums, uint32_t nt,
+__device__ __forceinline__ void k_scan_sums_body(VB vb_, uint32_t* __restrict__ sums, uint32_t nt,
                                                       uint32_t* __restrict__ total) {
     __shared__ uint32_t sh[33];
     uint32_t carry = 0;
@@ -65,12 +67,14 @@ __global__ void __launch_bounds__(kScanBS) k_scan_sums(uint32_t* __restrict__ su
     }
     if (threadIdx.x == 0 && total) *total = carry;
 }
+__global__ void __launch_bounds__(kScanBS) k_scan_sums(uint32_t* __restrict__ sums, uint32_t nt,
+                                                      uint32_t* __restrict__ total) { k_scan_sums_body(VB{blockIdx.x, gridDim.x}, sums, nt, total); }
 
-__global__ void __launch_bounds__(kScanBS) k_scan_apply(const uint32_t* __restrict__ in, uint32_t n,
+__device__ __forceinline__ void k_scan_apply_body(VB vb_, const uint32_t* __restrict__ in, uint32_t n,
                                                        const uint32_t* __restrict__ tile_off,
                                                        uint32_t* __restrict__ out) {
     __shared__ uint32_t sh[33];
-    size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanIPT;
+    size_t base = (size_t)vb_.bid * kScanTile + (size_t)threadIdx.x * kScanIPT;
     uint32_t v[kScanIPT];
     uint32_t s = 0;
 #pragma unroll
@@ -80,12 +84,15 @@ __global__ void __launch_bounds__(kScanBS) k_scan_apply(const uint32_t* __restri
     }
     uint32_t ex;
     block_exscan_u32(s, ex, sh);
-    uint32_t run = tile_off[blockIdx.x] + ex;
+    uint32_t run = tile_off[vb_.bid] + ex;
 #pragma unroll
     for (int q = 0; q < kScanIPT; ++q) {
         if (base + q < n) out[base + q] = run;
         run += v[q];
     }
 }
+__global__ void __launch_bounds__(kScanBS) k_scan_apply(const uint32_t* __restrict__ in, uint32_t n,
+                                                       const uint32_t* __restrict__ tile_off,
+                                                       uint32_t* __restrict__ out) { k_scan_apply_body(VB{blockIdx.x, gridDim.x}, in, n, tile_off, out); }
 
 }  // namespace sdr

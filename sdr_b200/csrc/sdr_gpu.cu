@@ -34,6 +34,7 @@
 #include "render.cuh"
 #include "scan.cuh"
 #include "sdf.cuh"
+#include "packed.cuh"
 
 using namespace sdr;
 
@@ -43,6 +44,9 @@ thread_local std::string g_err;
 std::atomic<uint64_t> g_launches{0};
 // sdr_debug_inject: the fault the next matching call on this thread injects.
 thread_local int g_fault = 0;
+// Set by a packed batch engine around sdr_solver_create: the new solver runs
+// on the engine's stream instead of a stream of its own.
+thread_local cudaStream_t g_engine_stream = nullptr;
 
 struct Fail {
     int code;
@@ -63,6 +67,12 @@ struct Fail {
         g_launches.fetch_add(1, std::memory_order_relaxed);             \
         CK(cudaGetLastError());                                         \
     } while (0)
+
+// A substep kernel through sdr_solver::issue (launched, or recorded while
+// packing); the call site's line keys its slot in a packed launch.
+#define SLAUNCH(kern, grid, block, smem, stream, ...) issue<kern##_op>(kern, __LINE__, (grid), (block), (smem), __VA_ARGS__)
+#define MSET(p, v, bytes) mset(__LINE__, (p), (v), (bytes))
+#define MCOPY(d, s, bytes) mcopy(__LINE__, (d), (s), (bytes))
 
 inline unsigned blocks(size_t n, unsigned bs) { return (unsigned)std::max<size_t>(1, (n + bs - 1) / bs); }
 
@@ -256,21 +266,66 @@ struct DevStatus {
     unsigned long long redist_cand, redist_sweeps, redist_long;  // cumulative
 };
 
-__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
-__global__ void k_redist_begin(RedistState* r) {
+__device__ __forceinline__ void k_set_u32_body(VB, uint32_t* p, uint32_t v) {
+    if (threadIdx.x == 0) *p = v;
+}
+__global__ void k_set_u32(uint32_t* p, uint32_t v) { k_set_u32_body(VB{blockIdx.x, gridDim.x}, p, v); }
+__device__ __forceinline__ void k_redist_begin_body(VB, RedistState* r) {
+    if (threadIdx.x != 0) return;
     r->ncand = 0;
     r->active = 1;
     r->nmoves = 0;
     r->par = 0;
     r->nmoves_par = 0;
+    r->err = 0;
 }
-__global__ void k_redist_end(const RedistState* r, DevStatus* s) {
+__global__ void k_redist_begin(RedistState* r) { k_redist_begin_body(VB{blockIdx.x, gridDim.x}, r); }
+__device__ __forceinline__ void k_redist_end_body(VB, const RedistState* r, DevStatus* s) {
+    if (threadIdx.x != 0) return;
     s->moves = r->moves_total;
     s->err |= r->err;
     s->redist_cand = r->cand_total;
     s->redist_sweeps = r->sweeps_total;
     s->redist_long = r->long_total;
 }
+__global__ void k_redist_end(const RedistState* r, DevStatus* s) { k_redist_end_body(VB{blockIdx.x, gridDim.x}, r, s); }
+
+// The kernels of a substep as packable operations (largest block of their call sites).
+SDR_OP(k_set_u32, 32)
+SDR_OP(k_scan_tiles, kScanBS)
+SDR_OP(k_scan_sums, kScanBS)
+SDR_OP(k_scan_apply, kScanBS)
+SDR_OP(k_cavity_and_base, 256)
+SDR_OP(k_base_labels, 256)
+SDR_OP(k_classify_keys, kBS)
+SDR_OP(k_sort_scatter, kBS)
+SDR_OP(k_sort_segments, 256)
+SDR_OP(k_sort_long, 256)
+SDR_OP(k_sorted_records, kBS)
+SDR_OP(k_p2g_nodes, kBS)
+SDR_OP(k_p2g, kBS)
+SDR_OP(k_add_forces, 256)
+SDR_OP(k_enforce_solid, 256)
+SDR_OP(k_lines_count, 256)
+SDR_OP(k_lines_assign, 256)
+SDR_OP(k_level_starts_dev, 256)
+SDR_OP(k_tables, 256)
+SDR_OP(k_fluid_flags, 256)
+SDR_OP(k_corder, 256)
+SDR_OP(k_pcg, kPcgBS)
+SDR_OP(k_gradient, 256)
+SDR_OP(k_extrap_valid, 256)
+SDR_OP(k_extrap, 256)
+SDR_OP(k_face_max, 256)
+SDR_OP(k_g2p_advect, kBS)
+SDR_OP(k_bounds_flags, kBS)
+SDR_OP(k_compact, kBS)
+SDR_OP(k_redist_begin, 32)
+SDR_OP(k_redist_hist_n, kBS)
+SDR_OP(k_redist_append, kBS)
+SDR_OP(k_redist_replay, kRedistBS)
+SDR_OP(k_redist_par, kRpBS)
+SDR_OP(k_redist_end, 32)
 __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
     size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < n) out[q] = (float)in[q];
@@ -309,6 +364,8 @@ inline V3 vnorm0(V3 a) {  // math.rs:73-80
 struct sdr_solver {
     int device = 0;
     cudaStream_t st = nullptr;
+    bool own_stream = true;   // false: the stream belongs to a packed batch engine
+    Packer* pk = nullptr;     // set: operations are recorded for a packed launch instead of issued
     std::vector<sdr_metrics*> collectors;  // live metrics collectors of this solver
     Grid g{};
     size_t ncell = 0, nu = 0, nv = 0, nw = 0;
@@ -404,11 +461,43 @@ struct sdr_solver {
     uint64_t particle_substeps = 0, substeps_total = 0;
     double device_ms = 0.0;
 
+    // A kernel of the substep: launched on the solver's stream, or recorded
+    // for the packed launch while a Packer is attached.
+    template <class Op, class Kern, class... A>
+    void issue(Kern kern, int line, unsigned grid, unsigned block, size_t smem, A... args) {
+        if (pk) {
+            pk->record<Op>(line, grid, block, smem, args...);
+            return;
+        }
+        kern<<<grid, block, smem, st>>>(args...);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        CK(cudaGetLastError());
+    }
+    void mset(int line, void* p, int v, size_t bytes) {
+        if (!bytes) return;
+        if (pk) {
+            pk->record<k_pack_memset_op>(line, (unsigned)((bytes + kPackChunk - 1) / kPackChunk), 256, 0,
+                                         static_cast<unsigned char*>(p), v, bytes);
+            return;
+        }
+        CK(cudaMemsetAsync(p, v, bytes, st));
+    }
+    // Device-to-device, or host-to-device from pinned staging.
+    void mcopy(int line, void* d, const void* s, size_t bytes) {
+        if (!bytes) return;
+        if (pk) {
+            pk->record<k_pack_copy_op>(line, (unsigned)((bytes + kPackChunk - 1) / kPackChunk), 256, 0,
+                                       static_cast<unsigned char*>(d), static_cast<const unsigned char*>(s), bytes);
+            return;
+        }
+        CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDefault, st));
+    }
+
     void create_events() {
         for (auto& e : ev) CK(cudaEventCreate(&e));
     }
     void mark(int i) {
-        if (profiling || i == 0 || i == 9) CK(cudaEventRecord(ev[i], st));
+        if (!pk && (profiling || i == 0 || i == 9)) CK(cudaEventRecord(ev[i], st));
     }
     float elapsed(int a, int b) const {
         float ms = 0.f;
@@ -431,9 +520,11 @@ struct sdr_solver {
     Faces saved() const { return Faces{su, sv, sw}; }
     uint32_t* dn() { return &dst->n; }
 
-    void scan(const uint32_t* in, uint32_t* out, size_t n_, uint32_t* total) {
+    // Exclusive scan; `site` (the caller's line) keys its kernels in a packed launch.
+    void scan(const uint32_t* in, uint32_t* out, size_t n_, uint32_t* total, int site) {
+        const int key = 1000000 + 4 * site;
         if (n_ == 0) {
-            if (total) LAUNCH(k_set_u32, 1, 1, 0, st, total, 0u);
+            if (total) issue<k_set_u32_op>(k_set_u32, key, 1, 1, 0, total, 0u);
             return;
         }
         uint32_t nt = (uint32_t)((n_ + kScanTile - 1) / kScanTile);
@@ -441,9 +532,9 @@ struct sdr_solver {
             dalloc(tsum, nt, st);
             tsum_cap = nt;
         }
-        LAUNCH(k_scan_tiles, nt, kScanBS, 0, st, in, (uint32_t)n_, tsum);
-        LAUNCH(k_scan_sums, 1, kScanBS, 0, st, tsum, nt, total);
-        LAUNCH(k_scan_apply, nt, kScanBS, 0, st, in, (uint32_t)n_, tsum, out);
+        issue<k_scan_tiles_op>(k_scan_tiles, key + 1, nt, kScanBS, 0, in, (uint32_t)n_, tsum);
+        issue<k_scan_sums_op>(k_scan_sums, key + 2, 1, kScanBS, 0, tsum, nt, total);
+        issue<k_scan_apply_op>(k_scan_apply, key + 3, nt, kScanBS, 0, in, (uint32_t)n_, tsum, out);
     }
 
     void ensure_capacity(size_t need) {
@@ -558,12 +649,12 @@ struct sdr_solver {
             if (e) cudaEventDestroy(e);
         if (ev_block) cudaEventDestroy(ev_block);
         ev_block = nullptr;
-        if (st) cudaStreamDestroy(st);
+        if (st && own_stream) cudaStreamDestroy(st);
         st = nullptr;
     }
 
     void refresh_base() {
-        LAUNCH(k_cavity_and_base, blocks(ncell, 256), 256, 0, st, g, sdf_d(), (int)has_outlet, outlet,
+        SLAUNCH(k_cavity_and_base, blocks(ncell, 256), 256, 0, st, g, sdf_d(), (int)has_outlet, outlet,
                cavity, base, 0);
     }
 
@@ -602,35 +693,35 @@ struct sdr_solver {
             h_epos[i] = make_float4((float)ps.x, (float)ps.y, (float)ps.z, 0.f);
             h_evel[i] = make_float4((float)vv.x, (float)vv.y, (float)vv.z, 0.f);
         }
-        CK(cudaMemcpyAsync(pos + n, h_epos, k * sizeof(float4), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(vel + n, h_evel, k * sizeof(float4), cudaMemcpyHostToDevice, st));
+        MCOPY(pos + n, h_epos, k * sizeof(float4));
+        MCOPY(vel + n, h_evel, k * sizeof(float4));
         if (profiling) prof.h2d_bytes += 2 * k * sizeof(float4);
         // The staging buffers are reused next substep; the status sync at the
         // end of this substep orders the copies before any reuse.
         n += (uint32_t)k;
         emitted += k;
-        LAUNCH(k_set_u32, 1, 1, 0, st, dn(), n);
+        SLAUNCH(k_set_u32, 1, 1, 0, st, dn(), n);
         sorted_valid = false;
     }
 
     void classify(bool mark) {
-        CK(cudaMemsetAsync(hist_valid, 0, (ncell + 1) * 4, st));
-        CK(cudaMemsetAsync(hist_sort, 0, (ncell + 1) * 4, st));
-        if (mark) LAUNCH(k_base_labels, blocks(ncell, 256), 256, 0, st, base, cells, ncell);
+        MSET(hist_valid, 0, (ncell + 1) * 4);
+        MSET(hist_sort, 0, (ncell + 1) * 4);
+        if (mark) SLAUNCH(k_base_labels, blocks(ncell, 256), 256, 0, st, base, cells, ncell);
         if (n)
-            LAUNCH(k_classify_keys, blocks(n, kBS), kBS, 0, st, g, pos, n, (int)has_outlet, outlet,
+            SLAUNCH(k_classify_keys, blocks(n, kBS), kBS, 0, st, g, pos, n, (int)has_outlet, outlet,
                    (int)mark, cells, key_cell, key_sort, hist_valid, hist_sort);
     }
 
     void sort() {  // counting sort by the f32 P2G cell key
-        scan(hist_sort, start, ncell + 1, &dst->total);
-        CK(cudaMemcpyAsync(fill, start, ncell * 4, cudaMemcpyDeviceToDevice, st));
-        if (n) LAUNCH(k_sort_scatter, blocks(n, kBS), kBS, 0, st, key_sort, n, fill, perm);
-        CK(cudaMemsetAsync(&dst->long_count, 0, 4, st));
-        LAUNCH(k_sort_segments, blocks(ncell, 256), 256, 0, st, start, (uint32_t)ncell, perm, long_list,
+        scan(hist_sort, start, ncell + 1, &dst->total, __LINE__);
+        MCOPY(fill, start, ncell * 4);
+        if (n) SLAUNCH(k_sort_scatter, blocks(n, kBS), kBS, 0, st, key_sort, n, fill, perm);
+        MSET(&dst->long_count, 0, 4);
+        SLAUNCH(k_sort_segments, blocks(ncell, 256), 256, 0, st, start, (uint32_t)ncell, perm, long_list,
                &dst->long_count);
-        LAUNCH(k_sort_long, 148, 256, 0, st, start, long_list, &dst->long_count, perm, ptmp);
-        if (n) LAUNCH(k_sorted_records, blocks(n, kBS), kBS, 0, st, g, pos, vel, perm, n, lrec, vrec);
+        SLAUNCH(k_sort_long, 148, 256, 0, st, start, long_list, &dst->long_count, perm, ptmp);
+        if (n) SLAUNCH(k_sorted_records, blocks(n, kBS), kBS, 0, st, g, pos, vel, perm, n, lrec, vrec);
         sorted_valid = true;
     }
 
@@ -650,18 +741,18 @@ struct sdr_solver {
         a.enforce = fused;
         // empty nodes at once, the rest queued for the eight-lane gather; its grid
         // follows the last queue length (the loop over the queue covers any length)
-        CK(cudaMemsetAsync(&dst->p2g_queue, 0, 4, st));
-        LAUNCH(k_p2g_nodes, blocks(nnodes(), kBS), kBS, 0, st, a, p2g_list, &dst->p2g_queue);
+        MSET(&dst->p2g_queue, 0, 4);
+        SLAUNCH(k_p2g_nodes, blocks(nnodes(), kBS), kBS, 0, st, a, p2g_list, &dst->p2g_queue);
         const size_t want = last_p2g_queue ? ((size_t)last_p2g_queue + last_p2g_queue / 4 + 64) * kP2GLanes
                                            : nnodes() * kP2GLanes;  // no history yet: every node
-        LAUNCH(k_p2g, (unsigned)std::min<size_t>(blocks(want, kBS), 148 * 16), kBS, 0, st, a, p2g_list,
+        SLAUNCH(k_p2g, (unsigned)std::min<size_t>(blocks(want, kBS), 148 * 16), kBS, 0, st, a, p2g_list,
                &dst->p2g_queue);
     }
 
     void add_forces(double dt) {  // solver.rs:593-604
-        if (fluid.gravity.x != 0.0) LAUNCH(k_add_forces, blocks(nu, 256), 256, 0, st, u, nu, fluid.gravity.x * dt);
-        if (fluid.gravity.y != 0.0) LAUNCH(k_add_forces, blocks(nv, 256), 256, 0, st, v, nv, fluid.gravity.y * dt);
-        if (fluid.gravity.z != 0.0) LAUNCH(k_add_forces, blocks(nw, 256), 256, 0, st, w, nw, fluid.gravity.z * dt);
+        if (fluid.gravity.x != 0.0) SLAUNCH(k_add_forces, blocks(nu, 256), 256, 0, st, u, nu, fluid.gravity.x * dt);
+        if (fluid.gravity.y != 0.0) SLAUNCH(k_add_forces, blocks(nv, 256), 256, 0, st, v, nv, fluid.gravity.y * dt);
+        if (fluid.gravity.z != 0.0) SLAUNCH(k_add_forces, blocks(nw, 256), 256, 0, st, w, nw, fluid.gravity.z * dt);
     }
 
     void project(double dt, bool enforce) {  // pressure.rs:123-239 + solver.rs:290-300
@@ -673,13 +764,13 @@ struct sdr_solver {
     // enforce_solid_faces, wavefront numbering, neighbour tables, RHS, dot chunks.
     void project_setup(double dt, bool enforce) {
         unsigned ngrid = blocks(nnodes(), 256);
-        if (enforce) LAUNCH(k_enforce_solid, ngrid, 256, 0, st, g, cells, u, v, w);
+        if (enforce) SLAUNCH(k_enforce_solid, ngrid, 256, 0, st, g, cells, u, v, w);
         size_t nl = (size_t)nlevels * g.nz;
-        LAUNCH(k_lines_count, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt);
-        CK(cudaMemsetAsync(lines_cnt + nl, 0, 4, st));
-        scan(lines_cnt, lines_cnt, nl + 1, &dst->nf);
-        LAUNCH(k_lines_assign, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt, pos_of_cell, lv_cell);
-        LAUNCH(k_level_starts_dev, blocks(nlevels + 1, 256), 256, 0, st, lines_cnt, nlevels, g.nz, &dst->nf,
+        SLAUNCH(k_lines_count, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt);
+        MSET(lines_cnt + nl, 0, 4);
+        scan(lines_cnt, lines_cnt, nl + 1, &dst->nf, __LINE__);
+        SLAUNCH(k_lines_assign, blocks(nl, 256), 256, 0, st, g, cells, nlevels, lines_cnt, pos_of_cell, lv_cell);
+        SLAUNCH(k_level_starts_dev, blocks(nlevels + 1, 256), 256, 0, st, lines_cnt, nlevels, g.nz, &dst->nf,
                level_start);
         TableArgs t{};
         t.g = g;
@@ -700,12 +791,12 @@ struct sdr_solver {
         t.vs_k = k_vol;
         t.vs_unit = g.dx / dt;
         t.vs_cap = 0.25 * t.vs_unit;
-        LAUNCH(k_tables, blocks(ncell, 256), 256, 0, st, t);
-        LAUNCH(k_fluid_flags, blocks(ncell, 256), 256, 0, st, cells, ncell, cflag);
-        scan(cflag, coff, ncell + 1, nullptr);
-        LAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, cinv, chunk_start,
+        SLAUNCH(k_tables, blocks(ncell, 256), 256, 0, st, t);
+        SLAUNCH(k_fluid_flags, blocks(ncell, 256), 256, 0, st, cells, ncell, cflag);
+        scan(cflag, coff, ncell + 1, nullptr, __LINE__);
+        SLAUNCH(k_corder, blocks(ncell, 256), 256, 0, st, cells, ncell, coff, pos_of_cell, corder, cinv, chunk_start,
                nchunks, &dst->nf);
-        CK(cudaMemsetAsync(p_dense, 0, ncell * 8, st));
+        MSET(p_dense, 0, ncell * 8);
     }
 
     void project_solve(double dt) {
@@ -739,6 +830,10 @@ struct sdr_solver {
         a.out_residual = &dst->residual;
         a.timing = kernel_timers ? dst->pcg_cycles : nullptr;
         a.exact_dots = exact_dots ? 1 : 0;
+        if (pk) {  // packed with other scenes: one block per scene, a plain (recordable) launch
+            SLAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+            return;
+        }
         const bool large = pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells && !shared_gpu;
         if ((pcg_kernel == SDR_PCG_TILES || large) && tiles_ready()) {
             launch_tiles(a);
@@ -769,7 +864,7 @@ struct sdr_solver {
             if (ctas == 1) {
                 // a plain launch: the kernel sees a cluster of one CTA, and the
                 // launch overlaps other streams' kernels like any other
-                LAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
+                SLAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
             } else {
                 launch_one_cluster_smem(k_pcg, ctas, kPcgBS, kPcgSmem, st, a);
             }
@@ -834,24 +929,24 @@ struct sdr_solver {
     void project_gradient(double dt) {
         unsigned ngrid = blocks(nnodes(), 256);
         double coef = dt / (fluid.density * g.dx);
-        LAUNCH(k_gradient, ngrid, 256, 0, st, g, cells, p_dense, coef, u, v, w);
+        SLAUNCH(k_gradient, ngrid, 256, 0, st, g, cells, p_dense, coef, u, v, w);
     }
 
     void extrapolate() {  // solver.rs:608-647
         unsigned ngrid = blocks(nnodes(), 256);
-        LAUNCH(k_extrap_valid, ngrid, 256, 0, st, g, cells, ku, kv, kw);
-        CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
+        SLAUNCH(k_extrap_valid, ngrid, 256, 0, st, g, cells, ku, kv, kw);
+        MSET(dst->maxbits, 0, sizeof(dst->maxbits));
         for (int it = 0; it < 4; ++it) {  // four sweeps, in place
             ExtrapArgs e{g, u, v, w, ku, kv, kw, it, it == 3 ? dst->maxbits : nullptr};
-            LAUNCH(k_extrap, ngrid, 256, 0, st, e);
+            SLAUNCH(k_extrap, ngrid, 256, 0, st, e);
         }
     }
 
     void face_max() {
-        CK(cudaMemsetAsync(dst->maxbits, 0, sizeof(dst->maxbits), st));
-        LAUNCH(k_face_max, 296, 256, 0, st, u, nu, &dst->maxbits[0]);
-        LAUNCH(k_face_max, 296, 256, 0, st, v, nv, &dst->maxbits[1]);
-        LAUNCH(k_face_max, 296, 256, 0, st, w, nw, &dst->maxbits[2]);
+        MSET(dst->maxbits, 0, sizeof(dst->maxbits));
+        SLAUNCH(k_face_max, 296, 256, 0, st, u, nu, &dst->maxbits[0]);
+        SLAUNCH(k_face_max, 296, 256, 0, st, v, nv, &dst->maxbits[1]);
+        SLAUNCH(k_face_max, 296, 256, 0, st, w, nw, &dst->maxbits[2]);
     }
 
     MoveArgs move_args(double dt) {
@@ -883,17 +978,17 @@ struct sdr_solver {
         a.do_g2p = g2p_on;
         a.do_advect = advect_on;
         a.do_bounds = bounds_on;
-        LAUNCH(k_g2p_advect, blocks(n, kBS), kBS, 0, st, a);
+        SLAUNCH(k_g2p_advect, blocks(n, kBS), kBS, 0, st, a);
     }
 
     void compact(bool flags_ready) {  // solver.rs:736-755
         if (!n) return;
         if (!flags_ready) {
             MoveArgs a = move_args(0.0);
-            LAUNCH(k_bounds_flags, blocks(n, kBS), kBS, 0, st, a);
+            SLAUNCH(k_bounds_flags, blocks(n, kBS), kBS, 0, st, a);
         }
-        scan(flag, off, n, dn());
-        LAUNCH(k_compact, blocks(n, kBS), kBS, 0, st, pos, vel, flag, drn, off, n, pos2, vel2, &dst->drained);
+        scan(flag, off, n, dn(), __LINE__);
+        SLAUNCH(k_compact, blocks(n, kBS), kBS, 0, st, pos, vel, flag, drn, off, n, pos2, vel2, &dst->drained);
         std::swap(pos, pos2);
         std::swap(vel, vel2);
         sorted_valid = false;
@@ -929,30 +1024,37 @@ struct sdr_solver {
         for (int d = 0; d < 6; ++d) ra.down[d] = dirs[d][0] * gd.x + dirs[d][1] * gd.y + dirs[d][2] * gd.z;
         ra.moves = moves;
         ra.rs = rds;
-        LAUNCH(k_redist_begin, 1, 1, 0, st, rds);
+        SLAUNCH(k_redist_begin, 1, 1, 0, st, rds);
         for (int sweep = 0; sweep < 4; ++sweep) {
-            CK(cudaMemsetAsync(hist_valid, 0, ncell * 4, st));
-            LAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), rds, key_cell, hist_valid);
-            LAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, g, key_cell, hist_valid, cavity, dn(), cap_, rds, cand,
+            MSET(hist_valid, 0, ncell * 4);
+            SLAUNCH(k_redist_hist_n, blocks(n_upper, kBS), kBS, 0, st, g, pos, dn(), rds, key_cell, hist_valid);
+            SLAUNCH(k_redist_append, blocks(n_upper, kBS), kBS, 0, st, g, key_cell, hist_valid, cavity, dn(), cap_, rds, cand,
                    (uint32_t)cand_n);
-            LAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
+            SLAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
             // long lists only (the replay kernel hands over through the state; otherwise it returns at once)
-            if (rp_ctas == 1) LAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
+            if (rp_ctas == 1) SLAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
             else launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
         }
-        LAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
+        SLAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
         sorted_valid = false;
     }
 
-    void sync_status() {
-        CK(cudaMemcpyAsync(hst, dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+    // The status block back to the host (recorded while packing).
+    void status_issue() {
+        MCOPY(hst, dst, sizeof(DevStatus));
         if (profiling) prof.d2h_bytes += sizeof(DevStatus);
+    }
+    void sync_status() {
+        status_issue();
         if (ev_block) {  // the waiting thread sleeps instead of spinning
             CK(cudaEventRecord(ev_block, st));
             CK(cudaEventSynchronize(ev_block));
         } else {
             CK(cudaStreamSynchronize(st));
         }
+        status_read();
+    }
+    void status_read() {
         n = hst->n;
         drained = hst->drained;
         culled = hst->culled;
@@ -980,6 +1082,17 @@ struct sdr_solver {
     }
 
     void substep(double dt) {  // solver.rs:284-310
+        substep_issue(dt);
+        sync_status();
+        substep_finish(dt);
+    }
+
+    uint32_t pending_n_before = 0;  // particles the substep in flight advanced
+    bool pending_timed = false;     // its start and end events were recorded
+
+    // Every operation of one substep, on the stream or into the Packer.
+    void substep_issue(double dt) {
+        pending_timed = pk == nullptr;
         mark(0);
         emit(dt);
         classify(true);
@@ -997,21 +1110,26 @@ struct sdr_solver {
         g2p_advect(dt, true, true, true, true);
         mark(6);
         uint32_t n_before = n;
+        pending_n_before = n_before;
         compact(true);
         mark(7);
         if (fluid.redistribute) redistribute(n_before);
         mark(8);
         mark(9);
-        sync_status();
+    }
+
+    // Bookkeeping once the substep's status block is on the host.
+    void substep_finish(double dt) {
+        const uint32_t n_before = pending_n_before;
         last_pcg_iters = (uint64_t)hst->iters;
         last_residual = hst->residual;
         last_nf = hst->nf;
         last_p2g_queue = hst->p2g_queue;
         read_grid_speed();
-        device_ms += elapsed(0, 9);
+        if (pending_timed) device_ms += elapsed(0, 9);
         particle_substeps += n_before;
         substeps_total += 1;
-        if (profiling) {
+        if (profiling && pending_timed) {
             prof.emit_classify_sort_ms += elapsed(0, 1);
             prof.p2g_ms += elapsed(1, 2);
             prof.pressure_setup_ms += elapsed(2, 3);
@@ -1260,7 +1378,12 @@ int sdr_solver_create(const sdr_sdf_desc* sdf, double sim_dx, const sdr_fluid_pa
             if (prop.major != 10)
                 throw Fail{SDR_ERR_NO_DEVICE, "this library is built for sm_100a (B200); device is sm_" +
                                                   std::to_string(prop.major) + std::to_string(prop.minor)};
-            CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+            if (g_engine_stream) {
+                s->st = g_engine_stream;
+                s->own_stream = false;
+            } else {
+                CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+            }
             s->create_events();
             s->shared_gpu = options && (options->flags & SDR_SOLVER_SHARED_GPU);
             if (options && (options->flags & SDR_SOLVER_BLOCKING_SYNC))
@@ -1810,7 +1933,7 @@ int sdr_render_slice(sdr_solver* s, const sdr_slice_plane* plane, uint32_t targe
             CK(cudaMemsetAsync(hist, 0, (nb + 1) * 4, st));
             CK(cudaMemsetAsync(lcount, 0, 4, st));
             if (n) LAUNCH(k_render_amber_keys, blocks(n, 256), 256, 0, st, v, s->pos, n, T, ntx, nty, key, cxy, hist);
-            s->scan(hist, start, nb + 1, nullptr);
+            s->scan(hist, start, nb + 1, nullptr, __LINE__);
             CK(cudaMemcpyAsync(fill, start, nb * 4, cudaMemcpyDeviceToDevice, st));
             if (n) LAUNCH(k_sort_scatter, blocks(n, 256), 256, 0, st, key, n, fill, perm);
             LAUNCH(k_sort_segments, blocks(nb, 256), 256, 0, st, start, nb, perm, longl, lcount);
@@ -2258,3 +2381,221 @@ int sdr_frame_writer_destroy(sdr_frame_writer* w) {
 }
 
 }  // extern "C"
+
+// ================================================================= packed batches
+// Many scenes advanced together: every packed step runs one substep of every
+// live scene (each at its own CFL step, Solver::step's arithmetic per scene),
+// with one launch per substep operation for all of them (packed.cuh). Scenes
+// join and leave between packed steps; a scene's frames, metrics and summary
+// are its own.
+#include "packed_engine.h"
+
+struct PackedEngine {
+    struct Scene {
+        uint64_t tag = 0;
+        sdr_solver* s = nullptr;
+        sdr_metrics* m = nullptr;
+        double frame_dt = 0, remaining = 0, floor_ = 0, sub = 0;
+        uint64_t frame = 0, frames = 0;
+        uint32_t taken = 0;
+    };
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Packer pk;
+    std::vector<Scene> live;
+    unsigned grid_cap = 0;
+    unsigned char* dev_arena = nullptr;
+    size_t dev_cap = 0;
+    unsigned char* host_arena = nullptr;  // pinned
+    size_t host_cap = 0;
+    uint64_t launches = 0, steps = 0;
+
+    void finish(Scene& sc, int status, const std::string& err, std::vector<PackedDone>& done) {
+        PackedDone d;
+        d.tag = sc.tag;
+        d.status = status;
+        d.error = err;
+        if (status == SDR_OK) {
+            if (sdr_metrics_summary(sc.m, &d.summary) != SDR_OK || sdr_solver_get_stats(sc.s, &d.stats) != SDR_OK) {
+                d.status = SDR_ERR_CUDA;
+                d.error = sdr_last_error();
+            }
+        }
+        if (sc.m) sdr_metrics_destroy(sc.m);
+        if (sc.s) sdr_solver_destroy(sc.s);
+        sc.m = nullptr;
+        sc.s = nullptr;
+        done.push_back(std::move(d));
+    }
+};
+
+PackedEngine* packed_engine_create(int32_t device) {
+    auto* e = new PackedEngine();
+    try {
+        check_device();
+        DeviceScope ds(device);
+        CK(cudaGetDevice(&e->device));
+        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        int nsm = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+        e->grid_cap = (unsigned)nsm * 16;  // persistent CTAs per packed launch
+    } catch (const Fail& f) {
+        if (e->st) cudaStreamDestroy(e->st);
+        delete e;
+        sdr_internal_set_error(f.msg);
+        return nullptr;
+    }
+    return e;
+}
+
+int packed_engine_add(PackedEngine* e, const sdr_scene_desc& d, uint64_t capacity, uint64_t tag,
+                      std::vector<PackedDone>& done) {
+    DeviceScope ds(e->device);
+    PackedEngine::Scene sc;
+    sc.tag = tag;
+    sdr_solver_options o{};
+    o.max_particles = capacity;
+    o.device = e->device;
+    o.flags = SDR_SOLVER_SHARED_GPU;
+    g_engine_stream = e->st;
+    int rc = sdr_solver_create(&d.sdf, d.sim_dx, &d.fluid, &d.needle, &o, &sc.s);
+    g_engine_stream = nullptr;
+    if (rc == SDR_OK && d.has_outlet) rc = sdr_solver_set_outlet(sc.s, &d.outlet);
+    if (rc == SDR_OK) rc = sdr_solver_set_solve_params(sc.s, &d.solve);
+    if (rc == SDR_OK) rc = sdr_metrics_create(sc.s, d.cavity_volume, &sc.m);
+    if (rc != SDR_OK) {
+        e->finish(sc, rc, sdr_last_error(), done);
+        return rc;
+    }
+    sc.frame_dt = d.frame_dt;
+    sc.remaining = d.frame_dt;
+    sc.floor_ = d.frame_dt / 512.0;  // solver.rs:248-249
+    sc.frames = d.frames;
+    if (sc.frames == 0) {
+        e->finish(sc, SDR_OK, "", done);
+        return SDR_OK;
+    }
+    e->live.push_back(sc);
+    return SDR_OK;
+}
+
+size_t packed_engine_live(const PackedEngine* e) { return e->live.size(); }
+
+void packed_engine_step(PackedEngine* e, std::vector<PackedDone>& done) {
+    if (e->live.empty()) return;
+    DeviceScope ds(e->device);
+    std::vector<char> recorded(e->live.size(), 0);
+    std::vector<std::string> errs(e->live.size());
+    std::vector<int> codes(e->live.size(), SDR_OK);
+    // every live scene records one substep (Solver::step's choice of dt, solver.rs:252-256)
+    for (size_t q = 0; q < e->live.size(); ++q) {
+        auto& sc = e->live[q];
+        sc.sub = std::fmin(std::fmax(sc.s->cfl_dt(), sc.floor_), sc.remaining);
+        e->pk.begin_scene();
+        sc.s->pk = &e->pk;
+        try {
+            sc.s->substep_issue(sc.sub);
+            sc.s->status_issue();
+            recorded[q] = 1;
+        } catch (const Fail& f) {
+            e->pk.drop_scene();
+            codes[q] = f.code;
+            errs[q] = f.msg;
+        } catch (...) {
+            e->pk.drop_scene();
+            codes[q] = SDR_ERR_CUDA;
+            errs[q] = "substep recording failed";
+        }
+        sc.s->pk = nullptr;
+    }
+    int rc = SDR_OK;
+    std::string msg;
+    try {
+        const size_t nl = e->pk.flush(
+            e->st, e->grid_cap,
+            [&](size_t bytes) {
+                if (bytes > e->dev_cap) {
+                    dalloc(e->dev_arena, bytes + bytes / 2, e->st);
+                    e->dev_cap = bytes + bytes / 2;
+                }
+                return e->dev_arena;
+            },
+            [&](unsigned char* dev, const unsigned char* host, size_t bytes) {
+                if (bytes > e->host_cap) {
+                    CK(cudaStreamSynchronize(e->st));  // the old staging block may still be read
+                    if (e->host_arena) hput(e->host_arena, e->host_cap);
+                    hget(e->host_arena, bytes + bytes / 2, &e->host_cap);
+                }
+                std::memcpy(e->host_arena, host, bytes);
+                CK(cudaMemcpyAsync(dev, e->host_arena, bytes, cudaMemcpyHostToDevice, e->st));
+            });
+        e->launches += nl;
+        g_launches.fetch_add(nl, std::memory_order_relaxed);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(e->st));
+    } catch (const Fail& f) {
+        rc = f.code;
+        msg = f.msg;
+    }
+    e->steps += 1;
+    std::vector<PackedEngine::Scene> keep;
+    for (size_t q = 0; q < e->live.size(); ++q) {
+        auto& sc = e->live[q];
+        if (rc != SDR_OK) {
+            e->finish(sc, rc, msg, done);
+            continue;
+        }
+        if (!recorded[q]) {
+            e->finish(sc, codes[q], errs[q], done);
+            continue;
+        }
+        try {
+            sc.s->status_read();
+            sc.s->substep_finish(sc.sub);
+        } catch (const Fail& f) {
+            e->finish(sc, f.code, f.msg, done);
+            continue;
+        }
+        sc.remaining -= sc.sub;
+        sc.taken += 1;
+        if (sc.remaining > 1e-12) {
+            keep.push_back(sc);
+            continue;
+        }
+        // the frame is complete: Solver::step's bookkeeping, then MetricsCollector::record
+        sc.s->last_substeps = sc.taken;
+        sdr_frame_metrics fm;
+        const int mrc = sdr_metrics_record(sc.m, sc.s, sc.frame, &fm);
+        if (mrc != SDR_OK) {
+            e->finish(sc, mrc, sdr_last_error(), done);
+            continue;
+        }
+        sc.frame += 1;
+        sc.taken = 0;
+        sc.remaining = sc.frame_dt;
+        if (sc.frame >= sc.frames) e->finish(sc, SDR_OK, "", done);
+        else keep.push_back(sc);
+    }
+    e->live.swap(keep);
+}
+
+void packed_engine_counters(const PackedEngine* e, uint64_t* launches, uint64_t* steps) {
+    if (launches) *launches = e->launches;
+    if (steps) *steps = e->steps;
+}
+
+void packed_engine_destroy(PackedEngine* e) {
+    if (!e) return;
+    DeviceScope ds(e->device);
+    std::vector<PackedDone> done;
+    for (auto& sc : e->live) e->finish(sc, SDR_ERR_INVALID, "engine destroyed before the scene finished", done);
+    e->live.clear();
+    if (e->st) cudaStreamSynchronize(e->st);
+    dfree(e->dev_arena, e->st);
+    if (e->host_arena) hput(e->host_arena, e->host_cap);
+    if (e->st) {
+        cudaStreamSynchronize(e->st);
+        cudaStreamDestroy(e->st);
+    }
+    delete e;
+}

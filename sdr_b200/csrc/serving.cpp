@@ -26,6 +26,7 @@
 #include <thread>
 #include <vector>
 
+#include "packed_engine.h"
 #include "sdr_gpu.h"
 
 void sdr_internal_set_error(const std::string& msg);
@@ -153,6 +154,7 @@ struct sdr_batch {
     int32_t device = -1;
     std::vector<std::unique_ptr<SceneCopy>> scenes;
     std::vector<SceneResult> results;
+    uint64_t packed_launches = 0, packed_steps = 0;  // of the last packed run
 };
 
 struct Request {
@@ -180,6 +182,67 @@ struct sdr_server {
     sdr_server_stats stats{};
     std::thread dispatcher;
     std::vector<std::thread> workers;
+    bool packed = false;  // one engine thread advances every admitted scene in packed steps
+
+    // Packed mode: admit between packed steps, step every live scene together,
+    // hand finished scenes back. Requests that arrive while others run join at
+    // the next step, as slots and budget free up.
+    void engine_loop() {
+        PackedEngine* e = packed_engine_create(device);
+        std::vector<PackedDone> done;
+        std::unique_lock<std::mutex> lk(mu);
+        const std::string fail_msg = e ? "" : std::string("packed engine: ") + sdr_last_error();
+        for (;;) {
+            std::vector<Request*> start;
+            while (head_fits()) {
+                Request* r = pending.front();
+                pending.pop_front();
+                stats.bytes_in_use += r->bytes;
+                stats.peak_bytes = std::max(stats.peak_bytes, stats.bytes_in_use);
+                r->state = SDR_REQ_RUNNING;
+                stats.active += 1;
+                stats.peak_active = std::max(stats.peak_active, stats.active);
+                start.push_back(r);
+            }
+            const size_t live = e ? packed_engine_live(e) : 0;
+            if (start.empty() && live == 0) {
+                if (stopping && pending.empty()) break;
+                cv_admit.wait(lk, [&] { return (stopping && pending.empty()) || head_fits(); });
+                continue;
+            }
+            lk.unlock();
+            done.clear();
+            for (Request* r : start) {
+                if (e) {
+                    packed_engine_add(e, r->scene->d, particle_capacity(r->scene->d), r->id, done);
+                } else {
+                    PackedDone d;
+                    d.tag = r->id;
+                    d.status = SDR_ERR_CUDA;
+                    d.error = fail_msg;
+                    done.push_back(d);
+                }
+            }
+            if (e && packed_engine_live(e)) packed_engine_step(e, done);
+            lk.lock();
+            for (auto& d : done) {
+                Request* r = requests[d.tag].get();
+                r->result.status = d.status;
+                r->result.error = d.error;
+                r->result.summary = d.summary;
+                r->result.stats = d.stats;
+                r->latency = std::chrono::duration<double>(Clock::now() - r->submitted).count();
+                r->state = d.status == SDR_OK ? SDR_REQ_DONE : SDR_REQ_FAILED;
+                r->scene.reset();
+                stats.active -= 1;
+                stats.bytes_in_use -= r->bytes;
+                if (r->state == SDR_REQ_DONE) stats.completed += 1;
+                else stats.failed += 1;
+            }
+        }
+        lk.unlock();
+        packed_engine_destroy(e);
+    }
 
     // Admit from the head of the queue while the head fits (arrival order: a
     // large request at the head is not overtaken by smaller ones behind it).
@@ -279,6 +342,43 @@ int sdr_batch_run(sdr_batch* b, uint32_t concurrency) {
     return SDR_OK;
 }
 
+int sdr_batch_run_packed(sdr_batch* b) {
+    if (!b) return invalid("null batch");
+    PackedEngine* e = packed_engine_create(b->device);
+    if (!e) return SDR_ERR_CUDA;
+    const auto t0 = Clock::now();
+    std::vector<PackedDone> done;
+    auto take = [&] {
+        const double t = std::chrono::duration<double>(Clock::now() - t0).count();
+        for (auto& d : done) {
+            SceneResult& r = b->results[d.tag];
+            r.status = d.status;
+            r.error = d.error;
+            r.summary = d.summary;
+            r.stats = d.stats;
+            r.seconds = t;
+        }
+        done.clear();
+    };
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        packed_engine_add(e, b->scenes[i]->d, particle_capacity(b->scenes[i]->d), i, done);
+    take();
+    while (packed_engine_live(e)) {
+        packed_engine_step(e, done);
+        take();
+    }
+    packed_engine_counters(e, &b->packed_launches, &b->packed_steps);
+    packed_engine_destroy(e);
+    return SDR_OK;
+}
+
+int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps) {
+    if (!b || !launches || !steps) return invalid("null argument");
+    *launches = b->packed_launches;
+    *steps = b->packed_steps;
+    return SDR_OK;
+}
+
 int sdr_batch_result(const sdr_batch* b, size_t i, int32_t* status, sdr_summary* summary,
                      sdr_solver_stats* stats_or_null, double* seconds_or_null, char* error, size_t error_cap) {
     if (!b || !status || !summary) return invalid("null argument");
@@ -308,6 +408,25 @@ int sdr_server_create(int32_t device, uint64_t budget_bytes, uint32_t max_active
         s->max_active = max_active;
         s->dispatcher = std::thread([p = s.get()] { p->dispatch_loop(); });
         for (uint32_t i = 0; i < max_active; ++i) s->workers.emplace_back([p = s.get()] { p->worker_loop(); });
+        *out = s.release();
+        return SDR_OK;
+    } catch (const std::exception& e) {
+        sdr_internal_set_error(std::string("server start failed: ") + e.what());
+        return SDR_ERR_INVALID;
+    }
+}
+
+int sdr_server_create_packed(int32_t device, uint64_t budget_bytes, uint32_t max_active, sdr_server** out) {
+    if (!out) return invalid("null argument");
+    if (budget_bytes == 0 || max_active == 0) return invalid("budget and max_active must be positive");
+    *out = nullptr;
+    try {
+        auto s = std::make_unique<sdr_server>();
+        s->device = device;
+        s->budget = budget_bytes;
+        s->max_active = max_active;
+        s->packed = true;
+        s->dispatcher = std::thread([p = s.get()] { p->engine_loop(); });
         *out = s.release();
         return SDR_OK;
     } catch (const std::exception& e) {

@@ -77,16 +77,26 @@ class SceneResult:
     error: str
 
 
-def run_batch(specs: Sequence[SceneSpec], concurrency: int = 0, device: int = -1) -> List[SceneResult]:
+def run_batch(specs: Sequence[SceneSpec], concurrency: int = 0, device: int = -1, packed: bool = False,
+              counters: Optional[dict] = None) -> List[SceneResult]:
     """Run every scene to its frame count, ``concurrency`` at a time (0 = all,
-    1 = one after another); results in input order."""
+    1 = one after another), or all packed into one launch per substep
+    operation (``packed``, sdr_batch_run_packed); results in input order.
+    ``counters`` receives the packed run's launches and packed steps."""
     L = _lib.load()
     descs = [_Desc(s) for s in specs]
     arr = (_lib.SceneDesc * len(descs))(*[d.c for d in descs])
     h = C.c_void_p()
     check(L.sdr_batch_create(arr, len(descs), int(device), C.byref(h)))
     try:
-        check(L.sdr_batch_run(h, int(concurrency)))
+        if packed:
+            check(L.sdr_batch_run_packed(h))
+            if counters is not None:
+                la, stp = C.c_uint64(), C.c_uint64()
+                check(L.sdr_batch_packed_counters(h, C.byref(la), C.byref(stp)))
+                counters.update(launches=la.value, steps=stp.value)
+        else:
+            check(L.sdr_batch_run(h, int(concurrency)))
         out = []
         for i in range(len(descs)):
             st = C.c_int32()
@@ -108,10 +118,11 @@ class Server:
     """Continuous batching: scenes submitted at any time run as soon as their
     footprint fits ``budget_bytes`` and one of ``max_active`` slots is free."""
 
-    def __init__(self, budget_bytes: int, max_active: int, device: int = -1):
+    def __init__(self, budget_bytes: int, max_active: int, device: int = -1, packed: bool = False):
         self._L = _lib.load()
         h = C.c_void_p()
-        check(self._L.sdr_server_create(int(device), int(budget_bytes), int(max_active), C.byref(h)))
+        create = self._L.sdr_server_create_packed if packed else self._L.sdr_server_create
+        check(create(int(device), int(budget_bytes), int(max_active), C.byref(h)))
         self._h = h
         self._keep = {}
 

@@ -115,3 +115,47 @@ def test_metrics_outlive_solver_and_growth_matches_preallocated():
     big, n_big = run(1 << 20)
     assert n_small > 4 * 256 and n_small == n_big
     _same(small, big)
+
+
+def test_packed_batch_one_launch_per_operation_same_results():
+    """sdr_batch_run_packed: every packed step advances all live scenes by one
+    substep with one launch per substep operation (ragged offset table,
+    persistent grid). The scenes - uneven flows and so uneven particle counts,
+    substep counts and PCG iterations - give the same summaries, stats and
+    particle counts bit for bit as one after another on their own solvers, and
+    the launches are those of the busiest scene, not of all scenes."""
+    specs = _specs(flows=(2.0, 4.0, 6.0, 8.0), frames=3)
+    seq = run_batch(specs, concurrency=1)
+    cnt = {}
+    packed = run_batch(specs, packed=True, counters=cnt)
+    assert all(r.status == _lib.SDR_OK for r in seq + packed), [r.error for r in seq + packed]
+    for a, b in zip(seq, packed):
+        _same(a.summary, b.summary)
+        for k in ("particles", "steps", "drained", "emitted", "culled", "particle_substeps", "last_pcg_iters"):
+            assert a.stats[k] == b.stats[k], (k, a.stats[k], b.stats[k])
+    subs = [r.stats["substeps_total"] for r in seq]
+    assert cnt["steps"] == max(subs)
+    per_step = cnt["launches"] / cnt["steps"]
+    record("packed_batch", {"counters": cnt, "launches_per_packed_step": per_step, "substeps": subs,
+                            "seconds_sequential": sum(r.seconds for r in seq),
+                            "seconds_packed": max(r.seconds for r in packed)})
+    assert per_step < 90  # one launch per operation, whatever the number of scenes
+
+
+def test_packed_server_continuous_batching_matches_batch():
+    """The request loop with one packed engine: requests that arrive while
+    others run join the packed steps as slots free up; each result equals its
+    scene run alone."""
+    specs = _specs(flows=(2.0, 3.0, 4.0, 5.0, 6.0))
+    ref = run_batch(specs, concurrency=1)
+    with Server(budget_bytes=64 << 30, max_active=3, packed=True) as srv:
+        tickets = [srv.submit(s) for s in specs[:2]]
+        more = [srv.submit(s) for s in specs[2:]]
+        res = srv.wait(tickets + more, timeout=600)
+        st = srv.stats()
+    assert all(r.status == _lib.REQ_DONE for r in res), [r.error for r in res]
+    for a, b in zip(ref, res):
+        _same(a.summary, b.summary)
+    assert st["completed"] == 5 and st["failed"] == 0 and 1 <= st["peak_active"] <= 3
+    assert st["active"] == 0 and st["bytes_in_use"] == 0
+    record("packed_server", {"stats": st, "time_to_summary": [r.seconds for r in res]})
