@@ -499,8 +499,16 @@ int sdr_batch_run(sdr_batch* b, uint32_t concurrency);
  * (sdr_batch_result's seconds) run from the start of the call to the scene's
  * last frame. */
 int sdr_batch_run_packed(sdr_batch* b);
-/* Launches and packed steps of the last sdr_batch_run_packed. */
-int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps);
+/* Of the last sdr_batch_run_packed: kernel launches, packed steps, CUDA-graph
+ * captures (a packed step is captured as one graph and replayed while its
+ * launch plan - the operations, the scenes in each and their grid sizes,
+ * rounded up to powers of two - is unchanged) and the CTAs per SM the
+ * autotuner chose for the persistent grids (it times 2, 4, 8 and 16 CTAs per
+ * SM over the first packed steps and keeps the fastest by particle-substeps
+ * per second; 0 if the run was too short to finish tuning). Either of the last
+ * two may be NULL. */
+int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps, uint64_t* graph_captures,
+                              int32_t* ctas_per_sm);
 /* status: SDR_OK or the scene's error code (message in `error`, may be NULL). */
 int sdr_batch_result(const sdr_batch* b, size_t i, int32_t* status, sdr_summary* summary,
                      sdr_solver_stats* stats_or_null, double* seconds_or_null, char* error, size_t error_cap);

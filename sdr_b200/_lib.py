@@ -227,7 +227,7 @@ SIGNATURES = {
     "sdr_batch_result": (i32, [vp, sz, P(C.c_int32), P(SummaryC), P(SolverStats), P(d), C.c_char_p, sz]),
     "sdr_batch_destroy": (i32, [vp]),
     "sdr_batch_run_packed": (i32, [vp]),
-    "sdr_batch_packed_counters": (i32, [vp, P(u64), P(u64)]),
+    "sdr_batch_packed_counters": (i32, [vp, P(u64), P(u64), P(u64), P(C.c_int32)]),
     "sdr_server_create_packed": (i32, [C.c_int32, u64, C.c_uint32, P(vp)]),
     "sdr_server_create": (i32, [C.c_int32, u64, C.c_uint32, P(vp)]),
     "sdr_server_submit": (i32, [vp, P(SceneDesc), P(u64)]),

@@ -103,20 +103,36 @@ SDR_OP(k_pack_copy, 256)
 using PackLaunch = void (*)(const unsigned char* dev_hdr, unsigned grid, unsigned block, size_t smem,
                             cudaStream_t st);
 
+using PackPrep = cudaError_t (*)(size_t smem);
+
 template <class Op, class Tup>
 void pack_launch(const unsigned char* dev_hdr, unsigned grid, unsigned block, size_t smem, cudaStream_t st) {
-    static bool attr = false;  // dynamic shared memory above the 48 KiB default, set once per instantiation
-    if (smem > 48 * 1024 && !attr) {
-        cudaFuncSetAttribute(k_packed<Op, Tup>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
     k_packed<Op, Tup><<<grid, block, smem, st>>>(dev_hdr);
 }
+// Dynamic shared memory above the 48 KiB default (set before any capture).
+template <class Op, class Tup>
+cudaError_t pack_prep(size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(k_packed<Op, Tup>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// One launch of a packed step: its kernel, table (offset into the arena) and shape.
+struct PackStep {
+    PackLaunch fn;
+    PackPrep prep;
+    size_t hdr_at;
+    unsigned grid, threads;
+    size_t smem;
+    bool operator==(const PackStep& o) const {
+        return fn == o.fn && hdr_at == o.hdr_at && grid == o.grid && threads == o.threads && smem == o.smem;
+    }
+};
 
 // One recorded operation of one scene.
 struct PackEntry {
     int line, occ;        // call site and its repetition within the substep
     PackLaunch fn;        // the slot's batched kernel
+    PackPrep prep;
     unsigned blocks, threads;
     size_t smem, align;
     std::vector<unsigned char> args;  // the argument tuple's bytes
@@ -139,6 +155,7 @@ class Packer {
         e.line = line;
         e.occ = occ_[line]++;
         e.fn = &pack_launch<Op, Tup>;
+        e.prep = &pack_prep<Op, Tup>;
         e.blocks = blocks;
         e.threads = threads;
         e.smem = smem;
@@ -148,11 +165,12 @@ class Packer {
         scenes_.back().push_back(std::move(e));
     }
 
-    // Lay out every slot's table, copy the arena to the device and launch the
-    // slots in order. grid_cap: the largest grid of one slot (persistent CTAs).
-    // Returns the number of launches.
-    template <class Alloc, class Upload>
-    size_t flush(cudaStream_t st, unsigned grid_cap, Alloc&& device_arena, Upload&& upload) {
+    // Lay out every slot's table in the host arena and plan the launches,
+    // one per slot, in order: grid = the slot's virtual blocks rounded up to a
+    // power of two, at most grid_cap (the CTAs then walk the virtual blocks),
+    // so the plan - and a graph captured from it - stays the same while the
+    // scenes' work changes within those buckets. Clears the recordings.
+    const std::vector<unsigned char>& build(unsigned grid_cap, std::vector<PackStep>& plan) {
         // slots: the union of the scenes' (line, occ) keys, each scene's order kept
         std::vector<std::pair<int, int>> order;
         std::map<std::pair<int, int>, size_t> where;
@@ -176,51 +194,41 @@ class Packer {
         for (auto& sc : scenes_)
             for (auto& e : sc) slot[where[std::make_pair(e.line, e.occ)]].push_back(&e);
         host_.clear();
-        std::vector<size_t> hdr_at(order.size());
+        plan.clear();
         for (size_t q = 0; q < order.size(); ++q) {
             const auto& es = slot[q];
             align(256);
-            hdr_at[q] = host_.size();
+            const size_t hdr_at = host_.size();
             PackHdr h{};
             h.ns = (uint32_t)es.size();
             host_.resize(host_.size() + sizeof(PackHdr));
-            h.off_at = (uint32_t)(host_.size() - hdr_at[q]);
+            h.off_at = (uint32_t)(host_.size() - hdr_at);
             uint32_t tot = 0;
+            unsigned threads = 0;
+            size_t smem = 0;
             for (auto* e : es) {
                 push_u32(tot);
                 tot += e->blocks;
+                threads = std::max(threads, e->threads);
+                smem = std::max(smem, e->smem);
             }
             push_u32(tot);
             h.total = tot;
             align(16);
-            h.args_at = (uint32_t)(host_.size() - hdr_at[q]);
+            h.args_at = (uint32_t)(host_.size() - hdr_at);
             h.stride = (uint32_t)((es[0]->args.size() + 15) & ~(size_t)15);
             for (auto* e : es) {
                 const size_t at = host_.size();
                 host_.resize(at + h.stride, 0);
                 std::memcpy(host_.data() + at, e->args.data(), e->args.size());
             }
-            std::memcpy(host_.data() + hdr_at[q], &h, sizeof(h));
-        }
-        unsigned char* dev = device_arena(host_.size());
-        upload(dev, host_.data(), host_.size());
-        size_t launches = 0;
-        for (size_t q = 0; q < order.size(); ++q) {
-            const auto& es = slot[q];
-            uint32_t tot = 0;
-            unsigned threads = 0;
-            size_t smem = 0;
-            for (auto* e : es) {
-                tot += e->blocks;
-                threads = std::max(threads, e->threads);
-                smem = std::max(smem, e->smem);
-            }
-            if (!tot) continue;
-            es[0]->fn(dev + hdr_at[q], std::min<unsigned>(tot, grid_cap), threads, smem, st);
-            ++launches;
+            std::memcpy(host_.data() + hdr_at, &h, sizeof(h));
+            unsigned grid = 1;
+            while (grid < tot && grid < grid_cap) grid <<= 1;
+            plan.push_back(PackStep{es[0]->fn, es[0]->prep, hdr_at, std::min(grid, grid_cap), threads, smem});
         }
         scenes_.clear();
-        return launches;
+        return host_;
     }
 
     // The last scene's recording is abandoned (it failed part way).

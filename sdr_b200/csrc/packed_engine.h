@@ -29,5 +29,8 @@ size_t packed_engine_live(const PackedEngine* e);
 // One substep of every live scene, one launch per substep operation for all of
 // them; scenes that completed their last frame (or failed) go to `done`.
 void packed_engine_step(PackedEngine* e, std::vector<PackedDone>& done);
-void packed_engine_counters(const PackedEngine* e, uint64_t* launches, uint64_t* steps);
+// Launches, packed steps, graph captures and the autotuned CTAs per SM (0
+// while still tuning).
+void packed_engine_counters(const PackedEngine* e, uint64_t* launches, uint64_t* steps, uint64_t* captures,
+                            int* ctas_per_sm);
 void packed_engine_destroy(PackedEngine* e);

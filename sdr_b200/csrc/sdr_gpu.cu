@@ -2408,7 +2408,52 @@ struct PackedEngine {
     size_t dev_cap = 0;
     unsigned char* host_arena = nullptr;  // pinned
     size_t host_cap = 0;
-    uint64_t launches = 0, steps = 0;
+    uint64_t launches = 0, steps = 0, captures = 0;
+    // the packed step as a CUDA graph, replayed while its launch plan is unchanged
+    std::vector<PackStep> plan, graph_plan;
+    const unsigned char* graph_arena = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    // autotuner of the persistent grid cap: candidate CTAs per SM, each timed
+    // over kTuneSteps packed steps (CUDA events), then the fastest kept
+    int nsm = 0;
+    static constexpr int kTuneCaps[4] = {2, 4, 8, 16};
+    static constexpr int kTuneSteps = 3;
+    int tune = 0;                 // candidate under test (4: done)
+    int tune_n = 0;               // its steps so far
+    double tune_ms[4] = {0, 0, 0, 0};
+    double tune_work[4] = {0, 0, 0, 0};  // particle-substeps of those steps
+    int chosen = 8;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    unsigned cap() const { return (unsigned)nsm * (unsigned)(tune < 4 ? kTuneCaps[tune] : chosen); }
+
+    // One packed step's launches: the graph captured from the same plan and
+    // arena if there is one, else a new capture.
+    void launch(const unsigned char* dev) {
+        if (!(gexec && dev == graph_arena && plan == graph_plan)) {
+            for (auto& p : plan) CK(p.prep(p.smem));
+            if (gexec) cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            for (auto& p : plan) p.fn(dev + p.hdr_at, p.grid, p.threads, p.smem, st);
+            const cudaError_t le = cudaGetLastError();
+            CK(cudaStreamEndCapture(st, &graph));
+            if (le != cudaSuccess) {
+                cudaGraphDestroy(graph);
+                throw Fail{SDR_ERR_CUDA, std::string("packed launch: ") + cudaGetErrorString(le)};
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(ie);
+            graph_plan = plan;
+            graph_arena = dev;
+            captures += 1;
+        }
+        CK(cudaGraphLaunch(gexec, st));
+        launches += plan.size();
+        g_launches.fetch_add(plan.size(), std::memory_order_relaxed);
+    }
 
     void finish(Scene& sc, int status, const std::string& err, std::vector<PackedDone>& done) {
         PackedDone d;
@@ -2438,7 +2483,9 @@ PackedEngine* packed_engine_create(int32_t device) {
         CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
         int nsm = 0;
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
-        e->grid_cap = (unsigned)nsm * 16;  // persistent CTAs per packed launch
+        e->nsm = nsm;
+        CK(cudaEventCreate(&e->ev0));
+        CK(cudaEventCreate(&e->ev1));
     } catch (const Fail& f) {
         if (e->st) cudaStreamDestroy(e->st);
         delete e;
@@ -2510,32 +2557,55 @@ void packed_engine_step(PackedEngine* e, std::vector<PackedDone>& done) {
     }
     int rc = SDR_OK;
     std::string msg;
+    uint64_t work = 0;  // particle-substeps of this packed step (the autotuner's unit of work)
+    for (size_t q = 0; q < e->live.size(); ++q)
+        if (recorded[q]) work += e->live[q].s->pending_n_before + 1;
     try {
-        const size_t nl = e->pk.flush(
-            e->st, e->grid_cap,
-            [&](size_t bytes) {
-                if (bytes > e->dev_cap) {
-                    dalloc(e->dev_arena, bytes + bytes / 2, e->st);
-                    e->dev_cap = bytes + bytes / 2;
-                }
-                return e->dev_arena;
-            },
-            [&](unsigned char* dev, const unsigned char* host, size_t bytes) {
-                if (bytes > e->host_cap) {
-                    CK(cudaStreamSynchronize(e->st));  // the old staging block may still be read
-                    if (e->host_arena) hput(e->host_arena, e->host_cap);
-                    hget(e->host_arena, bytes + bytes / 2, &e->host_cap);
-                }
-                std::memcpy(e->host_arena, host, bytes);
-                CK(cudaMemcpyAsync(dev, e->host_arena, bytes, cudaMemcpyHostToDevice, e->st));
-            });
-        e->launches += nl;
-        g_launches.fetch_add(nl, std::memory_order_relaxed);
-        CK(cudaGetLastError());
+        const std::vector<unsigned char>& host = e->pk.build(e->cap(), e->plan);
+        const size_t bytes = host.size();
+        if (bytes > e->dev_cap) {
+            dalloc(e->dev_arena, bytes + bytes / 2, e->st);
+            e->dev_cap = bytes + bytes / 2;
+        }
+        if (bytes > e->host_cap) {
+            CK(cudaStreamSynchronize(e->st));  // the old staging block may still be read
+            if (e->host_arena) hput(e->host_arena, e->host_cap);
+            e->host_cap = 0;
+            hget(e->host_arena, bytes + bytes / 2, &e->host_cap);
+        }
+        std::memcpy(e->host_arena, host.data(), bytes);
+        CK(cudaMemcpyAsync(e->dev_arena, e->host_arena, bytes, cudaMemcpyHostToDevice, e->st));
+        CK(cudaEventRecord(e->ev0, e->st));
+        e->launch(e->dev_arena);
+        CK(cudaEventRecord(e->ev1, e->st));
         CK(cudaStreamSynchronize(e->st));
+        if (e->tune < 4) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+            if (e->tune_n > 0) {  // the first step of a candidate pays its capture
+                e->tune_ms[e->tune] += ms;
+                e->tune_work[e->tune] += (double)work;
+            }
+            if (++e->tune_n > PackedEngine::kTuneSteps) {
+                e->tune_n = 0;
+                if (++e->tune == 4) {
+                    int best = 2;
+                    double best_rate = -1.0;
+                    for (int c = 0; c < 4; ++c) {
+                        const double rate = e->tune_ms[c] > 0 ? e->tune_work[c] / e->tune_ms[c] : 0.0;
+                        if (rate > best_rate) {
+                            best_rate = rate;
+                            best = c;
+                        }
+                    }
+                    e->chosen = PackedEngine::kTuneCaps[best];
+                }
+            }
+        }
     } catch (const Fail& f) {
         rc = f.code;
         msg = f.msg;
+        cudaStreamSynchronize(e->st);
     }
     e->steps += 1;
     std::vector<PackedEngine::Scene> keep;
@@ -2579,9 +2649,12 @@ void packed_engine_step(PackedEngine* e, std::vector<PackedDone>& done) {
     e->live.swap(keep);
 }
 
-void packed_engine_counters(const PackedEngine* e, uint64_t* launches, uint64_t* steps) {
+void packed_engine_counters(const PackedEngine* e, uint64_t* launches, uint64_t* steps, uint64_t* captures,
+                            int* ctas_per_sm) {
     if (launches) *launches = e->launches;
     if (steps) *steps = e->steps;
+    if (captures) *captures = e->captures;
+    if (ctas_per_sm) *ctas_per_sm = e->tune < 4 ? 0 : e->chosen;
 }
 
 void packed_engine_destroy(PackedEngine* e) {
@@ -2591,6 +2664,9 @@ void packed_engine_destroy(PackedEngine* e) {
     for (auto& sc : e->live) e->finish(sc, SDR_ERR_INVALID, "engine destroyed before the scene finished", done);
     e->live.clear();
     if (e->st) cudaStreamSynchronize(e->st);
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
     dfree(e->dev_arena, e->st);
     if (e->host_arena) hput(e->host_arena, e->host_cap);
     if (e->st) {

@@ -154,7 +154,8 @@ struct sdr_batch {
     int32_t device = -1;
     std::vector<std::unique_ptr<SceneCopy>> scenes;
     std::vector<SceneResult> results;
-    uint64_t packed_launches = 0, packed_steps = 0;  // of the last packed run
+    uint64_t packed_launches = 0, packed_steps = 0, packed_captures = 0;  // of the last packed run
+    int packed_ctas = 0;
 };
 
 struct Request {
@@ -367,15 +368,18 @@ int sdr_batch_run_packed(sdr_batch* b) {
         packed_engine_step(e, done);
         take();
     }
-    packed_engine_counters(e, &b->packed_launches, &b->packed_steps);
+    packed_engine_counters(e, &b->packed_launches, &b->packed_steps, &b->packed_captures, &b->packed_ctas);
     packed_engine_destroy(e);
     return SDR_OK;
 }
 
-int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps) {
+int sdr_batch_packed_counters(const sdr_batch* b, uint64_t* launches, uint64_t* steps, uint64_t* graph_captures,
+                              int32_t* ctas_per_sm) {
     if (!b || !launches || !steps) return invalid("null argument");
     *launches = b->packed_launches;
     *steps = b->packed_steps;
+    if (graph_captures) *graph_captures = b->packed_captures;
+    if (ctas_per_sm) *ctas_per_sm = b->packed_ctas;
     return SDR_OK;
 }
 

@@ -92,9 +92,10 @@ def run_batch(specs: Sequence[SceneSpec], concurrency: int = 0, device: int = -1
         if packed:
             check(L.sdr_batch_run_packed(h))
             if counters is not None:
-                la, stp = C.c_uint64(), C.c_uint64()
-                check(L.sdr_batch_packed_counters(h, C.byref(la), C.byref(stp)))
-                counters.update(launches=la.value, steps=stp.value)
+                la, stp, cap, ctas = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_int32()
+                check(L.sdr_batch_packed_counters(h, C.byref(la), C.byref(stp), C.byref(cap), C.byref(ctas)))
+                counters.update(launches=la.value, steps=stp.value, graph_captures=cap.value,
+                                ctas_per_sm=ctas.value)
         else:
             check(L.sdr_batch_run(h, int(concurrency)))
         out = []

@@ -140,6 +140,7 @@ def test_packed_batch_one_launch_per_operation_same_results():
                             "seconds_sequential": sum(r.seconds for r in seq),
                             "seconds_packed": max(r.seconds for r in packed)})
     assert per_step < 90  # one launch per operation, whatever the number of scenes
+    assert cnt["graph_captures"] < cnt["steps"] / 4  # the packed step's graph is replayed
 
 
 def test_packed_server_continuous_batching_matches_batch():
