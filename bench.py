@@ -396,13 +396,36 @@ def frame_record(w, key: str, cpu: bool, cpu_budget: float):
     return {key: out}, solver, sdf
 
 
-def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
-    """Plain (one scene after another, default solvers), batched and served runs of the same scenes."""
-    import math
+def _serve(specs, rate: float, seed: int, packed: bool) -> tuple:
+    """Poisson arrivals at `rate` into the request server; (results, seconds, stats)."""
     import random
 
+    from sdr_b200.serving import Server
+    rng = random.Random(seed)
+    with Server(budget_bytes=150 << 30, max_active=len(specs), packed=packed) as srv:
+        t0 = time.perf_counter()
+        tickets, t_next = [], 0.0
+        for sp in specs:
+            t_next += rng.expovariate(rate)
+            delay = t0 + t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(sp))
+        res = srv.wait(tickets, timeout=3600)
+        t_srv = time.perf_counter() - t0
+        sst = srv.stats()
+    return res, t_srv, sst
+
+
+def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
+    """The same scenes one after another on default solvers (the plain path),
+    concurrently on one stream and solver each (sdr_batch_run), packed into one
+    launch per substep operation (sdr_batch_run_packed), and served: Poisson
+    arrivals into the request server, stream-per-scene and packed."""
+    import math
+
     from sdr_b200 import _lib, workloads
-    from sdr_b200.serving import Server, run_batch
+    from sdr_b200.serving import run_batch
     t0 = time.perf_counter()
     specs = []
     for i in range(n_scenes):
@@ -417,41 +440,42 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
     t0 = time.perf_counter()
     mix = run_batch(specs, concurrency=0)
     t_mix = time.perf_counter() - t0
-    ok = all(r.status == _lib.SDR_OK for r in plain + mix)
-    same = ok and all(a.summary == b.summary for a, b in zip(plain, mix))
-    ps = sum(r.stats["particle_substeps"] for r in mix) if ok else 0
-    subs = sum(r.stats["substeps_total"] for r in mix) if ok else 0
-    rate = 0.8 * n_scenes / t_mix  # arrivals at 80 % of the batched throughput
-    rng = random.Random(seed0)
-    with Server(budget_bytes=150 << 30, max_active=n_scenes) as srv:
-        t0 = time.perf_counter()
-        tickets, t_next = [], 0.0
-        for sp in specs:
-            t_next += rng.expovariate(rate)
-            delay = t0 + t_next - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            tickets.append(srv.submit(sp))
-        res = srv.wait(tickets, timeout=3600)
-        t_srv = time.perf_counter() - t0
-        sst = srv.stats()
-    lat = sorted(r.seconds for r in res)
-    served_same = ok and all(r.summary == b.summary for r, b in zip(res, mix))
+    cnt = {}
+    t0 = time.perf_counter()
+    packed = run_batch(specs, packed=True, counters=cnt)
+    t_packed = time.perf_counter() - t0
+    ok = all(r.status == _lib.SDR_OK for r in plain + mix + packed)
+    same = ok and all(a.summary == b.summary == c.summary for a, b, c in zip(plain, mix, packed))
+    ps = sum(r.stats["particle_substeps"] for r in packed) if ok else 0
+    subs = sum(r.stats["substeps_total"] for r in packed) if ok else 0
+    best = min(t_mix, t_packed)
+    rate = 0.8 * n_scenes / best  # arrivals at 80 % of the better batched throughput
 
-    def pct(q):
-        return lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+    def served(packed_mode: bool) -> dict:
+        res, t_srv, sst = _serve(specs, rate, seed0, packed_mode)
+        lat = sorted(r.seconds for r in res)
+
+        def pct(q):
+            return lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+        return {"mode": "packed engine" if packed_mode else "one stream and host thread per scene",
+                "arrivals": "poisson", "rate_per_s": rate, "scenes_per_s": n_scenes / t_srv,
+                "p50_time_to_summary_s": pct(0.5), "p99_time_to_summary_s": pct(0.99),
+                "peak_active": sst["peak_active"], "peak_bytes": sst["peak_bytes"], "budget_bytes": 150 << 30,
+                "results_identical": ok and all(r.summary == b.summary for r, b in zip(res, plain))}
     sample = (f"{n_scenes} scenes of the batched family (seeds {seed0}..{seed0 + n_scenes - 1}), each one frame "
               f"of {cfl_steps} jet-CFL steps from t = 0; SDFs built on the device in {build_s:.1f} s")
     return {
         "batched": {"scenes": n_scenes, "cfl_steps_per_scene": cfl_steps, "sample": sample,
-                    "plain_scenes_per_s": n_scenes / t_plain, "batched_scenes_per_s": n_scenes / t_mix,
-                    "speedup": t_plain / t_mix, "plain_s": t_plain, "batched_s": t_mix,
-                    "plain_solver": "default (sdr_solver_create flags 0)",
-                    "particle_substeps_per_s": ps / t_mix, "substeps": subs, "results_identical": same},
-        "served": {"arrivals": "poisson", "rate_per_s": rate, "scenes_per_s": n_scenes / t_srv,
-                   "p50_time_to_summary_s": pct(0.5), "p99_time_to_summary_s": pct(0.99),
-                   "peak_active": sst["peak_active"], "peak_bytes": sst["peak_bytes"],
-                   "budget_bytes": 150 << 30, "results_identical": served_same},
+                    "plain_scenes_per_s": n_scenes / t_plain, "plain_s": t_plain,
+                    "plain_solver": "default (sdr_solver_create flags 0), one scene after another",
+                    "streams_scenes_per_s": n_scenes / t_mix, "streams_s": t_mix,
+                    "packed_scenes_per_s": n_scenes / t_packed, "packed_s": t_packed,
+                    "packed_counters": cnt,
+                    "speedup_streams": t_plain / t_mix, "speedup_packed": t_plain / t_packed,
+                    "particle_substeps_per_s_packed": ps / t_packed, "substeps": subs,
+                    "results_identical": same},
+        "served": served(False),
+        "served_packed": served(True),
     }
 
 
