@@ -7,7 +7,13 @@ README figures (uselessgoddess/sdr README.md:58-61 and 146-151):
                                peak membrane 1099.3 mmHg (146558 Pa),
                                mean membrane 3.3 mmHg (436 Pa), drained 8.11 ml of 10.0
   examples/maxillary_real.toml fill 44.9 %, 92 % of fluid in the lower half (along gravity)
-Usage: python tests/golden/make_readme_pins.py [scene|maxillary] [threads]
+Usage: python tests/golden/make_readme_pins.py [scene|maxillary] [threads] [variant]
+
+variant (optional) reruns the scene perturbed, to measure how far its chaotic
+summary moves on its own: "f32" rounds the particle state to f32 after every
+substep (the device's storage precision), "seed" starts the emission stream
+from another seed (0x9e3779b97f4a7c15). The result goes to the scene's
+"variants" entry.
 """
 import json
 import os
@@ -26,7 +32,10 @@ from tests.helpers import cavity_volume, oracle_sdf, oracle_solver  # noqa: E402
 REF = os.environ.get("SDR_REFERENCE")
 
 
-def run(name: str, threads: int):
+VARIANT_SEED = 0x9E3779B97F4A7C15
+
+
+def run(name: str, threads: int, variant: str = ""):
     if not REF:
         raise SystemExit("set SDR_REFERENCE to the reference checkout (the directory holding examples/)")
     oracle.set_threads(threads)
@@ -41,11 +50,24 @@ def run(name: str, threads: int):
     s = oracle_solver(res, sdf)
     vol = cavity_volume(res, tris)
     m = oracle.Metrics(s, vol)
+    if variant == "seed":
+        sc0 = s.scalars()
+        s.set_scalars(sc0["time"], sc0["emit_accum"], sc0["steps"], sc0["drained"], VARIANT_SEED)
     frames = []
     for f in range(res.frames):
-        s.step(res.frame_dt)
+        if variant == "f32":  # Solver::step (solver.rs:237-259) with the state rounded after every substep
+            remaining, floor, taken = res.frame_dt, res.frame_dt / 512, 0
+            while remaining > 1e-12:
+                sub = min(max(s.cfl_dt(), floor), remaining)
+                s.substep(sub)
+                p, v = s.particles()
+                s.set_particles(p.astype(np.float32).astype(np.float64), v.astype(np.float32).astype(np.float64))
+                remaining -= sub
+                taken += 1
+        else:
+            s.step(res.frame_dt)
         r = m.record(s, f)
-        r["substeps"] = s.scalars()["last_substeps"]
+        r["substeps"] = s.scalars()["last_substeps"] if variant != "f32" else taken
         frames.append(r)
         print(name, f, r["time_s"], r["particles"], r["fill_fraction"], r["pcg_iters"], r["substeps"],
               f"{time.time() - t0:.0f}s", flush=True)
@@ -71,10 +93,15 @@ def run(name: str, threads: int):
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "scene"
     threads = int(sys.argv[2]) if len(sys.argv) > 2 else 4
-    res = run(which, threads)
+    variant = sys.argv[3] if len(sys.argv) > 3 else ""
+    res = run(which, threads, variant)
     dst = os.path.join(HERE, "readme_pins.json")
     data = json.load(open(dst)) if os.path.exists(dst) else {}
-    data[which] = res
+    if variant:
+        data[which].setdefault("variants", {})[variant] = {"summary": res["summary"],
+                                                           "wall_seconds": res["wall_seconds"]}
+    else:
+        data[which] = res
     with open(dst, "w") as f:
         json.dump(data, f, indent=1)
     print(json.dumps(res["summary"], indent=1))
