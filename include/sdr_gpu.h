@@ -155,6 +155,7 @@ typedef struct {
     uint64_t h2d_bytes;
     uint64_t d2h_bytes;
     uint64_t pcg_tile_launches; /* solves that ran on the whole-GPU tiled kernel */
+    uint64_t redist_rounds;     /* decision rounds of long redistribution lists */
 } sdr_profile;
 
 /* FrameMetrics, src/metrics.rs:28-65 (counts as u64). */

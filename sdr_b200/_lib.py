@@ -84,7 +84,8 @@ class Profile(C.Structure):
                 ("particles", C.c_uint64), ("pcg_section_cycles", C.c_uint64 * 16),
                 ("redist_candidates", C.c_uint64), ("redist_sweeps", C.c_uint64),
                 ("redist_long_sweeps", C.c_uint64), ("pcg_cluster_launches", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("pcg_tile_launches", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("pcg_tile_launches", C.c_uint64),
+                ("redist_rounds", C.c_uint64)]
 
     def to_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}

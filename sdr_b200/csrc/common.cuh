@@ -16,6 +16,67 @@ enum : uint8_t { SOLID = 0, FLUID = 1, AIR = 2 };
 
 constexpr int kInvalid = -1;
 
+// ---------------------------------------------------------------- GPU-scope ordering
+__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acqrel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+constexpr long long kGridWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
+constexpr uint32_t kErrGridWait = 32u;            // error bit: a grid barrier gave up
+
+// Barrier over every CTA of a cooperative launch: an arrival counter and a
+// generation word (release/acquire at GPU scope). It gives up after about a
+// second, or at once when another CTA already has (error word non-zero),
+// sets `bit` in *err and returns false; every CTA then winds down.
+__device__ inline bool grid_sync_bounded(unsigned* bar, uint32_t* err, uint32_t bit) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned gen = ld_acquire_gpu_u32(bar + 1);
+        const unsigned arrived = atom_add_acqrel_gpu(bar, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            bar[0] = 0u;  // ordered before the release of the next generation
+            st_release_gpu_u32(bar + 1, gen + 1u);
+        } else {
+            const long long t0 = clock64();
+            while (ld_acquire_gpu_u32(bar + 1) == gen) {
+                if (*(volatile uint32_t*)err != 0u) {
+                    ok = 0;
+                    break;
+                }
+                if (clock64() - t0 > kGridWaitCycles) {
+                    atomicOr(err, bit);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        if (ok && *(volatile uint32_t*)err != 0u) ok = 0;
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
 // The block a kernel body runs as: its index and the block count of its
 // launch. A plain launch passes (blockIdx.x, gridDim.x); a packed launch of
 // many scenes passes the block's place within its own scene's share.

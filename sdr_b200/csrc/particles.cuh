@@ -503,6 +503,7 @@ struct RedistState {
     uint32_t round_base;  // claim stamps used so far by k_redist_par (grows across sweeps)
     uint32_t nmoves_par;  // moves appended by k_redist_par this sweep
     uint32_t pad;
+    unsigned long long rounds_total;  // decision rounds of long lists, all sweeps so far
 };
 
 __device__ __forceinline__ void k_redist_hist_n_body(VB vb_, Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
@@ -914,34 +915,60 @@ constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable *
 // rounds end; a bound on them still records an error bit if they did not.
 constexpr int kRpBS = 512;
 
-__device__ __forceinline__ double rp_cluster_sum(double v, double* slots, int& parity, double* sh) {
+// The CTAs that decide one long list: one thread-block cluster (barrier in
+// hardware), or every CTA of a cooperative launch (a bounded grid barrier;
+// false if it gave up, with an error bit set).
+struct RpCluster {
+    __device__ int rank() const { return (int)cluster_rank(); }
+    __device__ int size() const { return (int)cluster_size(); }
+    __device__ bool sync() const {
+        cluster_sync_all();
+        return true;
+    }
+    double* slots;  // 2 x 16
+};
+struct RpGrid {
+    __device__ int rank() const { return (int)blockIdx.x; }
+    __device__ int size() const { return (int)gridDim.x; }
+    __device__ bool sync() const { return grid_sync_bounded(bar, err, kErrGridWait); }
+    double* slots;  // 2 x gridDim.x
+    unsigned* bar;  // [0] arrivals, [1] generation
+    uint32_t* err;
+};
+
+// Sum over the team of per-thread values (the pending count): CTA sums
+// through a double-buffered slot array.
+template <class Team>
+__device__ __forceinline__ double rp_team_sum(const Team& t, double v, int& parity, double* sh, bool& ok) {
     double bs = block_sum<kRpBS>(v, sh);
-    double* sl = slots + parity * 16;
+    double* sl = t.slots + parity * t.size();
     parity ^= 1;
-    if (threadIdx.x == 0) sl[cluster_rank()] = bs;
-    cluster_sync_all();
+    if (threadIdx.x == 0) sl[t.rank()] = bs;
+    ok = t.sync() && ok;
     double s = 0.0;
-    const int n = (int)cluster_size();
+    const int n = t.size();
     for (int q = 0; q < n; ++q) s += __ldcg(sl + q);
     return s;
 }
 
-__device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
+template <class Team>
+__device__ void redist_par_run(const RedistArgs& a, const Team& team) {
     __shared__ double sh[40];
     RedistState* rs = a.rs;
     if (!rs->active || !rs->par) return;  // written by earlier launches: the same in every CTA
-    const int rank = (int)cluster_rank(), nct = (int)cluster_size();
+    const int rank = team.rank(), nct = team.size();
+    bool ok = true;
     const uint32_t gt = (uint32_t)(rank * kRpBS + threadIdx.x), G = (uint32_t)(nct * kRpBS);
     const uint32_t nc = rs->ncand, cap = a.cap;
     const Grid& g = a.g;
     const int sxy = g.nx * g.ny;
     uint32_t base = rs->round_base;
-    cluster_sync_all();  // every CTA has read the state before it changes
+    ok = team.sync() && ok;  // every CTA has read the state before it changes
     if (base > 0xF0000000u) {  // stamps about to wrap: clear the claims and start again
         const size_t nce = (size_t)g.nx * g.ny * g.nz;
         for (size_t c = gt; c < nce; c += G) a.claim[c] = 0ull;
         base = 0;
-        cluster_sync_all();
+        ok = team.sync() && ok;
     }
     int parity = 0;
     uint32_t round = 0;
@@ -977,7 +1004,7 @@ __device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
             }
             atomicMax(a.claim + c, key);
         }
-        cluster_sync_all();
+        ok = team.sync() && ok;
         // candidates holding all their claims run (counts are as in the claim step)
         double pending = 0.0;
         for (uint32_t m = gt; m < nc; m += G) {
@@ -1028,7 +1055,7 @@ __device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
             a.moves[2 * slot + 1] = (uint32_t)best;
             a.cand[m] = p | kResolved;
         }
-        done = rp_cluster_sum(pending, a.slots, parity, sh) == 0.0;
+        done = rp_team_sum(team, pending, parity, sh, ok) == 0.0 || !ok;
         if (!done && round > nc) {  // cannot happen: the lowest pending candidate always runs
             if (rank == 0 && threadIdx.x == 0) atomicOr(&rs->err, 4u);
             done = true;
@@ -1036,7 +1063,7 @@ __device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
     }
     const uint32_t nm = __ldcg(&rs->nmoves_par);
     for (uint32_t mv = gt; mv < nm; mv += G) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
-    cluster_sync_all();
+    ok = team.sync() && ok;
     if (rank == 0 && threadIdx.x == 0) {
         rs->nmoves = nm;
         rs->moves_total += nm;
@@ -1047,9 +1074,24 @@ __device__ __forceinline__ void k_redist_par_body(VB vb_, RedistArgs a) {
         rs->par = 0;
         rs->nmoves_par = 0;
         rs->round_base = base + round + 1;
+        rs->rounds_total += round;
         if (nm == 0) rs->active = 0;
     }
 }
+__device__ __forceinline__ void k_redist_par_body(VB, RedistArgs a) {
+    RpCluster t;
+    t.slots = a.slots;
+    redist_par_run(a, t);
+}
 __global__ void __launch_bounds__(kRpBS, 1) k_redist_par(RedistArgs a) { k_redist_par_body(VB{blockIdx.x, gridDim.x}, a); }
+
+// The same rounds over every SM: a cooperative launch, one CTA per team rank.
+__global__ void __launch_bounds__(kRpBS, 2) k_redist_par_grid(RedistArgs a, double* slots, unsigned* bar) {
+    RpGrid t;
+    t.slots = slots;
+    t.bar = bar;
+    t.err = &a.rs->err;
+    redist_par_run(a, t);
+}
 
 }  // namespace sdr

@@ -73,27 +73,6 @@ struct TwArgs {
 };
 
 // ---------------------------------------------------------------- memory-order helpers
-__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_gpu(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire_gpu_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_gpu_u32(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned atom_add_acqrel_gpu(unsigned* p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
 __device__ __forceinline__ unsigned long long ld_acquire_cta_sh(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.cta.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(smem_addr(p)) : "memory");
@@ -414,9 +393,18 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     const double TAU = 0.97, SIGMA = 0.25;
     const bool yb = fwd ? lj == 0 : lj == kTwJ - 1;  // this line reads the y neighbour tile
     const bool zb = fwd ? lk == 0 : lk == kTwK - 1;
+    unsigned long long* const timing = a.timing;  // optional section timers (thread 0)
+    long long t_loop = 0, t_wait = 0;
+    if (timing && tid == 0) t_loop = clock64();
     for (int s = s_first; s <= s_last; ++s) {
         const int L = fwd ? s : nlevels - 1 - s;
-        if (tid == 0 && nby >= 0) tw_wait(t, sh, 0, (unsigned long long)s);
+        if (timing && tid == 0 && nby >= 0) {
+            const long long w0 = clock64();
+            tw_wait(t, sh, 0, (unsigned long long)s);
+            t_wait += clock64() - w0;
+        } else if (tid == 0 && nby >= 0) {
+            tw_wait(t, sh, 0, (unsigned long long)s);
+        }
         if (tid == 32 && nbz >= 0) tw_wait(t, sh, 1, (unsigned long long)s);
         tw_bar();
         if (tid == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);  // levels before s are complete
@@ -519,6 +507,12 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     if (tid == 0) {
         st_release_cta_sh(&sh.mine, kTwDone);
         st_release_cta_sh(&sh.done, 1ull);
+        if (timing && s_last >= s_first) {  // per tile: level-loop cycles, waits, levels, sweeps
+            atomicAdd(timing + 9, (unsigned long long)(clock64() - t_loop));
+            atomicAdd(timing + 8, (unsigned long long)t_wait);
+            atomicAdd(timing + 10, (unsigned long long)(s_last - s_first + 1));
+            atomicAdd(timing + 11, 1ull);
+        }
     }
     __syncthreads();  // the progress warp has published the final count and left
 }
@@ -553,6 +547,17 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
     int parity = 0;
     unsigned long long epoch = t.epoch0;
     double residual = 0.0, sigma = 0.0;
+    // phase timers of CTA 0 (between grid barriers every CTA passes together)
+    const bool timed = a.timing != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+    long long tck = timed ? clock64() : 0;
+#define TW_SECTION(idx)                                              \
+    do {                                                             \
+        if (timed) {                                                 \
+            const long long now_ = clock64();                        \
+            atomicAdd(a.timing + (idx), (unsigned long long)(now_ - tck)); \
+            tck = now_;                                              \
+        }                                                            \
+    } while (0)
     int iters = 0;
     double mx = 0.0;
     for (uint32_t i = gt; i < nf; i += G) mx = fmax(mx, fabs(a.b[i]));
@@ -582,6 +587,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
         if (!tw_grid_sync(t, sh)) goto out;
         if (!tw_sweep_all<TW_BUILD>(t, sh, epoch++, nlevels)) goto out;
         if (!tw_grid_sync(t, sh)) goto out;  // the factor's exchange planes are reused by the sweeps
+        TW_SECTION(0);
         if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
         if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
         // dot(z, r)
@@ -640,6 +646,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 if (!tw_grid_sync(t, sh)) goto out;
                 denom = tw_tile_total(t, ntile, sh);
             }
+            TW_SECTION(3);
             if (fabs(denom) < 1e-30) break;
             const double alpha = ddiv(sigma, denom);
             double mr = 0.0;
@@ -651,6 +658,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 mr = fmax(mr, fabs(rv));
             }
             if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and r_c
+            TW_SECTION(5);
             if (residual <= a.tol) break;
             if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
             if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
@@ -668,19 +676,24 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                     if (lane == 0) a.tpart[tl] = acc;
                 }
                 if (!tw_grid_sync(t, sh)) goto out;
+                TW_SECTION(1);  // the sweeps end at this barrier
                 sigma_new = tw_tile_total(t, ntile, sh);
             }
             const double beta = ddiv(sigma_new, sigma);
             for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(t.z_c + a.cinv[i]), dmul(beta, a.s[i]));
             if (!tw_grid_sync(t, sh)) goto out;  // s complete before the next matvec reads neighbours
+            TW_SECTION(6);
             sigma = sigma_new;
         }
         for (uint32_t i = gt; i < nf; i += G) a.p_dense[a.lv_cell[i]] = a.p[i];
     }
 out:
+    TW_SECTION(7);
+#undef TW_SECTION
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *a.out_iters = iters;
         *a.out_residual = residual;
+        if (a.timing) a.timing[14] += 1;
     }
 }
 

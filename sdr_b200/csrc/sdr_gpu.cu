@@ -264,6 +264,7 @@ struct DevStatus {
     unsigned long long wall_count;
     unsigned long long pcg_cycles[16];
     unsigned long long redist_cand, redist_sweeps, redist_long;  // cumulative
+    unsigned long long redist_rounds;                            // cumulative
 };
 
 __device__ __forceinline__ void k_set_u32_body(VB, uint32_t* p, uint32_t v) {
@@ -287,6 +288,7 @@ __device__ __forceinline__ void k_redist_end_body(VB, const RedistState* r, DevS
     s->redist_cand = r->cand_total;
     s->redist_sweeps = r->sweeps_total;
     s->redist_long = r->long_total;
+    s->redist_rounds = r->rounds_total;
 }
 __global__ void k_redist_end(const RedistState* r, DevStatus* s) { k_redist_end_body(VB{blockIdx.x, gridDim.x}, r, s); }
 
@@ -430,7 +432,11 @@ struct sdr_solver {
     MetricsOut* mout = nullptr;
     MetricsOut* h_mout = nullptr;
     bool sorted_valid = false;  // perm/start describe the current particle set
-    unsigned long long redist_seen[3] = {0, 0, 0};  // device redistribution counters at the last status read
+    unsigned long long redist_seen[4] = {0, 0, 0, 0};  // device redistribution counters at the last status read
+    // long candidate lists decided over every SM (k_redist_par_grid), set up on first use
+    int rp_grid = 0;                // CTAs of its cooperative launch (0: not set up, -1: unavailable)
+    double* rp_slots = nullptr;
+    unsigned* rp_bar = nullptr;
     // timing
     cudaEvent_t ev[10] = {};
     cudaEvent_t ev_block = nullptr;  // blocking-sync event (SDR_SOLVER_BLOCKING_SYNC)
@@ -637,6 +643,7 @@ struct sdr_solver {
         dfree(tw_mask, st); dfree(tw_diag, st); dfree(tw_exm, st); dfree(tw_ic, st); dfree(tw_pc, st); dfree(tw_r, st);
         dfree(tw_q, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
         dfree(tw_hi, st); dfree(tw_flags, st); dfree(tw_bar, st);
+        dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
@@ -871,6 +878,27 @@ struct sdr_solver {
         }
     }
 
+    // Cooperative launch of k_redist_par_grid (every CTA resident): false if
+    // the device cannot run it (then the cluster decides long lists).
+    bool rounds_grid_ready() {
+        if (rp_grid != 0) return rp_grid > 0;
+        int coop = 0, nsm = 0, occ = 0;
+        CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_redist_par_grid, kRpBS, 0) != cudaSuccess) {
+            cudaGetLastError();
+            occ = 0;
+        }
+        if (!coop || occ < 1) {
+            rp_grid = -1;
+            return false;
+        }
+        rp_grid = nsm * std::min(occ, 2);
+        dalloc(rp_slots, 2 * (size_t)rp_grid, st);
+        dalloc(rp_bar, 2, st);
+        return true;
+    }
+
     // The whole-GPU tiled solve needs a cooperative launch with every CTA
     // resident; its buffers are allocated on first use. False if the device
     // cannot run it (then the cluster kernel solves).
@@ -905,8 +933,7 @@ struct sdr_solver {
 
     void launch_tiles(const PcgArgs& a) {
         TwArgs t{};
-        t.a = a;
-        t.a.timing = nullptr;
+        t.a = a;  // a.timing: the section timers of profiling level 2
         t.nx = g.nx; t.ny = g.ny; t.nz = g.nz;
         t.tj = tw_tj; t.tk = tw_tk; t.ntiles = tw_tj * tw_tk;
         t.coff = coff;
@@ -1015,8 +1042,10 @@ struct sdr_solver {
         ra.claim = rclaim;
         ra.rounds = shared_gpu ? 0 : 1;  // many scenes: spend no SM time on rounds
         ra.slots = cl_slots;
-        // On a shared GPU one CTA: a cluster launch waits for a whole GPC of
-        // free SMs, which other scenes' solves rarely leave.
+        // A GPU of its own: long lists over every SM. On a shared GPU one CTA:
+        // a cluster launch waits for a whole GPC of free SMs, which other
+        // scenes' solves rarely leave.
+        const bool grid_rounds = !shared_gpu && !pk && rounds_grid_ready();
         if (!shared_gpu && !ctas_rp) ctas_rp = cluster_ctas(k_redist_par, 1, kRpBS, device);
         const int rp_ctas = shared_gpu ? 1 : ctas_rp;
         ra.cap = cap_;
@@ -1032,8 +1061,20 @@ struct sdr_solver {
                    (uint32_t)cand_n);
             SLAUNCH(k_redist_replay, 1, kRedistBS, kRedistSmem, st, ra);
             // long lists only (the replay kernel hands over through the state; otherwise it returns at once)
-            if (rp_ctas == 1) SLAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
-            else launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
+            if (grid_rounds) {
+                // every SM decides the long list (a cooperative launch; it returns at once for short lists)
+                CK(cudaMemsetAsync(rp_bar, 0, 2 * sizeof(unsigned), st));
+                double* sl = rp_slots;
+                unsigned* br = rp_bar;
+                void* args[] = {&ra, &sl, &br};
+                CK(cudaLaunchCooperativeKernel((const void*)k_redist_par_grid, dim3((unsigned)rp_grid), dim3(kRpBS),
+                                               args, 0, st));
+                g_launches.fetch_add(1, std::memory_order_relaxed);
+            } else if (rp_ctas == 1) {
+                SLAUNCH(k_redist_par, 1, kRpBS, 0, st, ra);
+            } else {
+                launch_one_cluster(k_redist_par, rp_ctas, kRpBS, st, ra);
+            }
         }
         SLAUNCH(k_redist_end, 1, 1, 0, st, rds, dst);
         sorted_valid = false;
@@ -1156,10 +1197,12 @@ struct sdr_solver {
             prof.redist_candidates += hst->redist_cand - redist_seen[0];
             prof.redist_sweeps += hst->redist_sweeps - redist_seen[1];
             prof.redist_long_sweeps += hst->redist_long - redist_seen[2];
+            prof.redist_rounds += hst->redist_rounds - redist_seen[3];
         }
         redist_seen[0] = hst->redist_cand;
         redist_seen[1] = hst->redist_sweeps;
         redist_seen[2] = hst->redist_long;
+        redist_seen[3] = hst->redist_rounds;
     }
 
     double cfl_dt() const {  // solver.rs:262-281
