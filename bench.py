@@ -309,7 +309,7 @@ def pool_line(args, rank, world, local):
                     "mean_iters": prof["pcg_cell_iters"] / max(prof["fluid_cells"], 1),
                     "mean_fluid_cells": prof["fluid_cells"] / n_pcg},
             "redistribution": {"candidates": prof["redist_candidates"], "sweeps": prof["redist_sweeps"],
-                               "long_sweeps": prof["redist_long_sweeps"]},
+                               "long_sweeps": prof["redist_long_sweeps"], "rounds": prof["redist_rounds"]},
             "setup_s": setup_s}
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle

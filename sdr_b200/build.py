@@ -4,8 +4,11 @@
     python -m sdr_b200.build --force
 
 The library is a plain C ABI (include/sdr_gpu.h); Python loads it via ctypes.
-Host code is compiled without FMA contraction so the f64 emission math and
-the CFL arithmetic follow the reference's operation order.
+Host and device code are compiled without FMA contraction (-ffp-contract=off,
+--fmad=false): the f64 emission math and the CFL arithmetic follow the
+reference's operation order, and every device float operation is rounded on
+its own, so a kernel body gives the same bits in every kernel it is inlined
+into (a scene's substep alone and inside a packed launch).
 """
 from __future__ import annotations
 
@@ -46,7 +49,8 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
+    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-shared", "-Xcompiler",
+           "-fPIC,-ffp-contract=off",
            "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *sources(), "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -936,8 +936,11 @@ struct RpGrid {
     uint32_t* err;
 };
 
-// Sum over the team of per-thread values (the pending count): CTA sums
-// through a double-buffered slot array.
+// Sum over the team of per-thread values (the pending count, an integer, so
+// the order is free): CTA sums through a double-buffered slot array, read
+// back by one warp per CTA and handed to the CTA through shared memory (every
+// thread reading every slot put hundreds of thousands of loads a round on
+// the same few L2 lines).
 template <class Team>
 __device__ __forceinline__ double rp_team_sum(const Team& t, double v, int& parity, double* sh, bool& ok) {
     double bs = block_sum<kRpBS>(v, sh);
@@ -945,9 +948,17 @@ __device__ __forceinline__ double rp_team_sum(const Team& t, double v, int& pari
     parity ^= 1;
     if (threadIdx.x == 0) sl[t.rank()] = bs;
     ok = t.sync() && ok;
-    double s = 0.0;
-    const int n = t.size();
-    for (int q = 0; q < n; ++q) s += __ldcg(sl + q);
+    __shared__ double total;
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int q = (int)threadIdx.x; q < t.size(); q += 32) s += __ldcg(sl + q);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) total = s;
+    }
+    __syncthreads();
+    const double s = total;
+    __syncthreads();  // `total` is rewritten by the next call
     return s;
 }
 

@@ -22,7 +22,9 @@
 // order and tiling of the other kernels, spread over the grid. The sweeps work
 // in cell order (a line's fluid cells are contiguous there); the residual is
 // copied into cell order by the update phase and z is read back through the
-// cell-order map.
+// cell-order map. Each compute thread keeps the operands of its line's next
+// kTwDepth cells in flight to shared memory (cp.async), so a level's step
+// never waits on a global load.
 //
 // Synchronisation: one cooperative launch (every CTA resident). Phases are
 // separated by a grid barrier (an arrival counter and a generation word,
@@ -44,6 +46,7 @@ constexpr int kTwLines = kTwJ * kTwK;        // compute threads: one per line
 constexpr int kTwBS = kTwLines + 32;         // plus the progress warp
 constexpr int kTwWarps = kTwBS / 32;
 constexpr int kTwRing = 32;                  // levels of neighbour boundary values staged ahead
+constexpr int kTwDepth = 6;                  // cells of each line whose operands are in flight to shared memory
 constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
 constexpr unsigned long long kTwDone = (1ull << 21) - 1;  // progress count of a finished sweep
 constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
@@ -53,12 +56,9 @@ struct TwArgs {
     int nx, ny, nz;
     int tj, tk, ntiles;          // tiles along y and z
     const uint32_t* coff;        // dense cell -> cell-order index of its fluid cell (exclusive scan, ncell + 1)
-    uint8_t* mask_c;             // cell order: fluid-neighbour bits (NB_*)
-    uint8_t* diag_c;             // cell order: non-solid neighbour count
-    int16_t* ic;                 // cell order: i
-    double* pc_c;                // cell order: MIC(0) factor
-    double* r_c;                 // cell order: residual
-    double* q_c;                 // cell order: forward sweep result
+    uint32_t* icm;               // cell order: i | fluid-neighbour bits (NB_*) << 16 | non-solid count << 24
+    double2* rp;                 // cell order: (residual, MIC(0) factor), the forward sweep's operands
+    double2* qp;                 // cell order: (forward sweep result, MIC(0) factor), the backward sweep's
     double* z_c;                 // cell order: backward sweep result
     double* exf;                 // forward exchange planes: per tile [kTwK][nx] (+y face) then [kTwJ][nx] (+z face)
     double* exb;                 // backward exchange planes: the -y and -z faces
@@ -81,7 +81,13 @@ __device__ __forceinline__ unsigned long long ld_acquire_cta_sh(const unsigned l
 __device__ __forceinline__ void st_release_cta_sh(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.cta.shared::cta.u64 [%0], %1;" ::"r"(smem_addr(p)), "l"(v) : "memory");
 }
-__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+// 4-byte asynchronous copy into shared memory (cp_async16 and cp_commit are
+// pressure.cuh's), and a wait until at most N of this thread's groups are pending.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_wait_n() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ bool tw_failed(const TwArgs& t) { return *(volatile uint32_t*)t.err != 0u; }
 // Barrier of the compute warps (named barrier 1).
 __device__ __forceinline__ void tw_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kTwLines) : "memory"); }
@@ -91,6 +97,8 @@ struct TwShared {
     uint8_t m[2][kTwLines];           // the factorisation's neighbour masks, by line
     double ring[2][kTwRing][16];      // upstream neighbours' boundary values by level ([0] y face, [1] z face)
     uint8_t ringm[2][kTwRing][16];    // their masks (factorisation)
+    double2 rec[kTwDepth][kTwLines];  // each line's next cells: (r or q, factor), by cell ordinal mod kTwDepth
+    uint32_t icm[kTwDepth][kTwLines]; // and their (i, mask, count) words
     unsigned long long mine;          // levels this tile has completed (sweep order), for the progress warp
     unsigned long long avail[2];      // levels whose y / z neighbour values are in the ring
     unsigned long long done;          // the tile's sweep is over
@@ -320,27 +328,24 @@ __device__ __forceinline__ void tw_wait(const TwArgs& t, TwShared& sh, int which
     }
 }
 
-// Operands of one cell in sweep order: its level, neighbour mask and the
-// values the sweep reads (diag for the factor; r and the factor forward; q
-// and the factor backward).
+// Operands of a line's o-th cell in sweep order into its shared-memory slot
+// (o mod kTwDepth), as one cp.async group: the (i, mask, count) word, and for
+// the solves the 16-byte (r, factor) or (q, factor) record through L2 (r is
+// written by other CTAs in the update phase). Cells past the line's end
+// commit an empty group, so every level commits exactly one.
 template <int MODE>
-__device__ __forceinline__ void tw_load(const TwArgs& t, int c, int jk, int& L, uint8_t& m, double& ra, double& rb) {
-    L = (int)t.ic[c] + jk;
-    m = t.mask_c[c];
-    if (MODE == TW_BUILD) {
-        ra = (double)t.diag_c[c];
-        rb = 0.0;
-    } else if (MODE == TW_FORWARD) {
-        ra = __ldcg(t.r_c + c);  // written by other CTAs in the update phase
-        rb = t.pc_c[c];
-    } else {
-        ra = t.q_c[c];
-        rb = t.pc_c[c];
+__device__ __forceinline__ void tw_stage(const TwArgs& t, TwShared& sh, int tid, int first, int step, int count, int o) {
+    if (o < count) {
+        const int c = first + step * o;
+        const int slot = o % kTwDepth;
+        cp_async4(&sh.icm[slot][tid], t.icm + c);
+        if (MODE != TW_BUILD) cp_async16(&sh.rec[slot][tid], (MODE == TW_FORWARD ? t.rp : t.qp) + c);
     }
+    cp_commit();
 }
 
-// One tile's sweep. BUILD: the MIC(0) factor into pc_c (forward order).
-// FORWARD: q = L^-1 r_c. BACKWARD: z = L^-T q, plus the z*r products in cell
+// One tile's sweep. BUILD: the MIC(0) factor into rp.y and qp.y (forward
+// order). FORWARD: q = L^-1 r into qp.x. BACKWARD: z = L^-T q, plus the z*r products in cell
 // order for the reference dot order.
 template <int MODE>
 __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long long epoch, int nlevels) {
@@ -378,16 +383,20 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     const size_t plane = (size_t)(kTwJ + kTwK) * nx;
     double* ex_own = (fwd ? t.exf : t.exb) + (size_t)tile * plane;
     uint8_t* exm_own = t.exm + (size_t)tile * plane;
-    // this line's next two cells in sweep order: the operands of the cell
-    // after next load while the next levels run
+    // This line's cells in sweep order, ordinals 0 .. count-1. The operands of
+    // the next kTwDepth cells are in flight to shared memory at all times:
+    // consuming ordinal o stages o + kTwDepth, one cp.async group per level.
+    // A cell is consumed at least one level after its predecessor, so when
+    // ordinal o is read the group that staged it has at least kTwDepth - 1
+    // groups after it, and waiting until kTwDepth - 1 are pending suffices.
     const int step = fwd ? 1 : -1;
-    int cur = fwd ? (int)beg : (int)end - 1;
-    const int stop = fwd ? (int)end : (int)beg - 1;
-    int L0 = -1, L1 = -1;
-    uint8_t m0 = 0, m1 = 0;
-    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-    if (cur != stop) tw_load<MODE>(t, cur, jk, L0, m0, a0, b0);
-    if (cur != stop && cur + step != stop) tw_load<MODE>(t, cur + step, jk, L1, m1, a1, b1);
+    const int first = fwd ? (int)beg : (int)end - 1;
+    const int count = (int)(end - beg);
+    for (int o = 0; o < kTwDepth; ++o) tw_stage<MODE>(t, sh, tid, first, step, count, o);
+    int ord = 0;       // next cell to consume
+    int cur = first;   // its cell-order index
+    int L0 = -1;       // its level (-1: none left)
+    bool fresh = true; // L0 is still to be read from the slot of `ord`
     double carry = 0.0;   // the value of this line's previous cell (the -x / +x predecessor)
     uint8_t carry_m = 0;  // its neighbour mask (factorisation)
     const double TAU = 0.97, SIGMA = 0.25;
@@ -395,9 +404,14 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     const bool zb = fwd ? lk == 0 : lk == kTwK - 1;
     unsigned long long* const timing = a.timing;  // optional section timers (thread 0)
     long long t_loop = 0, t_wait = 0;
-    if (timing && tid == 0) t_loop = clock64();
+    if (timing && (tid == 0 || tid == 32)) t_loop = clock64();
     for (int s = s_first; s <= s_last; ++s) {
         const int L = fwd ? s : nlevels - 1 - s;
+        if (fresh) {
+            fresh = false;
+            cp_wait_n<kTwDepth - 1>();
+            L0 = ord < count ? (int)(sh.icm[ord % kTwDepth][tid] & 0xffffu) + jk : -1;
+        }
         if (timing && tid == 0 && nby >= 0) {
             const long long w0 = clock64();
             tw_wait(t, sh, 0, (unsigned long long)s);
@@ -405,13 +419,27 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
         } else if (tid == 0 && nby >= 0) {
             tw_wait(t, sh, 0, (unsigned long long)s);
         }
-        if (tid == 32 && nbz >= 0) tw_wait(t, sh, 1, (unsigned long long)s);
+        if (timing && tid == 32 && nbz >= 0) {
+            const long long w0 = clock64();
+            tw_wait(t, sh, 1, (unsigned long long)s);
+            t_wait += clock64() - w0;
+        } else if (tid == 32 && nbz >= 0) {
+            tw_wait(t, sh, 1, (unsigned long long)s);
+        }
         tw_bar();
         if (tid == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);  // levels before s are complete
         const int wp = (s - 1) & 1, wc = s & 1, rs = s % kTwRing;
-        if (L != L0) continue;
+        if (L != L0) {
+            cp_commit();  // one group per level
+            continue;
+        }
         const int i = L - jk;
-        const uint8_t m = m0;
+        const int slot = ord % kTwDepth;
+        const uint32_t word = sh.icm[slot][tid];
+        const uint8_t m = (uint8_t)(word >> 16);
+        const double2 rec = MODE == TW_BUILD ? make_double2(0.0, 0.0) : sh.rec[slot][tid];
+        const double a0 = MODE == TW_BUILD ? (double)(word >> 24) : rec.x;  // diag, r or q
+        const double b0 = rec.y;                                              // the factor
         if (MODE == TW_BUILD) {
             double axi = 0, pxi = 0, axi_y = 0, axi_z = 0;
             double ayj = 0, pyj = 0, ayj_x = 0, ayj_z = 0;
@@ -445,7 +473,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
                             dmul(TAU, dadd(dadd(mx, my), mz)));
             if (e < dmul(SIGMA, diag)) e = diag;
             const double pc = e > 0.0 ? ddiv(1.0, __dsqrt_rn(e)) : 0.0;
-            t.pc_c[cur] = pc;
+            t.rp[cur].y = pc;
+            t.qp[cur].y = pc;
             sh.v[wc][tid] = pc;
             sh.m[wc][tid] = m;
             carry = pc;
@@ -466,7 +495,7 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             if (m >> NB_MZ & 1) tt = dadd(tt, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid - kTwJ]);
             const double qv = dmul(tt, b0);
             const double pqv = dmul(b0, qv);
-            t.q_c[cur] = qv;
+            t.qp[cur].x = qv;
             sh.v[wc][tid] = pqv;
             carry = pqv;
             if (lj == kTwJ - 1) ex_own[(size_t)lk * nx + i] = pqv;
@@ -480,40 +509,36 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             if (m >> NB_PZ & 1) tt = dadd(tt, dmul(pc, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid + kTwJ]));
             const double zv = dmul(tt, pc);
             t.z_c[cur] = zv;
-            if (a.exact_dots) a.prod[cur] = dmul(zv, __ldcg(t.r_c + cur));
+            if (a.exact_dots) a.prod[cur] = dmul(zv, __ldcg(&t.rp[cur].x));
             sh.v[wc][tid] = zv;
             carry = zv;
             if (lj == 0) ex_own[(size_t)lk * nx + i] = zv;
             if (lk == 0) ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = zv;
         }
-        // shift the cursor; the cell after next starts loading now
+        // the slot's values are in registers: it takes the cell kTwDepth ahead
+        tw_stage<MODE>(t, sh, tid, first, step, count, ord + kTwDepth);
+        ++ord;
         cur += step;
-        L0 = L1;
-        m0 = m1;
-        a0 = a1;
-        b0 = b1;
-        L1 = -1;
-        const int nxt = cur + step;
-        if (cur != stop && nxt != stop) {
-            tw_load<MODE>(t, nxt, jk, L1, m1, a1, b1);
-            const int ahead = nxt + 8 * step;
-            if (MODE != TW_BUILD && (fwd ? ahead < (int)end : ahead >= (int)beg)) {
-                prefetch_l1(t.pc_c + ahead);
-                if (MODE == TW_BACKWARD) prefetch_l1(t.q_c + ahead);
-            }
-        }
+        fresh = true;
     }
+    cp_wait_n<0>();  // nothing in flight into the slots the next sweep reuses
     tw_bar();
     if (tid == 0) {
         st_release_cta_sh(&sh.mine, kTwDone);
         st_release_cta_sh(&sh.done, 1ull);
-        if (timing && s_last >= s_first) {  // per tile: level-loop cycles, waits, levels, sweeps
-            atomicAdd(timing + 9, (unsigned long long)(clock64() - t_loop));
+        if (timing && s_last >= s_first) {  // per tile: level-loop cycles, y waits, levels, sweeps
+            const unsigned long long loop = (unsigned long long)(clock64() - t_loop);
+            atomicAdd(timing + 9, loop);
             atomicAdd(timing + 8, (unsigned long long)t_wait);
             atomicAdd(timing + 10, (unsigned long long)(s_last - s_first + 1));
             atomicAdd(timing + 11, 1ull);
+            if (nby < 0 && nbz < 0) {  // a tile that never waits: the bare level step
+                atomicAdd(timing + 12, loop);
+                atomicAdd(timing + 13, (unsigned long long)(s_last - s_first + 1));
+            }
         }
     }
+    if (timing && tid == 32 && s_last >= s_first) atomicAdd(timing + 15, (unsigned long long)t_wait);  // z waits
     __syncthreads();  // the progress warp has published the final count and left
 }
 
@@ -573,11 +598,9 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
             const uint32_t cell = a.lv_cell[i];
             const int ii = (int)(cell % (uint32_t)t.nx), jj = (int)((cell / (uint32_t)t.nx) % (uint32_t)t.ny),
                       kk = (int)(cell / ((uint32_t)t.nx * (uint32_t)t.ny));
-            t.mask_c[c] = a.nmask[i];
-            t.diag_c[c] = a.diag[i];
-            t.ic[c] = (int16_t)ii;
+            t.icm[c] = (uint32_t)ii | (uint32_t)a.nmask[i] << 16 | (uint32_t)a.diag[i] << 24;
             const double bv = a.b[i];
-            t.r_c[c] = bv;
+            t.rp[c].x = bv;
             a.r[i] = bv;
             a.p[i] = 0.0;
             const int tile = jj / kTwJ + (kk / kTwK) * t.tj;
@@ -654,10 +677,10 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 a.p[i] = dadd(a.p[i], dmul(alpha, __ldcg(a.s + i)));
                 const double rv = dsub(a.r[i], dmul(alpha, __ldcg(a.as + i)));
                 a.r[i] = rv;
-                t.r_c[a.cinv[i]] = rv;
+                t.rp[a.cinv[i]].x = rv;
                 mr = fmax(mr, fabs(rv));
             }
-            if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and r_c
+            if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and rp.x
             TW_SECTION(5);
             if (residual <= a.tol) break;
             if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;

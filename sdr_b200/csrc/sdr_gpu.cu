@@ -453,9 +453,10 @@ struct sdr_solver {
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
     double* cl_slots = nullptr;     // CTA partials of the cluster kernels
     // whole-GPU tiled solve (k_pcg_tiles), allocated on first use
-    uint8_t *tw_mask = nullptr, *tw_diag = nullptr, *tw_exm = nullptr;
-    int16_t* tw_ic = nullptr;
-    double *tw_pc = nullptr, *tw_r = nullptr, *tw_q = nullptr, *tw_z = nullptr, *tw_exf = nullptr, *tw_exb = nullptr,
+    uint8_t* tw_exm = nullptr;
+    uint32_t* tw_icm = nullptr;
+    double2 *tw_rp = nullptr, *tw_qp = nullptr;
+    double *tw_z = nullptr, *tw_exf = nullptr, *tw_exb = nullptr,
            *tw_slots = nullptr;
     int *tw_lo = nullptr, *tw_hi = nullptr;
     unsigned long long* tw_flags = nullptr;
@@ -640,8 +641,7 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(tw_mask, st); dfree(tw_diag, st); dfree(tw_exm, st); dfree(tw_ic, st); dfree(tw_pc, st); dfree(tw_r, st);
-        dfree(tw_q, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
+        dfree(tw_exm, st); dfree(tw_icm, st); dfree(tw_rp, st); dfree(tw_qp, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
         dfree(tw_hi, st); dfree(tw_flags, st); dfree(tw_bar, st);
         dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
@@ -841,14 +841,18 @@ struct sdr_solver {
             SLAUNCH(k_pcg, 1, kPcgBS, kPcgSmem, st, a);
             return;
         }
-        const bool large = pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells && !shared_gpu;
+        // fluid cells of the last solve; before the first one, the cells the
+        // particles fill at particles_per_cell each
+        const uint64_t nf_hint =
+            last_nf ? (uint64_t)last_nf : (uint64_t)n / std::max<uint64_t>(fluid.particles_per_cell, 1);
+        const bool large = pcg_kernel == SDR_PCG_AUTO && nf_hint >= kClusterMinFluidCells && !shared_gpu;
         if ((pcg_kernel == SDR_PCG_TILES || large) && tiles_ready()) {
             launch_tiles(a);
             if (profiling) prof.pcg_tile_launches += 1;
             return;
         }
         const bool cluster = pcg_kernel == SDR_PCG_CLUSTER || pcg_kernel == SDR_PCG_TILES || large ||
-                             (pcg_kernel == SDR_PCG_AUTO && last_nf >= kClusterMinFluidCells);
+                             (pcg_kernel == SDR_PCG_AUTO && nf_hint >= kClusterMinFluidCells);
         if (cluster) {
             // One cluster of up to 16 CTAs (one per SM); the levels of each
             // sweep are separated by the hardware cluster barrier.
@@ -920,8 +924,7 @@ struct sdr_solver {
         tw_tj = (g.ny + kTwJ - 1) / kTwJ;
         tw_tk = (g.nz + kTwK - 1) / kTwK;
         const size_t nt = (size_t)tw_tj * tw_tk, plane = (size_t)(kTwJ + kTwK) * g.nx;
-        dalloc(tw_mask, ncell, st); dalloc(tw_diag, ncell, st); dalloc(tw_ic, ncell, st);
-        dalloc(tw_pc, ncell, st); dalloc(tw_r, ncell, st); dalloc(tw_q, ncell, st); dalloc(tw_z, ncell, st);
+        dalloc(tw_icm, ncell, st); dalloc(tw_rp, ncell, st); dalloc(tw_qp, ncell, st); dalloc(tw_z, ncell, st);
         dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st); dalloc(tw_exm, nt * plane, st);
         dalloc(tw_lo, nt, st); dalloc(tw_hi, nt, st);
         dalloc(tw_flags, nt, st);
@@ -937,8 +940,7 @@ struct sdr_solver {
         t.nx = g.nx; t.ny = g.ny; t.nz = g.nz;
         t.tj = tw_tj; t.tk = tw_tk; t.ntiles = tw_tj * tw_tk;
         t.coff = coff;
-        t.mask_c = tw_mask; t.diag_c = tw_diag; t.ic = tw_ic;
-        t.pc_c = tw_pc; t.r_c = tw_r; t.q_c = tw_q; t.z_c = tw_z;
+        t.icm = tw_icm; t.rp = tw_rp; t.qp = tw_qp; t.z_c = tw_z;
         t.exf = tw_exf; t.exb = tw_exb; t.exm = tw_exm;
         t.tlo = tw_lo; t.thi = tw_hi;
         t.flags = tw_flags;
