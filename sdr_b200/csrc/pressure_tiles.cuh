@@ -48,7 +48,6 @@ constexpr int kTwWarps = kTwBS / 32;
 constexpr int kTwRing = 32;                  // levels of neighbour boundary values staged ahead
 constexpr int kTwDepth = 6;                  // cells of each line whose operands are in flight to shared memory
 constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
-constexpr unsigned long long kTwDone = (1ull << 21) - 1;  // progress count of a finished sweep
 constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
 
 struct TwArgs {
@@ -62,11 +61,8 @@ struct TwArgs {
     double* z_c;                 // cell order: backward sweep result
     double* exf;                 // forward exchange planes: per tile [kTwK][nx] (+y face) then [kTwJ][nx] (+z face)
     double* exb;                 // backward exchange planes: the -y and -z faces
-    uint8_t* exm;                // mask planes of the factorisation (+y, +z faces)
     int* tlo;                    // per tile: first and last level of its fluid cells
     int* thi;
-    unsigned long long* flags;   // per tile: (epoch << 21) | levels completed in sweep order
-    unsigned long long epoch0;   // first sweep epoch of this solve
     unsigned* bar;               // grid barrier: [0] arrivals, [1] generation
     double* gslots;              // 2 x gridDim CTA partials of grid maxima
     uint32_t* err;               // error bits
@@ -80,6 +76,21 @@ __device__ __forceinline__ unsigned long long ld_acquire_cta_sh(const unsigned l
 }
 __device__ __forceinline__ void st_release_cta_sh(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.cta.shared::cta.u64 [%0], %1;" ::"r"(smem_addr(p)), "l"(v) : "memory");
+}
+// Exchange-plane entries: written and polled with relaxed GPU-scope accesses.
+// kTwEmpty is a signalling-NaN pattern no arithmetic produces (IEEE results
+// are quiet NaNs), so it can mark an entry not yet written.
+constexpr unsigned long long kTwEmpty = 0x7FF4DEADBEEF0001ull;
+__device__ __forceinline__ double ld_relaxed_gpu_f64(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu_f64(double* p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_gpu_u64(double* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 // 4-byte asynchronous copy into shared memory (cp_async16 and cp_commit are
 // pressure.cuh's), and a wait until at most N of this thread's groups are pending.
@@ -101,7 +112,6 @@ struct TwShared {
     uint32_t icm[kTwDepth][kTwLines]; // and their (i, mask, count) words
     unsigned long long mine;          // levels this tile has completed (sweep order), for the progress warp
     unsigned long long avail[2];      // levels whose y / z neighbour values are in the ring
-    unsigned long long done;          // the tile's sweep is over
     int ok;
     double red[kTwWarps];
 };
@@ -227,88 +237,99 @@ __device__ bool tw_exact_dot(const TwArgs& t, TwShared& sh, double& out) {
 // ---------------------------------------------------------------- the tile sweeps
 enum { TW_BUILD = 0, TW_FORWARD = 1, TW_BACKWARD = 2 };
 
-// The progress warp of one tile's sweep. Lane 0 publishes the tile's
-// progress to global memory (release); lanes 1 and 2 poll the two upstream
-// neighbours' progress (acquire); then lanes 0-15 copy the y neighbour's
-// boundary values of every newly completed level into the shared ring and
-// lanes 16-31 the z neighbour's, as far as the ring has room, and publish how
-// many levels are staged.
+// The progress warp of one tile's sweep: it stages the upstream tiles'
+// boundary values into the shared ring, lanes 0-15 the y face (line
+// (jb, k0 + l)), lanes 16-31 the z face (line (j0 + l, kb)), and publishes per
+// face how many levels are staged. The values carry their own readiness: every
+// entry of an exchange plane holds kTwEmpty until its producer writes it (the
+// planes are filled at the start of the solve), a lane polls the entries its
+// next levels need (relaxed loads, up to eight levels at a time), and resets
+// each entry it staged to kTwEmpty (the producer writes it again only in the
+// next sweep of this direction, after a grid barrier). So a hand-off costs
+// the producer's store reaching L2 and one poll, with no progress flags and no
+// GPU-scope fences. A level needs no entry where the producer tile has no
+// level before it (its range is in tlo/thi) or the cell lies outside the grid:
+// the ring gets 0 there. The factorisation also stages the upstream cell's
+// neighbour mask, read from the static cell tables.
 template <int MODE>
-__device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nby, int nbz, unsigned long long epoch,
-                                 int s_first, int s_last, int nlevels) {
+__device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nby, int nbz, int s_first,
+                                 int s_last, int nlevels) {
     constexpr bool fwd = MODE != TW_BACKWARD;
     const int lane = threadIdx.x & 31;
     const int J = tile % t.tj, K = tile / t.tj;
     const int j0 = J * kTwJ, k0 = K * kTwK, nx = t.nx;
     const size_t plane = (size_t)(kTwJ + kTwK) * nx;
-    const double* ex = fwd ? t.exf : t.exb;
-    // this lane's boundary line: lanes 0-15 the y face (line (jb, k0 + lane)),
-    // lanes 16-31 the z face (line (j0 + lane - 16, kb))
     const int face = lane >> 4, l = lane & 15;
     const int nb = face == 0 ? nby : nbz;
+    // this tile's boundary line and the producer's line beside it
     const int jl = face == 0 ? (fwd ? j0 : j0 + kTwJ - 1) : j0 + l;
     const int kl = face == 0 ? k0 + l : (fwd ? k0 : k0 + kTwK - 1);
-    const bool line_ok = nb >= 0 && jl < t.ny && kl < t.nz;
+    const int jp = face == 0 ? (fwd ? jl - 1 : jl + 1) : jl;
+    const int kp = face == 0 ? kl : (fwd ? kl - 1 : kl + 1);
+    const bool line_ok = nb >= 0 && (face == 0 ? l < kTwK : l < kTwJ) && jl < t.ny && kl < t.nz;
     const size_t row = (size_t)(face == 0 ? 0 : kTwK * nx) + (size_t)l * nx;
-    const double* src = nb >= 0 ? ex + (size_t)nb * plane + row : nullptr;
-    const uint8_t* srcm = nb >= 0 ? t.exm + (size_t)nb * plane + row : nullptr;
-    const unsigned long long base = epoch << 21;
-    unsigned long long published = ~0ull;
-    int copied = s_first;  // next level (sweep order) to stage, for this lane's face
+    double* src = nb >= 0 ? (fwd ? t.exf : t.exb) + (size_t)nb * plane + row : nullptr;
+    // the producer's levels in sweep order
+    int pf = 1, pl = 0;
+    if (line_ok) {
+        const int lo = __ldcg(t.tlo + nb), hi = __ldcg(t.thi + nb);
+        if (hi >= lo) {
+            pf = fwd ? lo : nlevels - 1 - hi;
+            pl = fwd ? hi : nlevels - 1 - lo;
+        }
+    }
+    int next = line_ok ? s_first : s_last + 1;  // next level (sweep order) this lane stages
+    int staged_face = -1;                       // levels of this face published so far
     const long long t0 = clock64();
-    for (;;) {
-        const unsigned long long done = ld_acquire_cta_sh(&sh.done);
-        const unsigned long long mine = ld_acquire_cta_sh(&sh.mine);
-        if (lane == 0 && mine != published) {
-            st_release_gpu(t.flags + tile, base | mine);
-            published = mine;
-        }
-        if (done) break;
-        // neighbours' progress: levels before `prog` are complete
-        unsigned long long pv = 0ull;
-        if (lane == 1 && nby >= 0) pv = ld_acquire_gpu(t.flags + nby);
-        if (lane == 2 && nbz >= 0) pv = ld_acquire_gpu(t.flags + nbz);
-        const unsigned long long py = __shfl_sync(0xffffffffu, pv, 1), pz = __shfl_sync(0xffffffffu, pv, 2);
-        const unsigned long long p = face == 0 ? py : pz;
-        const long long prog = nb < 0 ? (long long)s_last + 1 : (p < base ? 0ll : (long long)(p - base));
-        // stage the levels s with s <= prog (the neighbour's level s - 1 is complete), ring room permitting
-        const int lim = (int)min(min((long long)s_last, prog), (long long)mine + kTwRing - 1);
-        if (line_ok) {
-            // eight levels at a time: their loads are independent (consecutive i of one line)
-            for (int sq0 = copied; sq0 <= lim; sq0 += 8) {
-                double v[8];
-                uint8_t vm[8];
+    for (unsigned polls = 1;; ++polls) {
+        const int mine = (int)ld_acquire_cta_sh(&sh.mine);
+        const int lim = min(s_last, mine + kTwRing - 1);  // ring room
+        if (next <= lim) {
+            // up to eight levels: an entry per level that needs one, loaded at once
+            double v[8];
+            bool need[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int sq = sq0 + u;
-                    const int L = fwd ? sq : nlevels - 1 - sq;
-                    const int i = L - jl - kl;
-                    const bool in = sq <= lim && i >= 0 && i < nx;
-                    v[u] = in ? __ldcg(src + i) : 0.0;
-                    vm[u] = (MODE == TW_BUILD && in) ? __ldcg(srcm + i) : (uint8_t)0;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int sq = sq0 + u;
-                    if (sq <= lim) {
-                        sh.ring[face][sq % kTwRing][l] = v[u];
-                        if (MODE == TW_BUILD) sh.ringm[face][sq % kTwRing][l] = vm[u];
-                    }
-                }
+            for (int u = 0; u < 8; ++u) {
+                const int sq = next + u;
+                const int L = fwd ? sq : nlevels - 1 - sq;
+                const int i = L - jl - kl;
+                need[u] = sq <= lim && sq - 1 >= pf && sq - 1 <= pl && i >= 0 && i < nx;
+                v[u] = need[u] ? ld_relaxed_gpu_f64(src + i) : 0.0;
             }
+            int u = 0;
+            for (; u < 8 && next + u <= lim; ++u) {
+                if (need[u] && __double_as_longlong(v[u]) == (long long)kTwEmpty) break;  // not written yet
+                const int sq = next + u;
+                const int L = fwd ? sq : nlevels - 1 - sq;
+                const int i = L - jl - kl;
+                sh.ring[face][sq % kTwRing][l] = need[u] ? v[u] : 0.0;
+                if (MODE == TW_BUILD) {
+                    uint8_t m = 0;
+                    if (need[u]) {
+                        const size_t d = ((size_t)kp * t.ny + jp) * (size_t)nx + i;
+                        const uint32_t c0 = __ldcg(t.coff + d), c1 = __ldcg(t.coff + d + 1);
+                        if (c1 != c0) m = (uint8_t)(__ldcg(t.icm + c0) >> 16);
+                    }
+                    sh.ringm[face][sq % kTwRing][l] = m;
+                }
+                if (need[u]) st_relaxed_gpu_u64(src + i, kTwEmpty);
+            }
+            next += u;
         }
-        // every lane of a face has staged up to its `lim`: publish it (lanes 0 and 16)
-        const int lim_y = __shfl_sync(0xffffffffu, lim, 0), lim_z = __shfl_sync(0xffffffffu, lim, 16);
+        // a face's levels are staged up to the least of its lanes
+        int fm = next;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) fm = min(fm, __shfl_xor_sync(0xffffffffu, fm, o));
         __syncwarp();
-        if (lane == 0 && lim_y + 1 > copied) st_release_cta_sh(&sh.avail[0], (unsigned long long)(lim_y + 1));
-        if (lane == 16 && lim_z + 1 > copied) st_release_cta_sh(&sh.avail[1], (unsigned long long)(lim_z + 1));
-        copied = max(copied, lim + 1);
-        const bool give_up = __shfl_sync(0xffffffffu, (int)(tw_failed(t) || clock64() - t0 > kTwWaitCycles), 0);
-        if (give_up) {
+        if ((lane == 0 || lane == 16) && fm > staged_face) {
+            st_release_cta_sh(&sh.avail[face], (unsigned long long)fm);
+            staged_face = fm;
+        }
+        if (__all_sync(0xffffffffu, next > s_last)) break;
+        if ((polls & 63u) == 0u && __shfl_sync(0xffffffffu, (int)(tw_failed(t) || clock64() - t0 > kTwWaitCycles), 0)) {
             if (lane == 0) {
                 atomicOr(t.err, kTwErrWait);
-                st_release_gpu(t.flags + tile, base | kTwDone);  // release whoever waits on this tile
-                st_release_cta_sh(&sh.avail[0], ~0ull >> 1);      // and this tile's compute warps
+                st_release_cta_sh(&sh.avail[0], ~0ull >> 1);  // release this tile's compute warps
                 st_release_cta_sh(&sh.avail[1], ~0ull >> 1);
             }
             break;
@@ -348,7 +369,7 @@ __device__ __forceinline__ void tw_stage(const TwArgs& t, TwShared& sh, int tid,
 // order). FORWARD: q = L^-1 r into qp.x. BACKWARD: z = L^-T q, plus the z*r products in cell
 // order for the reference dot order.
 template <int MODE>
-__device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long long epoch, int nlevels) {
+__device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     const PcgArgs& a = t.a;
     const int tid = threadIdx.x;
     const int J = tile % t.tj, K = tile / t.tj;
@@ -362,11 +383,10 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     if (tid == 0) {
         sh.mine = (unsigned long long)s_first;
         sh.avail[0] = sh.avail[1] = (unsigned long long)s_first;
-        sh.done = 0ull;
     }
     __syncthreads();
     if (tid >= kTwLines) {
-        tw_progress_warp<MODE>(t, sh, tile, nby, nbz, epoch, s_first, s_last, nlevels);
+        tw_progress_warp<MODE>(t, sh, tile, nby, nbz, s_first, s_last, nlevels);
         __syncthreads();
         return;
     }
@@ -382,7 +402,13 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     const int jk = j + k;
     const size_t plane = (size_t)(kTwJ + kTwK) * nx;
     double* ex_own = (fwd ? t.exf : t.exb) + (size_t)tile * plane;
-    uint8_t* exm_own = t.exm + (size_t)tile * plane;
+    // the lines on the downstream faces write an exchange entry at every level
+    // of the sweep (0 where the line has no cell), so the downstream tile's
+    // progress warp finds every entry it polls written
+    const bool in_grid = j < t.ny && k < t.nz;
+    double* const ex_y = in_grid && (fwd ? lj == kTwJ - 1 : lj == 0) ? ex_own + (size_t)lk * nx : nullptr;
+    double* const ex_z = in_grid && (fwd ? lk == kTwK - 1 : lk == 0) ? ex_own + (size_t)kTwK * nx + (size_t)lj * nx
+                                                                      : nullptr;
     // This line's cells in sweep order, ordinals 0 .. count-1. The operands of
     // the next kTwDepth cells are in flight to shared memory at all times:
     // consuming ordinal o stages o + kTwDepth, one cp.async group per level.
@@ -427,13 +453,19 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             tw_wait(t, sh, 1, (unsigned long long)s);
         }
         tw_bar();
-        if (tid == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);  // levels before s are complete
+        // levels before s are complete (every eighth level: the progress warp
+        // only needs it to reuse ring slots, 32 levels deep)
+        if (tid == 0 && ((s - s_first) & 7) == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);
         const int wp = (s - 1) & 1, wc = s & 1, rs = s % kTwRing;
+        const int i = L - jk;
         if (L != L0) {
+            if (i >= 0 && i < nx) {  // no cell here: the downstream entry still gets written
+                if (ex_y) st_relaxed_gpu_f64(ex_y + i, 0.0);
+                if (ex_z) st_relaxed_gpu_f64(ex_z + i, 0.0);
+            }
             cp_commit();  // one group per level
             continue;
         }
-        const int i = L - jk;
         const int slot = ord % kTwDepth;
         const uint32_t word = sh.icm[slot][tid];
         const uint8_t m = (uint8_t)(word >> 16);
@@ -479,14 +511,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             sh.m[wc][tid] = m;
             carry = pc;
             carry_m = m;
-            if (lj == kTwJ - 1) {
-                ex_own[(size_t)lk * nx + i] = pc;
-                exm_own[(size_t)lk * nx + i] = m;
-            }
-            if (lk == kTwK - 1) {
-                ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = pc;
-                exm_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = m;
-            }
+            if (ex_y) st_relaxed_gpu_f64(ex_y + i, pc);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + i, pc);
         } else if (MODE == TW_FORWARD) {
             // t = r + pq[-x] + pq[-y] + pq[-z]; q = t * pc (pcg_apply_mic0, forward)
             double tt = a0;
@@ -498,8 +524,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             t.qp[cur].x = qv;
             sh.v[wc][tid] = pqv;
             carry = pqv;
-            if (lj == kTwJ - 1) ex_own[(size_t)lk * nx + i] = pqv;
-            if (lk == kTwK - 1) ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = pqv;
+            if (ex_y) st_relaxed_gpu_f64(ex_y + i, pqv);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + i, pqv);
         } else {
             // t = q + pc z[+x] + pc z[+y] + pc z[+z]; z = t * pc (pcg_apply_mic0, backward)
             const double pc = b0;
@@ -512,8 +538,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
             if (a.exact_dots) a.prod[cur] = dmul(zv, __ldcg(&t.rp[cur].x));
             sh.v[wc][tid] = zv;
             carry = zv;
-            if (lj == 0) ex_own[(size_t)lk * nx + i] = zv;
-            if (lk == 0) ex_own[(size_t)kTwK * nx + (size_t)lj * nx + i] = zv;
+            if (ex_y) st_relaxed_gpu_f64(ex_y + i, zv);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + i, zv);
         }
         // the slot's values are in registers: it takes the cell kTwDepth ahead
         tw_stage<MODE>(t, sh, tid, first, step, count, ord + kTwDepth);
@@ -524,8 +550,6 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
     cp_wait_n<0>();  // nothing in flight into the slots the next sweep reuses
     tw_bar();
     if (tid == 0) {
-        st_release_cta_sh(&sh.mine, kTwDone);
-        st_release_cta_sh(&sh.done, 1ull);
         if (timing && s_last >= s_first) {  // per tile: level-loop cycles, y waits, levels, sweeps
             const unsigned long long loop = (unsigned long long)(clock64() - t_loop);
             atomicAdd(timing + 9, loop);
@@ -547,13 +571,13 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, unsigned long 
 // decreasing order backward, so waits always point to tiles earlier in some
 // CTA's order and the earliest unfinished tile can always run.
 template <int MODE>
-__device__ bool tw_sweep_all(const TwArgs& t, TwShared& sh, unsigned long long epoch, int nlevels) {
+__device__ bool tw_sweep_all(const TwArgs& t, TwShared& sh, int nlevels) {
     const int G = (int)gridDim.x, b = (int)blockIdx.x;
     if (MODE == TW_BACKWARD) {
         if (b < t.ntiles)
-            for (int tile = b + ((t.ntiles - 1 - b) / G) * G; tile >= 0; tile -= G) tw_sweep<MODE>(t, sh, tile, epoch, nlevels);
+            for (int tile = b + ((t.ntiles - 1 - b) / G) * G; tile >= 0; tile -= G) tw_sweep<MODE>(t, sh, tile, nlevels);
     } else {
-        for (int tile = b; tile < t.ntiles; tile += G) tw_sweep<MODE>(t, sh, tile, epoch, nlevels);
+        for (int tile = b; tile < t.ntiles; tile += G) tw_sweep<MODE>(t, sh, tile, nlevels);
     }
     return !tw_failed(t);
 }
@@ -570,7 +594,6 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
     const int gw = blockIdx.x * kTwWarps + (threadIdx.x >> 5), nw = gridDim.x * kTwWarps;
     const int nlevels = a.nlevels;
     int parity = 0;
-    unsigned long long epoch = t.epoch0;
     double residual = 0.0, sigma = 0.0;
     // phase timers of CTA 0 (between grid barriers every CTA passes together)
     const bool timed = a.timing != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
@@ -590,6 +613,15 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
         t.tlo[q] = INT32_MAX;
         t.thi[q] = -1;
     }
+    {  // every exchange entry unwritten (the grid barrier below orders this before the sweeps)
+        const size_t ne = (size_t)t.ntiles * (size_t)(kTwJ + kTwK) * (size_t)t.nx;
+        unsigned long long* ef = reinterpret_cast<unsigned long long*>(t.exf);
+        unsigned long long* eb = reinterpret_cast<unsigned long long*>(t.exb);
+        for (size_t q = gt; q < ne; q += G) {
+            ef[q] = kTwEmpty;
+            eb[q] = kTwEmpty;
+        }
+    }
     if (!tw_grid_max(t, sh, mx, parity, residual)) goto out;
     if (residual > a.tol) {
         // cell-order tables, r and p, and the tiles' level ranges
@@ -608,11 +640,11 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
             atomicMax(t.thi + tile, ii + jj + kk);
         }
         if (!tw_grid_sync(t, sh)) goto out;
-        if (!tw_sweep_all<TW_BUILD>(t, sh, epoch++, nlevels)) goto out;
+        if (!tw_sweep_all<TW_BUILD>(t, sh, nlevels)) goto out;
         if (!tw_grid_sync(t, sh)) goto out;  // the factor's exchange planes are reused by the sweeps
         TW_SECTION(0);
-        if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
-        if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
+        if (!tw_sweep_all<TW_FORWARD>(t, sh, nlevels)) goto out;
+        if (!tw_sweep_all<TW_BACKWARD>(t, sh, nlevels)) goto out;
         // dot(z, r)
         if (a.exact_dots) {
             if (!tw_exact_dot(t, sh, sigma)) goto out;
@@ -683,8 +715,8 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
             if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and rp.x
             TW_SECTION(5);
             if (residual <= a.tol) break;
-            if (!tw_sweep_all<TW_FORWARD>(t, sh, epoch++, nlevels)) goto out;
-            if (!tw_sweep_all<TW_BACKWARD>(t, sh, epoch++, nlevels)) goto out;
+            if (!tw_sweep_all<TW_FORWARD>(t, sh, nlevels)) goto out;
+            if (!tw_sweep_all<TW_BACKWARD>(t, sh, nlevels)) goto out;
             double sigma_new;  // dot(z, r)
             if (a.exact_dots) {
                 if (!tw_exact_dot(t, sh, sigma_new)) goto out;

@@ -453,16 +453,13 @@ struct sdr_solver {
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
     double* cl_slots = nullptr;     // CTA partials of the cluster kernels
     // whole-GPU tiled solve (k_pcg_tiles), allocated on first use
-    uint8_t* tw_exm = nullptr;
     uint32_t* tw_icm = nullptr;
     double2 *tw_rp = nullptr, *tw_qp = nullptr;
     double *tw_z = nullptr, *tw_exf = nullptr, *tw_exb = nullptr,
            *tw_slots = nullptr;
     int *tw_lo = nullptr, *tw_hi = nullptr;
-    unsigned long long* tw_flags = nullptr;
     unsigned* tw_bar = nullptr;
     int tw_tj = 0, tw_tk = 0, tw_grid = 0;  // tiles along y and z; CTAs of the cooperative launch (0: not set up)
-    unsigned long long tw_epoch = 1;        // next sweep epoch
     unsigned long long* rclaim = nullptr;  // per cell: claim stamps of the parallel redistribution replay
     sdr_profile prof{};
     uint64_t particle_substeps = 0, substeps_total = 0;
@@ -641,8 +638,8 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(tw_exm, st); dfree(tw_icm, st); dfree(tw_rp, st); dfree(tw_qp, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
-        dfree(tw_hi, st); dfree(tw_flags, st); dfree(tw_bar, st);
+        dfree(tw_icm, st); dfree(tw_rp, st); dfree(tw_qp, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
+        dfree(tw_hi, st); dfree(tw_bar, st);
         dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
         dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
@@ -925,10 +922,8 @@ struct sdr_solver {
         tw_tk = (g.nz + kTwK - 1) / kTwK;
         const size_t nt = (size_t)tw_tj * tw_tk, plane = (size_t)(kTwJ + kTwK) * g.nx;
         dalloc(tw_icm, ncell, st); dalloc(tw_rp, ncell, st); dalloc(tw_qp, ncell, st); dalloc(tw_z, ncell, st);
-        dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st); dalloc(tw_exm, nt * plane, st);
+        dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st);
         dalloc(tw_lo, nt, st); dalloc(tw_hi, nt, st);
-        dalloc(tw_flags, nt, st);
-        CK(cudaMemsetAsync(tw_flags, 0, nt * sizeof(unsigned long long), st));
         dalloc(tw_bar, 2, st);
         dalloc(tw_slots, 2 * (size_t)tw_grid, st);
         return true;
@@ -941,11 +936,8 @@ struct sdr_solver {
         t.tj = tw_tj; t.tk = tw_tk; t.ntiles = tw_tj * tw_tk;
         t.coff = coff;
         t.icm = tw_icm; t.rp = tw_rp; t.qp = tw_qp; t.z_c = tw_z;
-        t.exf = tw_exf; t.exb = tw_exb; t.exm = tw_exm;
+        t.exf = tw_exf; t.exb = tw_exb;
         t.tlo = tw_lo; t.thi = tw_hi;
-        t.flags = tw_flags;
-        t.epoch0 = tw_epoch;
-        tw_epoch += 2 * (unsigned long long)std::min<uint64_t>(max_iters, (uint64_t)INT32_MAX) + 8;
         t.bar = tw_bar;
         t.gslots = tw_slots;
         t.err = &dst->err;

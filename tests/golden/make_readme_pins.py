@@ -13,8 +13,11 @@ variant (optional) reruns the scene perturbed, to measure how far its chaotic
 summary moves on its own: "f32" rounds the particle state to f32 after every
 substep (the device's storage precision), "seed" starts the emission stream
 from another seed (0x9e3779b97f4a7c15). The result goes to the scene's
-"variants" entry.
+"variants" entry. "noredist" and "nosource" switch one physics option off
+(Solver::redistribute, solver.rs:454-557; the volume source, solver.rs:392-423)
+to see which of them moves the summary towards the README's figures.
 """
+import dataclasses
 import json
 import os
 import sys
@@ -44,6 +47,10 @@ def run(name: str, threads: int, variant: str = ""):
     if cfg.sinus["mesh"] is not None:
         cfg.sinus["mesh"] = os.path.join(REF, cfg.sinus["mesh"])
     res = cfg.resolve()
+    if variant == "noredist":
+        res = dataclasses.replace(res, fluid=dataclasses.replace(res.fluid, redistribute=False))
+    elif variant == "nosource":
+        res = dataclasses.replace(res, fluid=dataclasses.replace(res.fluid, volume_stiffness=0.0))
     tris = None if res.sinus is not None else sc.load_mesh(res.mesh_path) * sc.MM
     t0 = time.time()
     sdf = oracle_sdf(res, tris)

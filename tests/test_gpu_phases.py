@@ -392,14 +392,22 @@ SUB_PRESSURE_TOL = 1e-6  # pressure, relative to its largest value: the f32 face
 # (each a jump of about a cell). At most this fraction of the particles may do
 # so, each within two cells; every other particle holds the bounds above.
 SUB_BRANCH_FRACTION = 1e-5
+# PCG stops at the first iteration whose residual max-norm is below the
+# absolute tolerance (pressure.rs:377-380). Over a whole substep the device's
+# right-hand side comes from its f32 P2G faces and the oracle's from f64 faces
+# (~1e-7 relative apart), which can move that iteration by one where the
+# residual crosses the tolerance near the end (the 0.2 mm pool: 216 against
+# 217, pressure still within 1.2e-8). From identical faces the project phase
+# has equal iterations and identical pressure bits (test_project_*).
+SUB_ITERS_SLACK = 1
 
 
 def test_full_substep_shadow(pair):
     """One full substep from identical state, both in the reference dot order:
-    particle count, labels, drained count and PCG iterations exactly; the
-    pressure of every cell, and every particle's position and velocity but
-    for the redistribution branch flips described above, within the stated
-    bounds."""
+    particle count, labels and drained count exactly, PCG iterations within
+    one; the pressure of every cell, and every particle's position and
+    velocity but for the redistribution branch flips described above, within
+    the stated bounds."""
     gpu, orc, res, name = pair
     gpu_to_oracle(gpu, orc)
     sync_faces(gpu, orc)
@@ -430,7 +438,7 @@ def test_full_substep_shadow(pair):
     record(f"full_substep[{name}]", rec)
     assert len(pg) == len(po)
     assert gpu.drained == orc.scalars()["drained"]
-    assert rec["iters_gpu"] == rec["iters_orc"]
+    assert abs(rec["iters_gpu"] - rec["iters_orc"]) <= SUB_ITERS_SLACK
     assert np.array_equal(gpu.cells(), orc.cells())
     assert rec["pressure_rel_max"] < SUB_PRESSURE_TOL
     assert rec["branch_flips"] <= SUB_BRANCH_FRACTION * len(pg)
