@@ -504,6 +504,7 @@ struct RedistState {
     uint32_t nmoves_par;  // moves appended by k_redist_par this sweep
     uint32_t pad;
     unsigned long long rounds_total;  // decision rounds of long lists, all sweeps so far
+    uint32_t pend_n[2];               // entries of the two pending lists of k_redist_par's rounds
 };
 
 __device__ __forceinline__ void k_redist_hist_n_body(VB vb_, Grid g, const float4* __restrict__ pos, const uint32_t* __restrict__ n_dev,
@@ -566,9 +567,8 @@ struct RedistArgs {
     const int* key_cell;
     uint32_t* count;         // histogram at sweep start (the fallback path mutates it)
     const uint8_t* cavity;
-    uint32_t* cand;          // candidate particles (sorted in place when long)
+    uint32_t* cand;          // candidate particles (sorted in place when short, in append order when long)
     uint32_t cand_cap;
-    uint32_t* bitmap;        // long lists: scratch of ceil(n_upper / 32) words
     uint32_t n_upper;        // bound on the particle count (and on every candidate index)
     uint32_t cap;
     double down[6];          // dir . gdir for -x,+x,-y,+y,-z,+z (f64, solver.rs:490-511)
@@ -576,7 +576,8 @@ struct RedistArgs {
     RedistState* rs;
     unsigned long long* claim;  // per cell: the latest claim stamp (k_redist_par); zero at allocation
     int rounds;                 // short lists: parallel rounds (1) or one thread in index order (0)
-    double* slots;              // 2 x 16 doubles: CTA partials of k_redist_par's reductions
+    double* slots;              // unused by the rounds (kept for the launch layout)
+    uint32_t* pend;             // 2 x cand_cap: the rounds' pending candidate indices, double-buffered
 };
 
 // A move: the particle goes near the destination centre with its index-keyed
@@ -647,35 +648,9 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 __syncthreads();
             }
     } else {
-        // Long lists: mark the candidates in a bitmap over particle indices,
-        // then compact the bitmap in index order: O(n / 32 + candidates).
-        __shared__ uint32_t ssh[33];
-        const uint32_t nw = (a.n_upper + 31) >> 5;
-        for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) a.bitmap[t] = 0u;
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < nc; t += blockDim.x) {
-            uint32_t p = a.cand[t];
-            if (p < a.n_upper) atomicOr(&a.bitmap[p >> 5], 1u << (p & 31));
-        }
-        __syncthreads();
-        uint32_t base = 0;  // candidates written by earlier chunks (block-uniform)
-        for (uint32_t w0 = 0; w0 < nw; w0 += blockDim.x) {
-            const uint32_t w = w0 + threadIdx.x;
-            uint32_t bits = w < nw ? a.bitmap[w] : 0u;
-            uint32_t ex;
-            const uint32_t tot = block_exscan_u32((uint32_t)__popc(bits), ex, ssh);
-            uint32_t o = base + ex;
-            while (bits) {
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                if (o < nc) a.cand[o] = (w << 5) + (uint32_t)b;
-                ++o;
-            }
-            base += tot;
-        }
-        __syncthreads();
-        // The list is now in index order in a.cand: k_redist_par (the next
-        // launch) decides the moves in parallel rounds and applies them.
+        // Long lists go to k_redist_par (the next launch) in append order: its
+        // rounds order the candidates by particle index through their claim
+        // stamps, so the list needs no sort.
         if (threadIdx.x == 0) rs->par = 1;
         return;
     }
@@ -906,7 +881,8 @@ constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable *
 // are below the cap (changed only by candidates that may choose them); every
 // other neighbour is full or outside the cavity for the rest of the sweep.
 // Each round every pending candidate m claims its cell and each neighbour
-// still below the cap with a stamp that orders lower indices first; m runs
+// still below the cap with a stamp that orders lower particle indices first
+// (the list itself stays in append order); m runs
 // when it holds all its claims, i.e. when no lower pending candidate can
 // change what m reads or read what m changes. Those candidates run at once
 // (their cells are disjoint), which is the sequential result. Candidates whose
@@ -936,35 +912,8 @@ struct RpGrid {
     uint32_t* err;
 };
 
-// Sum over the team of per-thread values (the pending count, an integer, so
-// the order is free): CTA sums through a double-buffered slot array, read
-// back by one warp per CTA and handed to the CTA through shared memory (every
-// thread reading every slot put hundreds of thousands of loads a round on
-// the same few L2 lines).
-template <class Team>
-__device__ __forceinline__ double rp_team_sum(const Team& t, double v, int& parity, double* sh, bool& ok) {
-    double bs = block_sum<kRpBS>(v, sh);
-    double* sl = t.slots + parity * t.size();
-    parity ^= 1;
-    if (threadIdx.x == 0) sl[t.rank()] = bs;
-    ok = t.sync() && ok;
-    __shared__ double total;
-    if (threadIdx.x < 32) {
-        double s = 0.0;
-        for (int q = (int)threadIdx.x; q < t.size(); q += 32) s += __ldcg(sl + q);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) total = s;
-    }
-    __syncthreads();
-    const double s = total;
-    __syncthreads();  // `total` is rewritten by the next call
-    return s;
-}
-
 template <class Team>
 __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
-    __shared__ double sh[40];
     RedistState* rs = a.rs;
     if (!rs->active || !rs->par) return;  // written by earlier launches: the same in every CTA
     const int rank = team.rank(), nct = team.size();
@@ -974,6 +923,7 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
     const Grid& g = a.g;
     const int sxy = g.nx * g.ny;
     uint32_t base = rs->round_base;
+    if (rank == 0 && threadIdx.x == 0) rs->pend_n[0] = rs->pend_n[1] = 0u;
     ok = team.sync() && ok;  // every CTA has read the state before it changes
     if (base > 0xF0000000u) {  // stamps about to wrap: clear the claims and start again
         const size_t nce = (size_t)g.nx * g.ny * g.nz;
@@ -981,14 +931,20 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
         base = 0;
         ok = team.sync() && ok;
     }
-    int parity = 0;
+    // The candidates still pending after a round go to the other half of
+    // `pend` (any order: a claim's stamp carries the candidate's index), so a
+    // round touches only those; the first round takes every candidate.
+    const uint32_t* pa = nullptr;
+    uint32_t* pb = a.pend;
+    uint32_t na = nc;
     uint32_t round = 0;
-    bool done = nc == 0;
-    while (!done) {
+    while (na > 0 && ok) {
         ++round;
+        const int cur = (int)(round & 1u);
         const unsigned long long stamp = (unsigned long long)(base + round) << 32;
         // claims (or leave the list)
-        for (uint32_t m = gt; m < nc; m += G) {
+        for (uint32_t q = gt; q < na; q += G) {
+            const uint32_t m = pa ? pa[q] : q;
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
             const int c = a.key_cell[p];
@@ -999,11 +955,11 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / sxy;
             const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
                                j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
-            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - p);
             bool any = false;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const int n = nb[q];
+            for (int qq = 0; qq < 6; ++qq) {
+                const int n = nb[qq];
                 if (n >= 0 && a.cavity[n] && __ldcg(a.count + n) < cap) {
                     atomicMax(a.claim + n, key);
                     any = true;
@@ -1016,41 +972,42 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             atomicMax(a.claim + c, key);
         }
         ok = team.sync() && ok;
-        // candidates holding all their claims run (counts are as in the claim step)
-        double pending = 0.0;
-        for (uint32_t m = gt; m < nc; m += G) {
+        // candidates holding all their claims run (counts are as in the claim
+        // step); the others go on the next round's list
+        for (uint32_t q = gt; q < na; q += G) {
+            const uint32_t m = pa ? pa[q] : q;
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
             const int c = a.key_cell[p];
-            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
+            const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - p);
             const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / sxy;
             const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
                                j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
             uint32_t cnt[6];
             bool ready = __ldcg(a.claim + c) == key;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const int n = nb[q];
-                cnt[q] = 0xFFFFFFFFu;
+            for (int qq = 0; qq < 6; ++qq) {
+                const int n = nb[qq];
+                cnt[qq] = 0xFFFFFFFFu;
                 if (n >= 0 && a.cavity[n]) {
-                    cnt[q] = __ldcg(a.count + n);
-                    if (cnt[q] < cap && __ldcg(a.claim + n) != key) ready = false;
+                    cnt[qq] = __ldcg(a.count + n);
+                    if (cnt[qq] < cap && __ldcg(a.claim + n) != key) ready = false;
                 }
             }
             if (!ready) {
-                pending += 1.0;
+                pb[atomicAdd(&rs->pend_n[cur], 1u)] = m;
                 continue;
             }
             int best = -1;
             double best_down = -INFINITY;
             uint32_t best_room = 0;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
-                if (cnt[q] >= cap) continue;  // full, outside the cavity, or out of bounds
-                const uint32_t room = cap - cnt[q];
-                const double dn = a.down[q];
+            for (int qq = 0; qq < 6; ++qq) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
+                if (cnt[qq] >= cap) continue;  // full, outside the cavity, or out of bounds
+                const uint32_t room = cap - cnt[qq];
+                const double dn = a.down[qq];
                 if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                    best = nb[q];
+                    best = nb[qq];
                     best_down = dn;
                     best_room = room;
                 }
@@ -1066,10 +1023,16 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             a.moves[2 * slot + 1] = (uint32_t)best;
             a.cand[m] = p | kResolved;
         }
-        done = rp_team_sum(team, pending, parity, sh, ok) == 0.0 || !ok;
-        if (!done && round > nc) {  // cannot happen: the lowest pending candidate always runs
+        ok = team.sync() && ok;
+        na = __ldcg(&rs->pend_n[cur]);
+        // the other counter was last read after the previous round: clear it
+        // for the next round's appends (ordered before them by its first barrier)
+        if (rank == 0 && threadIdx.x == 0) rs->pend_n[cur ^ 1] = 0u;
+        pa = pb;
+        pb = (pb == a.pend) ? a.pend + a.cand_cap : a.pend;
+        if (na > 0 && round > nc) {  // cannot happen: the lowest pending candidate always runs
             if (rank == 0 && threadIdx.x == 0) atomicOr(&rs->err, 4u);
-            done = true;
+            break;
         }
     }
     const uint32_t nm = __ldcg(&rs->nmoves_par);

@@ -417,6 +417,7 @@ struct sdr_solver {
     int4 *frec = nullptr, *brec = nullptr;
     // redistribution
     uint32_t* cand = nullptr;
+    uint32_t* rpend = nullptr;  // 2 x cand_n: pending candidates of the long-list rounds
     size_t cand_n = 0;      // entries of `cand`
     size_t cand_limit = 0;  // sdr_solver_set_candidate_capacity (0: the particle capacity)
     uint32_t* moves = nullptr;
@@ -569,6 +570,7 @@ struct sdr_solver {
         dalloc(drn, ncap, st);
         cand_n = cand_limit ? std::min(ncap, cand_limit) : ncap;
         dalloc(cand, cand_n, st);
+        dalloc(rpend, 2 * cand_n, st);
         dalloc(moves, ncap * 2, st);
         dalloc(lrec, ncap, st);
         dalloc(vrec, ncap, st);
@@ -642,7 +644,7 @@ struct sdr_solver {
         dfree(tw_hi, st); dfree(tw_bar, st);
         dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
-        dfree(cand, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
+        dfree(cand, st); dfree(rpend, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
         if (hst) hput(hst, 1);
         if (h_epos) hput(h_epos, h_ecap);
@@ -1031,11 +1033,11 @@ struct sdr_solver {
         ra.cavity = cavity;
         ra.cand = cand;
         ra.cand_cap = (uint32_t)cand_n;
-        ra.bitmap = ptmp;  // free between the sort of one substep and the next
         ra.n_upper = n_upper;
         ra.claim = rclaim;
         ra.rounds = shared_gpu ? 0 : 1;  // many scenes: spend no SM time on rounds
         ra.slots = cl_slots;
+        ra.pend = rpend;
         // A GPU of its own: long lists over every SM. On a shared GPU one CTA:
         // a cluster launch waits for a whole GPC of free SMs, which other
         // scenes' solves rarely leave.
@@ -1580,6 +1582,7 @@ int sdr_solver_set_candidate_capacity(sdr_solver* s, uint64_t candidates) {
         s->cand_limit = (size_t)candidates;
         s->cand_n = s->cand_limit ? std::min(s->cap, s->cand_limit) : s->cap;
         dalloc(s->cand, s->cand_n, s->st);
+        dalloc(s->rpend, 2 * s->cand_n, s->st);
         CK(cudaStreamSynchronize(s->st));
     });
 }
