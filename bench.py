@@ -43,6 +43,12 @@ Extra records on one GPU:
 ``render``         preview images (600 px) of the cavity run's final state
                    beside the oracle drawing the same state.
 
+``--batched-full`` runs only the batched family at full duration instead:
+128 scenes for 0.6 s each, all at once (stream per scene and packed) against a
+seeded plain sample of 8 of them, then 64 Poisson requests (90 % family, 10 %
+the real-cavity scene) into both request servers against a plain sample of
+the requests; it prints its own line (scenes/s).
+
 Multi-GPU runs are independent replicas (one pool per rank): no collective on
 the data path; a barrier and a max-reduce of the timings use torch.distributed.
 """
@@ -479,6 +485,81 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
     }
 
 
+def batched_full(n_scenes: int = 128, n_plain: int = 8, n_requests: int = 64, seed0: int = 100) -> dict:
+    """The batched family at full duration (0.6 s, 18 frames per scene).
+
+    Batched: all n_scenes at once, one stream and solver each and packed into
+    one launch per substep operation. Plain: a seeded sample of n_plain of the
+    same scenes one after another on default solvers (the whole family on the
+    plain path would take about an hour); its time for all n_scenes is
+    estimated as the sample's time x n_scenes / n_plain, and the sampled
+    scenes' summaries must equal their batched ones. Served: n_requests
+    Poisson arrivals, 90 % drawn from the family (new seeds) and 10 % the
+    real-cavity scene (0.5 mm, 1 ml), into both request servers at 80 % of the
+    better batched rate, against a plain sample of the same requests."""
+    import math
+    import random
+
+    from sdr_b200 import _lib, workloads
+    from sdr_b200.serving import run_batch
+    t0 = time.perf_counter()
+    specs = [workloads.scene_spec(workloads.batch_scene(seed0 + i)) for i in range(n_scenes)]
+    build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    mix = run_batch(specs, concurrency=0)
+    t_mix = time.perf_counter() - t0
+    cnt = {}
+    t0 = time.perf_counter()
+    packed = run_batch(specs, packed=True, counters=cnt)
+    t_packed = time.perf_counter() - t0
+    rng = random.Random(seed0)
+    idx = sorted(rng.sample(range(n_scenes), n_plain))
+    t0 = time.perf_counter()
+    plain = run_batch([specs[i] for i in idx], concurrency=1)
+    t_plain_sample = time.perf_counter() - t0
+    ok = all(r.status == _lib.SDR_OK for r in mix + packed + plain)
+    same = ok and all(mix[i].summary == packed[i].summary for i in range(n_scenes)) and \
+        all(p.summary == mix[i].summary for p, i in zip(plain, idx))
+    subs = sum(r.stats["substeps_total"] for r in packed) if ok else 0
+    t_plain_est = t_plain_sample * n_scenes / n_plain
+    out = {"scenes": n_scenes, "frames_per_scene": 18, "duration_s": 0.6, "substeps": subs,
+           "sdf_build_s": build_s,
+           "streams_scenes_per_s": n_scenes / t_mix, "streams_s": t_mix,
+           "packed_scenes_per_s": n_scenes / t_packed, "packed_s": t_packed, "packed_counters": cnt,
+           "plain_sample": idx, "plain_sample_s": t_plain_sample, "plain_scenes_per_s": n_plain / t_plain_sample,
+           "plain_estimated_s": t_plain_est,
+           "speedup_streams": t_plain_est / t_mix, "speedup_packed": t_plain_est / t_packed,
+           "results_identical": same}
+    # serving: Poisson arrivals, 90 % family scenes and 10 % the real-cavity scene
+    rq = random.Random(seed0 + 1)
+    reqs = []
+    for q in range(n_requests):
+        if rq.random() < 0.1:
+            reqs.append(workloads.scene_spec(workloads.real_cavity(seed=2 + q)))
+        else:
+            reqs.append(workloads.scene_spec(workloads.batch_scene(seed0 + 1000 + q)))
+    rate = 0.8 * n_scenes / min(t_mix, t_packed)
+    pidx = sorted(rq.sample(range(n_requests), max(1, n_requests // 10)))
+    t0 = time.perf_counter()
+    pref = run_batch([reqs[i] for i in pidx], concurrency=1)
+    t_pref = time.perf_counter() - t0
+    srv = {"requests": n_requests, "mix": "90 % batched family, 10 % real cavity 0.5 mm", "rate_per_s": rate,
+           "plain_sample": pidx, "plain_sample_s": t_pref, "plain_scenes_per_s": len(pidx) / t_pref}
+    for packed_mode in (False, True):
+        res, t_srv, sst = _serve(reqs, rate, seed0, packed_mode)
+        lat = sorted(r.seconds for r in res)
+
+        def pct(q):
+            return lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+        key = "packed" if packed_mode else "streams"
+        srv[key] = {"scenes_per_s": n_requests / t_srv, "p50_time_to_summary_s": pct(0.5),
+                    "p99_time_to_summary_s": pct(0.99), "peak_active": sst["peak_active"],
+                    "peak_bytes": sst["peak_bytes"],
+                    "results_identical": all(r.status == _lib.REQ_DONE for r in res) and
+                    all(res[i].summary == p.summary for p, i in zip(pref, pidx))}
+    return {"batched_full": out, "served_full": srv}
+
+
 def render_bench(solver, w, sdf, cpu: bool, px: int = 600, reps: int = 5) -> dict:
     """Preview images (render_slice) of the solver's current state: the slice
     through the needle tip (speed dots) and the gravity projection (amber
@@ -521,6 +602,8 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=48)
     ap.add_argument("--batch-cfl", type=int, default=150)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batched-full", action="store_true",
+                    help="only the batched family at full duration and the serving mix (about 25 minutes)")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -531,6 +614,13 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.batched_full:
+        if rank == 0:
+            rec = batched_full()
+            print(json.dumps({"metric": "scenes/s", "value": rec["batched_full"]["packed_scenes_per_s"],
+                              "unit": "scenes/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+                              "config": {"workload": "batched family x128 at 0.6 s; serving mix"}, **rec}))
+        return
     if world > 1:
         import datetime
         import torch.distributed as dist

@@ -890,11 +890,13 @@ constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable *
 // again and leave the list. The lowest pending candidate always runs, so the
 // rounds end; a bound on them still records an error bit if they did not.
 constexpr int kRpBS = 512;
+constexpr uint32_t kRpSoloList = 4 * kRpBS;  // pending candidates CTA 0 decides alone on the grid form
 
 // The CTAs that decide one long list: one thread-block cluster (barrier in
 // hardware), or every CTA of a cooperative launch (a bounded grid barrier;
 // false if it gave up, with an error bit set).
 struct RpCluster {
+    static constexpr bool kGrid = false;
     __device__ int rank() const { return (int)cluster_rank(); }
     __device__ int size() const { return (int)cluster_size(); }
     __device__ bool sync() const {
@@ -904,6 +906,7 @@ struct RpCluster {
     double* slots;  // 2 x 16
 };
 struct RpGrid {
+    static constexpr bool kGrid = true;
     __device__ int rank() const { return (int)blockIdx.x; }
     __device__ int size() const { return (int)gridDim.x; }
     __device__ bool sync() const { return grid_sync_bounded(bar, err, kErrGridWait); }
@@ -933,17 +936,27 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
     }
     // The candidates still pending after a round go to the other half of
     // `pend` (any order: a claim's stamp carries the candidate's index), so a
-    // round touches only those; the first round takes every candidate.
+    // round touches only those; the first round takes every candidate. On the
+    // whole grid, once few remain CTA 0 decides them alone (block barriers
+    // instead of grid barriers) while the others wait at the barrier below.
     const uint32_t* pa = nullptr;
     uint32_t* pb = a.pend;
     uint32_t na = nc;
     uint32_t round = 0;
+    bool solo = false;
+    uint32_t gt_ = gt, G_ = G;
     while (na > 0 && ok) {
+        if (Team::kGrid && !solo && na <= kRpSoloList) {  // the same decision in every CTA
+            solo = true;
+            if (rank != 0) break;
+            gt_ = threadIdx.x;
+            G_ = kRpBS;
+        }
         ++round;
         const int cur = (int)(round & 1u);
         const unsigned long long stamp = (unsigned long long)(base + round) << 32;
         // claims (or leave the list)
-        for (uint32_t q = gt; q < na; q += G) {
+        for (uint32_t q = gt_; q < na; q += G_) {
             const uint32_t m = pa ? pa[q] : q;
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
@@ -971,10 +984,11 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             }
             atomicMax(a.claim + c, key);
         }
-        ok = team.sync() && ok;
+        if (solo) __syncthreads();
+        else ok = team.sync() && ok;
         // candidates holding all their claims run (counts are as in the claim
         // step); the others go on the next round's list
-        for (uint32_t q = gt; q < na; q += G) {
+        for (uint32_t q = gt_; q < na; q += G_) {
             const uint32_t m = pa ? pa[q] : q;
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
@@ -1023,7 +1037,8 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             a.moves[2 * slot + 1] = (uint32_t)best;
             a.cand[m] = p | kResolved;
         }
-        ok = team.sync() && ok;
+        if (solo) __syncthreads();
+        else ok = team.sync() && ok;
         na = __ldcg(&rs->pend_n[cur]);
         // the other counter was last read after the previous round: clear it
         // for the next round's appends (ordered before them by its first barrier)
@@ -1035,6 +1050,7 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             break;
         }
     }
+    if (solo) ok = team.sync() && ok;  // CTA 0 arrives once its rounds are done
     const uint32_t nm = __ldcg(&rs->nmoves_par);
     for (uint32_t mv = gt; mv < nm; mv += G) redist_apply_move(a, a.moves[2 * mv], a.moves[2 * mv + 1]);
     ok = team.sync() && ok;
