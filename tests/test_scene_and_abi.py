@@ -89,6 +89,23 @@ def test_readme_pins():
     assert abs(s["total_drained_ml"] - 8.11) / 8.11 < 0.03
 
 
+def test_readme_coverage_gap_is_frame_sampling():
+    """The wall coverage of examples/scene.toml (oracle 67.5 % against the
+    README's 59.1 %): the "walls" rerun of make_readme_pins.py reproduces the
+    collector's coverage from the recorded cells under metrics.rs:133-170's
+    wall (the bisect is self-consistent), other wall definitions raise it, and
+    sampling washed cells at every 6th frame end (10 frames over the 2 s
+    instead of 60) brings it within 1.5 points of the README."""
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "readme_pins.json")))["scene"]
+    w = d["variants"]["walls"]
+    cov = w["coverage_by_wall_definition"]
+    assert cov["reference"] == w["summary"]["peak_wall_coverage"]
+    assert cov["contact_26"] > cov["reference"] and cov["two_cells_deep"] > cov["reference"]
+    assert cov["reference_every_2_frames"] >= cov["reference_every_3_frames"] >= cov["reference_every_6_frames"]
+    assert abs(cov["reference_every_6_frames"] - 0.591) < 0.015
+    assert abs(cov["reference"] - 0.591) > 0.05  # every frame end: the gap the bisect explains
+
+
 def test_new_entry_points_reject_bad_arguments_without_a_device():
     """Null handles and out-of-range values fail cleanly with SDR_ERR_INVALID
     and a message, before any device work."""
