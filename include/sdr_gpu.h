@@ -243,10 +243,12 @@ int sdr_solver_set_dot_order(sdr_solver* s, int reference_order);
  * reference's). SDR_PCG_TILES: the whole GPU in one cooperative launch; the
  * grid's (j, k) lines cut into tiles of 16 x 16, one CTA per tile walking the
  * levels of its cells, tiles handing boundary values to their neighbours
- * through progress counters (large fluid regions on a GPU of their own; the
- * cluster kernel if the device cannot launch it). SDR_PCG_AUTO (default):
- * from 200,000 fluid cells in the previous solve the tiled solve, or the
- * cluster with SDR_SOLVER_SHARED_GPU; below that one block. */
+ * through exchange entries that mark their own readiness (large fluid regions
+ * on a GPU of their own; the cluster kernel if the device cannot launch it).
+ * SDR_PCG_AUTO (default): from 200,000 fluid cells in the previous solve
+ * (before the first solve: the particle count over particles_per_cell) the
+ * tiled solve, or the cluster with SDR_SOLVER_SHARED_GPU; below that one
+ * block. */
 enum { SDR_PCG_AUTO = 0, SDR_PCG_ONE_BLOCK = 1, SDR_PCG_CLUSTER = 2, SDR_PCG_TILES = 3 };
 int sdr_solver_set_pcg_kernel(sdr_solver* s, int kernel);
 /* CTAs of the SDR_PCG_ONE_BLOCK solve's cluster (CTA 0 runs the sweeps).
