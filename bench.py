@@ -44,10 +44,11 @@ Extra records on one GPU:
                    beside the oracle drawing the same state.
 
 ``--batched-full`` runs only the batched family at full duration instead:
-128 scenes for 0.6 s each, all at once (stream per scene and packed) against a
-seeded plain sample of 8 of them, then 64 Poisson requests (90 % family, 10 %
-the real-cavity scene) into both request servers against a plain sample of
-the requests; it prints its own line (scenes/s).
+128 scenes for 0.6 s each, all at once (packed, then stream per scene) against
+a seeded plain sample of 8 of them, then 32 Poisson requests (90 % family,
+10 % the real-cavity scene) into both request servers against a plain sample
+of the requests; each phase prints a line as it ends, then the summary line
+(scenes/s).
 
 Multi-GPU runs are independent replicas (one pool per rank): no collective on
 the data path; a barrier and a max-reduce of the timings use torch.distributed.
@@ -485,52 +486,60 @@ def batch_bench(n_scenes: int, cfl_steps: int, seed0: int = 100) -> dict:
     }
 
 
-def batched_full(n_scenes: int = 128, n_plain: int = 8, n_requests: int = 64, seed0: int = 100) -> dict:
+def batched_full(n_scenes: int = 128, n_plain: int = 8, n_requests: int = 32, seed0: int = 100) -> dict:
     """The batched family at full duration (0.6 s, 18 frames per scene).
 
-    Batched: all n_scenes at once, one stream and solver each and packed into
-    one launch per substep operation. Plain: a seeded sample of n_plain of the
-    same scenes one after another on default solvers (the whole family on the
-    plain path would take about an hour); its time for all n_scenes is
-    estimated as the sample's time x n_scenes / n_plain, and the sampled
-    scenes' summaries must equal their batched ones. Served: n_requests
-    Poisson arrivals, 90 % drawn from the family (new seeds) and 10 % the
-    real-cavity scene (0.5 mm, 1 ml), into both request servers at 80 % of the
-    better batched rate, against a plain sample of the same requests."""
-    import math
+    Packed (one launch per substep operation for all scenes) and then one
+    stream and solver per scene, all n_scenes at once. Plain: a seeded sample
+    of n_plain of the same scenes one after another on default solvers (the
+    whole family on the plain path would take about an hour); its time for all
+    n_scenes is estimated as the sample's time x n_scenes / n_plain, and the
+    sampled scenes' summaries must equal their batched ones. Served:
+    n_requests Poisson arrivals, 90 % drawn from the family (new seeds) and
+    10 % the real-cavity scene (0.5 mm, 1 ml), into both request servers at 80 %
+    of the packed rate, against a plain sample of the same requests. Each phase
+    prints a line ("phase": ...) as it ends."""
     import random
 
     from sdr_b200 import _lib, workloads
     from sdr_b200.serving import run_batch
+
+    def say(**kw):
+        print(json.dumps(kw), flush=True)
     t0 = time.perf_counter()
     specs = [workloads.scene_spec(workloads.batch_scene(seed0 + i)) for i in range(n_scenes)]
     build_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    mix = run_batch(specs, concurrency=0)
-    t_mix = time.perf_counter() - t0
     cnt = {}
     t0 = time.perf_counter()
     packed = run_batch(specs, packed=True, counters=cnt)
     t_packed = time.perf_counter() - t0
+    ok = all(r.status == _lib.SDR_OK for r in packed)
+    subs = sum(r.stats["substeps_total"] for r in packed) if ok else 0
+    say(phase="packed", scenes=n_scenes, seconds=t_packed, scenes_per_s=n_scenes / t_packed, substeps=subs,
+        counters=cnt, ok=ok)
     rng = random.Random(seed0)
     idx = sorted(rng.sample(range(n_scenes), n_plain))
     t0 = time.perf_counter()
     plain = run_batch([specs[i] for i in idx], concurrency=1)
     t_plain_sample = time.perf_counter() - t0
-    ok = all(r.status == _lib.SDR_OK for r in mix + packed + plain)
-    same = ok and all(mix[i].summary == packed[i].summary for i in range(n_scenes)) and \
-        all(p.summary == mix[i].summary for p, i in zip(plain, idx))
-    subs = sum(r.stats["substeps_total"] for r in packed) if ok else 0
     t_plain_est = t_plain_sample * n_scenes / n_plain
-    out = {"scenes": n_scenes, "frames_per_scene": 18, "duration_s": 0.6, "substeps": subs,
-           "sdf_build_s": build_s,
-           "streams_scenes_per_s": n_scenes / t_mix, "streams_s": t_mix,
+    same_plain = all(r.status == _lib.SDR_OK for r in plain) and \
+        all(p.summary == packed[i].summary for p, i in zip(plain, idx))
+    say(phase="plain_sample", sample=idx, seconds=t_plain_sample, estimated_all_s=t_plain_est,
+        results_identical=same_plain)
+    t0 = time.perf_counter()
+    mix = run_batch(specs, concurrency=0)
+    t_mix = time.perf_counter() - t0
+    same_mix = all(r.status == _lib.SDR_OK for r in mix) and \
+        all(mix[i].summary == packed[i].summary for i in range(n_scenes))
+    say(phase="streams", seconds=t_mix, scenes_per_s=n_scenes / t_mix, results_identical=same_mix)
+    out = {"scenes": n_scenes, "frames_per_scene": 18, "duration_s": 0.6, "substeps": subs, "sdf_build_s": build_s,
            "packed_scenes_per_s": n_scenes / t_packed, "packed_s": t_packed, "packed_counters": cnt,
+           "streams_scenes_per_s": n_scenes / t_mix, "streams_s": t_mix,
            "plain_sample": idx, "plain_sample_s": t_plain_sample, "plain_scenes_per_s": n_plain / t_plain_sample,
            "plain_estimated_s": t_plain_est,
-           "speedup_streams": t_plain_est / t_mix, "speedup_packed": t_plain_est / t_packed,
-           "results_identical": same}
-    # serving: Poisson arrivals, 90 % family scenes and 10 % the real-cavity scene
+           "speedup_packed": t_plain_est / t_packed, "speedup_streams": t_plain_est / t_mix,
+           "results_identical": ok and same_plain and same_mix}
     rq = random.Random(seed0 + 1)
     reqs = []
     for q in range(n_requests):
@@ -538,14 +547,15 @@ def batched_full(n_scenes: int = 128, n_plain: int = 8, n_requests: int = 64, se
             reqs.append(workloads.scene_spec(workloads.real_cavity(seed=2 + q)))
         else:
             reqs.append(workloads.scene_spec(workloads.batch_scene(seed0 + 1000 + q)))
-    rate = 0.8 * n_scenes / min(t_mix, t_packed)
-    pidx = sorted(rq.sample(range(n_requests), max(1, n_requests // 10)))
+    rate = 0.8 * n_scenes / t_packed
+    pidx = sorted(rq.sample(range(n_requests), max(1, n_requests // 8)))
     t0 = time.perf_counter()
     pref = run_batch([reqs[i] for i in pidx], concurrency=1)
     t_pref = time.perf_counter() - t0
     srv = {"requests": n_requests, "mix": "90 % batched family, 10 % real cavity 0.5 mm", "rate_per_s": rate,
            "plain_sample": pidx, "plain_sample_s": t_pref, "plain_scenes_per_s": len(pidx) / t_pref}
-    for packed_mode in (False, True):
+    say(phase="served_plain_sample", **srv)
+    for packed_mode in (True, False):
         res, t_srv, sst = _serve(reqs, rate, seed0, packed_mode)
         lat = sorted(r.seconds for r in res)
 
@@ -557,6 +567,7 @@ def batched_full(n_scenes: int = 128, n_plain: int = 8, n_requests: int = 64, se
                     "peak_bytes": sst["peak_bytes"],
                     "results_identical": all(r.status == _lib.REQ_DONE for r in res) and
                     all(res[i].summary == p.summary for p, i in zip(pref, pidx))}
+        say(phase="served_" + key, **srv[key])
     return {"batched_full": out, "served_full": srv}
 
 
@@ -603,7 +614,9 @@ def main():
     ap.add_argument("--batch-cfl", type=int, default=150)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batched-full", action="store_true",
-                    help="only the batched family at full duration and the serving mix (about 25 minutes)")
+                    help="only the batched family at full duration and the serving mix (tens of minutes)")
+    ap.add_argument("--full-scenes", type=int, default=128, help="scenes of --batched-full")
+    ap.add_argument("--full-requests", type=int, default=32, help="served requests of --batched-full")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -616,10 +629,11 @@ def main():
     torch.cuda.set_device(local)
     if args.batched_full:
         if rank == 0:
-            rec = batched_full()
+            rec = batched_full(args.full_scenes, max(1, min(8, args.full_scenes // 16)), args.full_requests)
             print(json.dumps({"metric": "scenes/s", "value": rec["batched_full"]["packed_scenes_per_s"],
                               "unit": "scenes/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
-                              "config": {"workload": "batched family x128 at 0.6 s; serving mix"}, **rec}))
+                              "config": {"workload": f"batched family x{args.full_scenes} at 0.6 s; serving mix"},
+                              **rec}))
         return
     if world > 1:
         import datetime

@@ -10,8 +10,8 @@
 // memory, double-buffered by level), or, on the tile's low faces, cells of
 // the neighbouring tiles. So a level costs one barrier of the tile's threads,
 // and tiles synchronise only with their two upstream neighbours through
-// per-tile progress counters: a tile runs as soon as its neighbours are one
-// level ahead, and a sweep takes about (levels x the level step) + (tile hops
+// exchange entries that mark their own readiness: a tile runs as soon as its
+// neighbours are one level ahead, and a sweep takes about (levels x the level step) + (tile hops
 // x the hand-off latency) instead of one grid-wide barrier per level. The
 // backward sweep mirrors it (tiles wait on their +y / +z neighbours, levels in
 // decreasing order).
@@ -19,20 +19,22 @@
 // Per cell the arithmetic is that of k_pcg / k_pcg_cluster (the same operands
 // in the same order), so the factor and both sweeps give the same bits, and so
 // does the solve: the matvec, the updates and the dots run in the wavefront
-// order and tiling of the other kernels, spread over the grid. The sweeps work
-// in cell order (a line's fluid cells are contiguous there); the residual is
-// copied into cell order by the update phase and z is read back through the
-// cell-order map. Each compute thread keeps the operands of its line's next
-// kTwDepth cells in flight to shared memory (cp.async), so a level's step
-// never waits on a global load.
+// order and tiling of the other kernels, spread over the grid. The sweeps'
+// operands live in rows: per tile one row of kTwLines entries per level of its
+// range, so the lines of a level are contiguous and every copy and store of a
+// level is coalesced (the lines' cells lie some 70 cells apart in cell order,
+// which made each warp access touch 32 cache lines). The update phase writes
+// the residual into the rows and the dots read z back through the wavefront
+// index -> row map. Each compute thread keeps its next kTwDepth levels'
+// operands in flight to shared memory (cp.async), so a level's step never
+// waits on a global load.
 //
 // Synchronisation: one cooperative launch (every CTA resident). Phases are
 // separated by a grid barrier (an arrival counter and a generation word,
 // release/acquire at GPU scope). In a sweep the 8 compute warps of a CTA share
-// a named barrier per level; a ninth warp publishes the tile's progress
-// (release), polls the neighbours' (acquire), and copies the neighbours'
-// boundary values of completed levels into a shared-memory ring, so compute
-// threads never wait on a global load. Every wait gives up after about a
+// a named barrier per level; a ninth warp polls the upstream tiles' exchange
+// entries and copies their boundary values into a shared-memory ring, so
+// compute threads never wait on a global load. Every wait gives up after about a
 // second (2^31 SM cycles) or as soon as another CTA has given up, sets an
 // error bit and lets the kernel wind down.
 #pragma once
@@ -49,16 +51,25 @@ constexpr int kTwRing = 32;                  // levels of neighbour boundary val
 constexpr int kTwDepth = 6;                  // cells of each line whose operands are in flight to shared memory
 constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
 constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
+constexpr uint32_t kTwNoCell = 0xFFFFFFFFu;  // a row entry without a fluid cell
 
 struct TwArgs {
     PcgArgs a;                   // wavefront-order vectors, tables and dots (as k_pcg)
     int nx, ny, nz;
     int tj, tk, ntiles;          // tiles along y and z
     const uint32_t* coff;        // dense cell -> cell-order index of its fluid cell (exclusive scan, ncell + 1)
-    uint32_t* icm;               // cell order: i | fluid-neighbour bits (NB_*) << 16 | non-solid count << 24
-    double2* rp;                 // cell order: (residual, MIC(0) factor), the forward sweep's operands
-    double2* qp;                 // cell order: (forward sweep result, MIC(0) factor), the backward sweep's
-    double* z_c;                 // cell order: backward sweep result
+    uint32_t* icm_c;             // cell order: i | fluid-neighbour bits (NB_*) << 16 | non-solid count << 24
+    // The sweeps' operands in rows: per tile, one row of kTwLines entries per
+    // level of its range (entry = rbase[tile] + (L - tlo[tile]) * kTwLines +
+    // line), so the lines of a level are contiguous and every access of a
+    // level is coalesced. Entries without a fluid cell hold kTwNoCell in icm.
+    uint32_t* icm;               // rows: the (i, mask, count) word, or kTwNoCell
+    double2* rp;                 // rows: (residual, MIC(0) factor), the forward sweep's operands
+    double2* qp;                 // rows: (forward sweep result, MIC(0) factor), the backward sweep's
+    double* zr;                  // rows: backward sweep result
+    uint32_t* tpos;              // wavefront index -> row entry of its cell
+    uint32_t* rbase;             // per tile: its first row entry (ntiles + 1 entries)
+    size_t rows_cap;             // row entries allocated
     double* exf;                 // forward exchange planes: per tile [kTwK][nx] (+y face) then [kTwJ][nx] (+z face)
     double* exb;                 // backward exchange planes: the -y and -z faces
     int* tlo;                    // per tile: first and last level of its fluid cells
@@ -308,7 +319,7 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
                     if (need[u]) {
                         const size_t d = ((size_t)kp * t.ny + jp) * (size_t)nx + i;
                         const uint32_t c0 = __ldcg(t.coff + d), c1 = __ldcg(t.coff + d + 1);
-                        if (c1 != c0) m = (uint8_t)(__ldcg(t.icm + c0) >> 16);
+                        if (c1 != c0) m = (uint8_t)(__ldcg(t.icm_c + c0) >> 16);
                     }
                     sh.ringm[face][sq % kTwRing][l] = m;
                 }
@@ -349,18 +360,18 @@ __device__ __forceinline__ void tw_wait(const TwArgs& t, TwShared& sh, int which
     }
 }
 
-// Operands of a line's o-th cell in sweep order into its shared-memory slot
-// (o mod kTwDepth), as one cp.async group: the (i, mask, count) word, and for
-// the solves the 16-byte (r, factor) or (q, factor) record through L2 (r is
-// written by other CTAs in the update phase). Cells past the line's end
-// commit an empty group, so every level commits exactly one.
+// Operands of this line's entry of the q-th level of the sweep into shared
+// slot q mod kTwDepth, as one cp.async group: the (i, mask, count) word, and
+// for the solves the 16-byte (r, factor) or (q, factor) record through L2 (r
+// is written by other CTAs in the update phase). The row layout makes each of
+// a warp's copies one contiguous stretch. Levels past the sweep's end commit
+// an empty group, so every level commits exactly one.
 template <int MODE>
-__device__ __forceinline__ void tw_stage(const TwArgs& t, TwShared& sh, int tid, int first, int step, int count, int o) {
-    if (o < count) {
-        const int c = first + step * o;
-        const int slot = o % kTwDepth;
-        cp_async4(&sh.icm[slot][tid], t.icm + c);
-        if (MODE != TW_BUILD) cp_async16(&sh.rec[slot][tid], (MODE == TW_FORWARD ? t.rp : t.qp) + c);
+__device__ __forceinline__ void tw_stage(const TwArgs& t, TwShared& sh, int tid, size_t e, bool live, int q) {
+    if (live) {
+        const int slot = q % kTwDepth;
+        cp_async4(&sh.icm[slot][tid], t.icm + e);
+        if (MODE != TW_BUILD) cp_async16(&sh.rec[slot][tid], (MODE == TW_FORWARD ? t.rp : t.qp) + e);
     }
     cp_commit();
 }
@@ -393,12 +404,6 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     const int lj = tid % kTwJ, lk = tid / kTwJ;
     const int j = J * kTwJ + lj, k = K * kTwK + lk;
     const int nx = t.nx;
-    uint32_t beg = 0, end = 0;
-    if (j < t.ny && k < t.nz) {
-        const size_t d = ((size_t)k * t.ny + j) * (size_t)nx;
-        beg = __ldcg(t.coff + d);
-        end = __ldcg(t.coff + d + nx);
-    }
     const int jk = j + k;
     const size_t plane = (size_t)(kTwJ + kTwK) * nx;
     double* ex_own = (fwd ? t.exf : t.exb) + (size_t)tile * plane;
@@ -409,20 +414,17 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     double* const ex_y = in_grid && (fwd ? lj == kTwJ - 1 : lj == 0) ? ex_own + (size_t)lk * nx : nullptr;
     double* const ex_z = in_grid && (fwd ? lk == kTwK - 1 : lk == 0) ? ex_own + (size_t)kTwK * nx + (size_t)lj * nx
                                                                       : nullptr;
-    // This line's cells in sweep order, ordinals 0 .. count-1. The operands of
-    // the next kTwDepth cells are in flight to shared memory at all times:
-    // consuming ordinal o stages o + kTwDepth, one cp.async group per level.
-    // A cell is consumed at least one level after its predecessor, so when
-    // ordinal o is read the group that staged it has at least kTwDepth - 1
-    // groups after it, and waiting until kTwDepth - 1 are pending suffices.
-    const int step = fwd ? 1 : -1;
-    const int first = fwd ? (int)beg : (int)end - 1;
-    const int count = (int)(end - beg);
-    for (int o = 0; o < kTwDepth; ++o) tw_stage<MODE>(t, sh, tid, first, step, count, o);
-    int ord = 0;       // next cell to consume
-    int cur = first;   // its cell-order index
-    int L0 = -1;       // its level (-1: none left)
-    bool fresh = true; // L0 is still to be read from the slot of `ord`
+    // This line's row entries, level q of the sweep (q = s - s_first) at
+    // row0 + (fwd ? q : nlev - 1 - q) * kTwLines + tid. The operands of the
+    // next kTwDepth levels are in flight to shared memory at all times: level
+    // q stages q + kTwDepth, one cp.async group per level, so when level q is
+    // read the group that staged it has kTwDepth - 1 groups after it.
+    const int nlev = s_last - s_first + 1;
+    const size_t row0 = nlev > 0 ? (size_t)__ldcg(t.rbase + tile) : 0;
+    auto entry = [&](int q) -> size_t {
+        return row0 + (size_t)(fwd ? q : nlev - 1 - q) * kTwLines + (size_t)tid;
+    };
+    for (int q = 0; q < kTwDepth; ++q) tw_stage<MODE>(t, sh, tid, q < nlev ? entry(q) : 0, q < nlev, q);
     double carry = 0.0;   // the value of this line's previous cell (the -x / +x predecessor)
     uint8_t carry_m = 0;  // its neighbour mask (factorisation)
     const double TAU = 0.97, SIGMA = 0.25;
@@ -433,11 +435,10 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     if (timing && (tid == 0 || tid == 32)) t_loop = clock64();
     for (int s = s_first; s <= s_last; ++s) {
         const int L = fwd ? s : nlevels - 1 - s;
-        if (fresh) {
-            fresh = false;
-            cp_wait_n<kTwDepth - 1>();
-            L0 = ord < count ? (int)(sh.icm[ord % kTwDepth][tid] & 0xffffu) + jk : -1;
-        }
+        const int q = s - s_first;
+        const int slot = q % kTwDepth;
+        cp_wait_n<kTwDepth - 1>();
+        const uint32_t word = sh.icm[slot][tid];
         if (timing && tid == 0 && nby >= 0) {
             const long long w0 = clock64();
             tw_wait(t, sh, 0, (unsigned long long)s);
@@ -458,16 +459,15 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
         if (tid == 0 && ((s - s_first) & 7) == 0) st_release_cta_sh(&sh.mine, (unsigned long long)s);
         const int wp = (s - 1) & 1, wc = s & 1, rs = s % kTwRing;
         const int i = L - jk;
-        if (L != L0) {
+        const size_t ent = entry(q);
+        if (word == kTwNoCell) {
             if (i >= 0 && i < nx) {  // no cell here: the downstream entry still gets written
                 if (ex_y) st_relaxed_gpu_f64(ex_y + i, 0.0);
                 if (ex_z) st_relaxed_gpu_f64(ex_z + i, 0.0);
             }
-            cp_commit();  // one group per level
+            tw_stage<MODE>(t, sh, tid, q + kTwDepth < nlev ? entry(q + kTwDepth) : 0, q + kTwDepth < nlev, q + kTwDepth);
             continue;
         }
-        const int slot = ord % kTwDepth;
-        const uint32_t word = sh.icm[slot][tid];
         const uint8_t m = (uint8_t)(word >> 16);
         const double2 rec = MODE == TW_BUILD ? make_double2(0.0, 0.0) : sh.rec[slot][tid];
         const double a0 = MODE == TW_BUILD ? (double)(word >> 24) : rec.x;  // diag, r or q
@@ -505,8 +505,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
                             dmul(TAU, dadd(dadd(mx, my), mz)));
             if (e < dmul(SIGMA, diag)) e = diag;
             const double pc = e > 0.0 ? ddiv(1.0, __dsqrt_rn(e)) : 0.0;
-            t.rp[cur].y = pc;
-            t.qp[cur].y = pc;
+            t.rp[ent].y = pc;
+            t.qp[ent].y = pc;
             sh.v[wc][tid] = pc;
             sh.m[wc][tid] = m;
             carry = pc;
@@ -521,7 +521,7 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
             if (m >> NB_MZ & 1) tt = dadd(tt, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid - kTwJ]);
             const double qv = dmul(tt, b0);
             const double pqv = dmul(b0, qv);
-            t.qp[cur].x = qv;
+            t.qp[ent].x = qv;
             sh.v[wc][tid] = pqv;
             carry = pqv;
             if (ex_y) st_relaxed_gpu_f64(ex_y + i, pqv);
@@ -534,18 +534,16 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
             if (m >> NB_PY & 1) tt = dadd(tt, dmul(pc, yb ? sh.ring[0][rs][lk] : sh.v[wp][tid + 1]));
             if (m >> NB_PZ & 1) tt = dadd(tt, dmul(pc, zb ? sh.ring[1][rs][lj] : sh.v[wp][tid + kTwJ]));
             const double zv = dmul(tt, pc);
-            t.z_c[cur] = zv;
-            if (a.exact_dots) a.prod[cur] = dmul(zv, __ldcg(&t.rp[cur].x));
+            t.zr[ent] = zv;
+            if (a.exact_dots)  // the reference dot order is over cells in cell order
+                a.prod[__ldcg(t.coff + ((size_t)k * t.ny + j) * (size_t)nx + i)] = dmul(zv, __ldcg(&t.rp[ent].x));
             sh.v[wc][tid] = zv;
             carry = zv;
             if (ex_y) st_relaxed_gpu_f64(ex_y + i, zv);
             if (ex_z) st_relaxed_gpu_f64(ex_z + i, zv);
         }
-        // the slot's values are in registers: it takes the cell kTwDepth ahead
-        tw_stage<MODE>(t, sh, tid, first, step, count, ord + kTwDepth);
-        ++ord;
-        cur += step;
-        fresh = true;
+        // the slot's values are in registers: it takes the level kTwDepth ahead
+        tw_stage<MODE>(t, sh, tid, q + kTwDepth < nlev ? entry(q + kTwDepth) : 0, q + kTwDepth < nlev, q + kTwDepth);
     }
     cp_wait_n<0>();  // nothing in flight into the slots the next sweep reuses
     tw_bar();
@@ -624,20 +622,61 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
     }
     if (!tw_grid_max(t, sh, mx, parity, residual)) goto out;
     if (residual > a.tol) {
-        // cell-order tables, r and p, and the tiles' level ranges
+        // r and p, the cell-order words, and the tiles' level ranges
         for (uint32_t i = gt; i < nf; i += G) {
-            const int c = a.cinv[i];
             const uint32_t cell = a.lv_cell[i];
             const int ii = (int)(cell % (uint32_t)t.nx), jj = (int)((cell / (uint32_t)t.nx) % (uint32_t)t.ny),
                       kk = (int)(cell / ((uint32_t)t.nx * (uint32_t)t.ny));
-            t.icm[c] = (uint32_t)ii | (uint32_t)a.nmask[i] << 16 | (uint32_t)a.diag[i] << 24;
-            const double bv = a.b[i];
-            t.rp[c].x = bv;
-            a.r[i] = bv;
+            t.icm_c[a.cinv[i]] = (uint32_t)ii | (uint32_t)a.nmask[i] << 16 | (uint32_t)a.diag[i] << 24;
+            a.r[i] = a.b[i];
             a.p[i] = 0.0;
             const int tile = jj / kTwJ + (kk / kTwK) * t.tj;
             atomicMin(t.tlo + tile, ii + jj + kk);
             atomicMax(t.thi + tile, ii + jj + kk);
+        }
+        if (!tw_grid_sync(t, sh)) goto out;
+        // each tile's first row entry: a prefix over the tiles' level counts (one warp)
+        if (blockIdx.x == 0 && threadIdx.x < 32) {
+            unsigned long long run = 0;
+            for (int b0 = 0; b0 < t.ntiles; b0 += 32) {
+                const int q = b0 + lane;
+                unsigned long long n = 0;
+                if (q < t.ntiles) {
+                    const int lo = __ldcg(t.tlo + q), hi = __ldcg(t.thi + q);
+                    n = hi >= lo ? (unsigned long long)(hi - lo + 1) * kTwLines : 0ull;
+                }
+                unsigned long long x = n;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (q < t.ntiles) t.rbase[q] = (uint32_t)(run + x - n);
+                run += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) {
+                t.rbase[t.ntiles] = (uint32_t)min(run, (unsigned long long)t.rows_cap);
+                if (run > (unsigned long long)t.rows_cap) atomicOr(t.err, kTwErrWait);  // cannot happen: sized per tile
+            }
+        }
+        if (!tw_grid_sync(t, sh)) goto out;
+        {  // rows: every entry without a cell, then every cell's entry
+            const size_t nrow = __ldcg(t.rbase + t.ntiles);
+            for (size_t q = gt; q < nrow; q += G) t.icm[q] = kTwNoCell;
+        }
+        if (!tw_grid_sync(t, sh)) goto out;
+        for (uint32_t i = gt; i < nf; i += G) {
+            const uint32_t cell = a.lv_cell[i];
+            const int ii = (int)(cell % (uint32_t)t.nx), jj = (int)((cell / (uint32_t)t.nx) % (uint32_t)t.ny),
+                      kk = (int)(cell / ((uint32_t)t.nx * (uint32_t)t.ny));
+            const int tile = jj / kTwJ + (kk / kTwK) * t.tj;
+            const size_t e = (size_t)__ldcg(t.rbase + tile) +
+                             (size_t)(ii + jj + kk - __ldcg(t.tlo + tile)) * kTwLines +
+                             (size_t)((kk % kTwK) * kTwJ + jj % kTwJ);
+            if (e >= t.rows_cap) continue;  // cannot happen: the ranges were sized above
+            t.icm[e] = (uint32_t)ii | (uint32_t)a.nmask[i] << 16 | (uint32_t)a.diag[i] << 24;
+            t.rp[e].x = a.b[i];
+            t.tpos[i] = (uint32_t)e;
         }
         if (!tw_grid_sync(t, sh)) goto out;
         if (!tw_sweep_all<TW_BUILD>(t, sh, nlevels)) goto out;
@@ -654,14 +693,14 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 double acc = 0.0;
                 const uint32_t e = min((tl + 1) * kTile, nf);
                 for (uint32_t i = tl * kTile + lane; i < e; i += 32)
-                    acc = dadd(acc, dmul(__ldcg(t.z_c + a.cinv[i]), __ldcg(a.r + i)));
+                    acc = dadd(acc, dmul(__ldcg(t.zr + t.tpos[i]), __ldcg(a.r + i)));
                 acc = warp_tree_sum(acc);
                 if (lane == 0) a.tpart[tl] = acc;
             }
             if (!tw_grid_sync(t, sh)) goto out;
             sigma = tw_tile_total(t, ntile, sh);
         }
-        for (uint32_t i = gt; i < nf; i += G) a.s[i] = __ldcg(t.z_c + a.cinv[i]);
+        for (uint32_t i = gt; i < nf; i += G) a.s[i] = __ldcg(t.zr + t.tpos[i]);
         if (!tw_grid_sync(t, sh)) goto out;
         for (int it = 0; it < a.max_iters; ++it) {
             iters = it + 1;
@@ -709,7 +748,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 a.p[i] = dadd(a.p[i], dmul(alpha, __ldcg(a.s + i)));
                 const double rv = dsub(a.r[i], dmul(alpha, __ldcg(a.as + i)));
                 a.r[i] = rv;
-                t.rp[a.cinv[i]].x = rv;
+                t.rp[t.tpos[i]].x = rv;
                 mr = fmax(mr, fabs(rv));
             }
             if (!tw_grid_max(t, sh, mr, parity, residual)) goto out;  // also publishes r and rp.x
@@ -726,7 +765,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                     double acc = 0.0;
                     const uint32_t e = min((tl + 1) * kTile, nf);
                     for (uint32_t i = tl * kTile + lane; i < e; i += 32)
-                        acc = dadd(acc, dmul(__ldcg(t.z_c + a.cinv[i]), __ldcg(a.r + i)));
+                        acc = dadd(acc, dmul(__ldcg(t.zr + t.tpos[i]), __ldcg(a.r + i)));
                     acc = warp_tree_sum(acc);
                     if (lane == 0) a.tpart[tl] = acc;
                 }
@@ -735,7 +774,7 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
                 sigma_new = tw_tile_total(t, ntile, sh);
             }
             const double beta = ddiv(sigma_new, sigma);
-            for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(t.z_c + a.cinv[i]), dmul(beta, a.s[i]));
+            for (uint32_t i = gt; i < nf; i += G) a.s[i] = dadd(__ldcg(t.zr + t.tpos[i]), dmul(beta, a.s[i]));
             if (!tw_grid_sync(t, sh)) goto out;  // s complete before the next matvec reads neighbours
             TW_SECTION(6);
             sigma = sigma_new;

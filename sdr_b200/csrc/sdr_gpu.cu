@@ -454,8 +454,9 @@ struct sdr_solver {
     uint32_t last_nf = 0;           // fluid cells of the last solve (picks the kernel under SDR_PCG_AUTO)
     double* cl_slots = nullptr;     // CTA partials of the cluster kernels
     // whole-GPU tiled solve (k_pcg_tiles), allocated on first use
-    uint32_t* tw_icm = nullptr;
+    uint32_t *tw_icm = nullptr, *tw_icm_c = nullptr, *tw_tpos = nullptr, *tw_rbase = nullptr;
     double2 *tw_rp = nullptr, *tw_qp = nullptr;
+    size_t tw_rows = 0;  // row entries of the sweeps' operand rows
     double *tw_z = nullptr, *tw_exf = nullptr, *tw_exb = nullptr,
            *tw_slots = nullptr;
     int *tw_lo = nullptr, *tw_hi = nullptr;
@@ -640,7 +641,7 @@ struct sdr_solver {
         dfree(lines_cnt, st); dfree(lv_cell, st); dfree(cflag, st); dfree(coff, st); dfree(level_start, st); dfree(pos_of_cell, st);
         dfree(nbr, st); dfree(corder, st); dfree(cinv, st); dfree(prod, st); dfree(frec, st); dfree(brec, st); dfree(chunk_start, st); dfree(diag, st); dfree(nmask, st);
         dfree(b, st); dfree(precon, st); dfree(p, st); dfree(r, st); dfree(z, st); dfree(s, st); dfree(as, st); dfree(q, st); dfree(pq, st);
-        dfree(tw_icm, st); dfree(tw_rp, st); dfree(tw_qp, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
+        dfree(tw_icm, st); dfree(tw_icm_c, st); dfree(tw_tpos, st); dfree(tw_rbase, st); dfree(tw_rp, st); dfree(tw_qp, st); dfree(tw_z, st); dfree(tw_exf, st); dfree(tw_exb, st); dfree(tw_slots, st); dfree(tw_lo, st);
         dfree(tw_hi, st); dfree(tw_bar, st);
         dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
@@ -923,7 +924,14 @@ struct sdr_solver {
         tw_tj = (g.ny + kTwJ - 1) / kTwJ;
         tw_tk = (g.nz + kTwK - 1) / kTwK;
         const size_t nt = (size_t)tw_tj * tw_tk, plane = (size_t)(kTwJ + kTwK) * g.nx;
-        dalloc(tw_icm, ncell, st); dalloc(tw_rp, ncell, st); dalloc(tw_qp, ncell, st); dalloc(tw_z, ncell, st);
+        // operand rows: a tile's levels span at most nx + kTwJ + kTwK - 2 of them
+        tw_rows = nt * (size_t)(g.nx + kTwJ + kTwK) * (size_t)kTwLines;
+        if (tw_rows >= (size_t)UINT32_MAX) {  // row entries are 32-bit
+            tw_grid = -1;
+            return false;
+        }
+        dalloc(tw_icm, tw_rows, st); dalloc(tw_rp, tw_rows, st); dalloc(tw_qp, tw_rows, st); dalloc(tw_z, tw_rows, st);
+        dalloc(tw_icm_c, ncell, st); dalloc(tw_tpos, ncell, st); dalloc(tw_rbase, nt + 1, st);
         dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st);
         dalloc(tw_lo, nt, st); dalloc(tw_hi, nt, st);
         dalloc(tw_bar, 2, st);
@@ -937,7 +945,8 @@ struct sdr_solver {
         t.nx = g.nx; t.ny = g.ny; t.nz = g.nz;
         t.tj = tw_tj; t.tk = tw_tk; t.ntiles = tw_tj * tw_tk;
         t.coff = coff;
-        t.icm = tw_icm; t.rp = tw_rp; t.qp = tw_qp; t.z_c = tw_z;
+        t.icm = tw_icm; t.rp = tw_rp; t.qp = tw_qp; t.zr = tw_z;
+        t.icm_c = tw_icm_c; t.tpos = tw_tpos; t.rbase = tw_rbase; t.rows_cap = tw_rows;
         t.exf = tw_exf; t.exb = tw_exb;
         t.tlo = tw_lo; t.thi = tw_hi;
         t.bar = tw_bar;
