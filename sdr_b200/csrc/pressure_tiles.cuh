@@ -52,6 +52,8 @@ constexpr int kTwDepth = 6;                  // cells of each line whose operand
 constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
 constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
 constexpr uint32_t kTwNoCell = 0xFFFFFFFFu;  // a row entry without a fluid cell
+constexpr int kTwFace = 16;                  // lines of a tile face (either face)
+static_assert(kTwJ == kTwFace && kTwK == kTwFace, "both tile faces hold kTwFace lines");
 
 struct TwArgs {
     PcgArgs a;                   // wavefront-order vectors, tables and dots (as k_pcg)
@@ -70,8 +72,12 @@ struct TwArgs {
     uint32_t* tpos;              // wavefront index -> row entry of its cell
     uint32_t* rbase;             // per tile: its first row entry (ntiles + 1 entries)
     size_t rows_cap;             // row entries allocated
-    double* exf;                 // forward exchange planes: per tile [kTwK][nx] (+y face) then [kTwJ][nx] (+z face)
-    double* exb;                 // backward exchange planes: the -y and -z faces
+    // Exchange planes, level-major like the rows: a tile's boundary values of
+    // its q-th level (sweep order) at rbase[tile] / kTwFace + q * kTwFace + l,
+    // l the line along the face; the z face plane follows the y face plane
+    // (rows_cap / kTwFace entries each). A level's values are one 128-byte line.
+    double* exf;                 // forward sweeps: the +y face, then the +z face
+    double* exb;                 // backward sweeps: the -y face, then the -z face
     int* tlo;                    // per tile: first and last level of its fluid cells
     int* thi;
     unsigned* bar;               // grid barrier: [0] arrivals, [1] generation
@@ -253,7 +259,7 @@ enum { TW_BUILD = 0, TW_FORWARD = 1, TW_BACKWARD = 2 };
 // (jb, k0 + l)), lanes 16-31 the z face (line (j0 + l, kb)), and publishes per
 // face how many levels are staged. The values carry their own readiness: every
 // entry of an exchange plane holds kTwEmpty until its producer writes it (the
-// planes are filled at the start of the solve), a lane polls the entries its
+// planes are filled when the solve lays out its rows), a lane polls the entries its
 // next levels need (relaxed loads, up to eight levels at a time), and resets
 // each entry it staged to kTwEmpty (the producer writes it again only in the
 // next sweep of this direction, after a grid barrier). So a hand-off costs
@@ -269,7 +275,6 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
     const int lane = threadIdx.x & 31;
     const int J = tile % t.tj, K = tile / t.tj;
     const int j0 = J * kTwJ, k0 = K * kTwK, nx = t.nx;
-    const size_t plane = (size_t)(kTwJ + kTwK) * nx;
     const int face = lane >> 4, l = lane & 15;
     const int nb = face == 0 ? nby : nbz;
     // this tile's boundary line and the producer's line beside it
@@ -278,8 +283,10 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
     const int jp = face == 0 ? (fwd ? jl - 1 : jl + 1) : jl;
     const int kp = face == 0 ? kl : (fwd ? kl - 1 : kl + 1);
     const bool line_ok = nb >= 0 && (face == 0 ? l < kTwK : l < kTwJ) && jl < t.ny && kl < t.nz;
-    const size_t row = (size_t)(face == 0 ? 0 : kTwK * nx) + (size_t)l * nx;
-    double* src = nb >= 0 ? (fwd ? t.exf : t.exb) + (size_t)nb * plane + row : nullptr;
+    // the producer's entries of this line: level q of its sweep at src + q * kTwFace
+    double* src = nb >= 0 ? (fwd ? t.exf : t.exb) + (face == 0 ? 0 : t.rows_cap / kTwFace) +
+                                (size_t)__ldcg(t.rbase + nb) / kTwFace + (size_t)l
+                          : nullptr;
     // the producer's levels in sweep order
     int pf = 1, pl = 0;
     if (line_ok) {
@@ -305,7 +312,7 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
                 const int L = fwd ? sq : nlevels - 1 - sq;
                 const int i = L - jl - kl;
                 need[u] = sq <= lim && sq - 1 >= pf && sq - 1 <= pl && i >= 0 && i < nx;
-                v[u] = need[u] ? ld_relaxed_gpu_f64(src + i) : 0.0;
+                v[u] = need[u] ? ld_relaxed_gpu_f64(src + (size_t)(sq - 1 - pf) * kTwFace) : 0.0;
             }
             int u = 0;
             for (; u < 8 && next + u <= lim; ++u) {
@@ -323,7 +330,7 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
                     }
                     sh.ringm[face][sq % kTwRing][l] = m;
                 }
-                if (need[u]) st_relaxed_gpu_u64(src + i, kTwEmpty);
+                if (need[u]) st_relaxed_gpu_u64(src + (size_t)(sq - 1 - pf) * kTwFace, kTwEmpty);
             }
             next += u;
         }
@@ -405,15 +412,6 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     const int j = J * kTwJ + lj, k = K * kTwK + lk;
     const int nx = t.nx;
     const int jk = j + k;
-    const size_t plane = (size_t)(kTwJ + kTwK) * nx;
-    double* ex_own = (fwd ? t.exf : t.exb) + (size_t)tile * plane;
-    // the lines on the downstream faces write an exchange entry at every level
-    // of the sweep (0 where the line has no cell), so the downstream tile's
-    // progress warp finds every entry it polls written
-    const bool in_grid = j < t.ny && k < t.nz;
-    double* const ex_y = in_grid && (fwd ? lj == kTwJ - 1 : lj == 0) ? ex_own + (size_t)lk * nx : nullptr;
-    double* const ex_z = in_grid && (fwd ? lk == kTwK - 1 : lk == 0) ? ex_own + (size_t)kTwK * nx + (size_t)lj * nx
-                                                                      : nullptr;
     // This line's row entries, level q of the sweep (q = s - s_first) at
     // row0 + (fwd ? q : nlev - 1 - q) * kTwLines + tid. The operands of the
     // next kTwDepth levels are in flight to shared memory at all times: level
@@ -421,6 +419,15 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
     // read the group that staged it has kTwDepth - 1 groups after it.
     const int nlev = s_last - s_first + 1;
     const size_t row0 = nlev > 0 ? (size_t)__ldcg(t.rbase + tile) : 0;
+    // the lines on the downstream faces write an exchange entry at every level
+    // of the sweep where their cell lies in the grid (0 where the line has no
+    // fluid cell), so the downstream tile's progress warp finds every entry it
+    // polls written; level q's entry of face line l is ex + q * kTwFace
+    double* const ex_own = (fwd ? t.exf : t.exb) + row0 / kTwFace;
+    const bool in_grid = j < t.ny && k < t.nz;
+    double* const ex_y = in_grid && (fwd ? lj == kTwJ - 1 : lj == 0) ? ex_own + (size_t)lk : nullptr;
+    double* const ex_z = in_grid && (fwd ? lk == kTwK - 1 : lk == 0) ? ex_own + t.rows_cap / kTwFace + (size_t)lj
+                                                                      : nullptr;
     auto entry = [&](int q) -> size_t {
         return row0 + (size_t)(fwd ? q : nlev - 1 - q) * kTwLines + (size_t)tid;
     };
@@ -462,8 +469,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
         const size_t ent = entry(q);
         if (word == kTwNoCell) {
             if (i >= 0 && i < nx) {  // no cell here: the downstream entry still gets written
-                if (ex_y) st_relaxed_gpu_f64(ex_y + i, 0.0);
-                if (ex_z) st_relaxed_gpu_f64(ex_z + i, 0.0);
+                if (ex_y) st_relaxed_gpu_f64(ex_y + (size_t)q * kTwFace, 0.0);
+                if (ex_z) st_relaxed_gpu_f64(ex_z + (size_t)q * kTwFace, 0.0);
             }
             tw_stage<MODE>(t, sh, tid, q + kTwDepth < nlev ? entry(q + kTwDepth) : 0, q + kTwDepth < nlev, q + kTwDepth);
             continue;
@@ -511,8 +518,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
             sh.m[wc][tid] = m;
             carry = pc;
             carry_m = m;
-            if (ex_y) st_relaxed_gpu_f64(ex_y + i, pc);
-            if (ex_z) st_relaxed_gpu_f64(ex_z + i, pc);
+            if (ex_y) st_relaxed_gpu_f64(ex_y + (size_t)q * kTwFace, pc);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + (size_t)q * kTwFace, pc);
         } else if (MODE == TW_FORWARD) {
             // t = r + pq[-x] + pq[-y] + pq[-z]; q = t * pc (pcg_apply_mic0, forward)
             double tt = a0;
@@ -524,8 +531,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
             t.qp[ent].x = qv;
             sh.v[wc][tid] = pqv;
             carry = pqv;
-            if (ex_y) st_relaxed_gpu_f64(ex_y + i, pqv);
-            if (ex_z) st_relaxed_gpu_f64(ex_z + i, pqv);
+            if (ex_y) st_relaxed_gpu_f64(ex_y + (size_t)q * kTwFace, pqv);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + (size_t)q * kTwFace, pqv);
         } else {
             // t = q + pc z[+x] + pc z[+y] + pc z[+z]; z = t * pc (pcg_apply_mic0, backward)
             const double pc = b0;
@@ -539,8 +546,8 @@ __device__ void tw_sweep(const TwArgs& t, TwShared& sh, int tile, int nlevels) {
                 a.prod[__ldcg(t.coff + ((size_t)k * t.ny + j) * (size_t)nx + i)] = dmul(zv, __ldcg(&t.rp[ent].x));
             sh.v[wc][tid] = zv;
             carry = zv;
-            if (ex_y) st_relaxed_gpu_f64(ex_y + i, zv);
-            if (ex_z) st_relaxed_gpu_f64(ex_z + i, zv);
+            if (ex_y) st_relaxed_gpu_f64(ex_y + (size_t)q * kTwFace, zv);
+            if (ex_z) st_relaxed_gpu_f64(ex_z + (size_t)q * kTwFace, zv);
         }
         // the slot's values are in registers: it takes the level kTwDepth ahead
         tw_stage<MODE>(t, sh, tid, q + kTwDepth < nlev ? entry(q + kTwDepth) : 0, q + kTwDepth < nlev, q + kTwDepth);
@@ -611,15 +618,6 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
         t.tlo[q] = INT32_MAX;
         t.thi[q] = -1;
     }
-    {  // every exchange entry unwritten (the grid barrier below orders this before the sweeps)
-        const size_t ne = (size_t)t.ntiles * (size_t)(kTwJ + kTwK) * (size_t)t.nx;
-        unsigned long long* ef = reinterpret_cast<unsigned long long*>(t.exf);
-        unsigned long long* eb = reinterpret_cast<unsigned long long*>(t.exb);
-        for (size_t q = gt; q < ne; q += G) {
-            ef[q] = kTwEmpty;
-            eb[q] = kTwEmpty;
-        }
-    }
     if (!tw_grid_max(t, sh, mx, parity, residual)) goto out;
     if (residual > a.tol) {
         // r and p, the cell-order words, and the tiles' level ranges
@@ -660,9 +658,18 @@ __global__ void __launch_bounds__(kTwBS, 2) k_pcg_tiles(TwArgs t) {
             }
         }
         if (!tw_grid_sync(t, sh)) goto out;
-        {  // rows: every entry without a cell, then every cell's entry
+        {  // rows: every entry without a cell, then every cell's entry; every exchange entry unwritten
             const size_t nrow = __ldcg(t.rbase + t.ntiles);
             for (size_t q = gt; q < nrow; q += G) t.icm[q] = kTwNoCell;
+            const size_t nex = nrow / kTwFace, xf = t.rows_cap / kTwFace;
+            unsigned long long* ef = reinterpret_cast<unsigned long long*>(t.exf);
+            unsigned long long* eb = reinterpret_cast<unsigned long long*>(t.exb);
+            for (size_t q = gt; q < nex; q += G) {
+                ef[q] = kTwEmpty;
+                ef[xf + q] = kTwEmpty;
+                eb[q] = kTwEmpty;
+                eb[xf + q] = kTwEmpty;
+            }
         }
         if (!tw_grid_sync(t, sh)) goto out;
         for (uint32_t i = gt; i < nf; i += G) {

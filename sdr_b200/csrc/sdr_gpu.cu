@@ -923,7 +923,7 @@ struct sdr_solver {
         tw_grid = nsm * std::min(occ, 2);
         tw_tj = (g.ny + kTwJ - 1) / kTwJ;
         tw_tk = (g.nz + kTwK - 1) / kTwK;
-        const size_t nt = (size_t)tw_tj * tw_tk, plane = (size_t)(kTwJ + kTwK) * g.nx;
+        const size_t nt = (size_t)tw_tj * tw_tk;
         // operand rows: a tile's levels span at most nx + kTwJ + kTwK - 2 of them
         tw_rows = nt * (size_t)(g.nx + kTwJ + kTwK) * (size_t)kTwLines;
         if (tw_rows >= (size_t)UINT32_MAX) {  // row entries are 32-bit
@@ -932,7 +932,8 @@ struct sdr_solver {
         }
         dalloc(tw_icm, tw_rows, st); dalloc(tw_rp, tw_rows, st); dalloc(tw_qp, tw_rows, st); dalloc(tw_z, tw_rows, st);
         dalloc(tw_icm_c, ncell, st); dalloc(tw_tpos, ncell, st); dalloc(tw_rbase, nt + 1, st);
-        dalloc(tw_exf, nt * plane, st); dalloc(tw_exb, nt * plane, st);
+        // exchange planes: two faces of one entry per line and row level
+        dalloc(tw_exf, 2 * (tw_rows / kTwFace), st); dalloc(tw_exb, 2 * (tw_rows / kTwFace), st);
         dalloc(tw_lo, nt, st); dalloc(tw_hi, nt, st);
         dalloc(tw_bar, 2, st);
         dalloc(tw_slots, 2 * (size_t)tw_grid, st);
