@@ -554,9 +554,13 @@ __global__ void k_redist_append(Grid g, const int* __restrict__ key_cell, const 
                                 uint32_t cand_cap) { k_redist_append_body(VB{blockIdx.x, gridDim.x}, g, key_cell, count, cavity, n_dev, cap, rs, cand, cand_cap); }
 
 constexpr int kRedistTable = 4096;   // shared-memory hash slots (power of two)
+constexpr int kRedistProbes = 64;    // linear probes before a cell counts as not fitting the table
 constexpr int kRedistBS = 1024;
 constexpr int kRedistSmemCand = 8192;  // candidates sorted and replayed in shared memory
 constexpr uint32_t kResolved = 0x80000000u;  // candidate-list flag: decided (particle indices are < 2^31)
+// A shared-memory round costs about as much as one thread deciding this many
+// candidates in index order: rounds that decide fewer hand the rest to thread 0.
+constexpr uint32_t kRoundsMinDecided = 32;
 
 struct RedistArgs {
     Grid g;
@@ -565,7 +569,7 @@ struct RedistArgs {
     float4* pos;
     float4* vel;
     const int* key_cell;
-    uint32_t* count;         // histogram at sweep start (the fallback path mutates it)
+    uint32_t* count;         // histogram at sweep start (k_redist_par's rounds update it)
     const uint8_t* cavity;
     uint32_t* cand;          // candidate particles (sorted in place when short, in append order when long)
     uint32_t cand_cap;
@@ -603,9 +607,9 @@ __device__ __forceinline__ uint32_t rd_hash(uint32_t c) { return (c * 2654435761
 
 // One block per sweep: sort the candidates by particle index, insert every
 // referenced cell into a shared hash table, replay the reference's sequential
-// loop (solver.rs:476-555) on thread 0, then apply the moves (solver.rs:545-554)
-// with all threads. If the table overflows or the list is too long for shared
-// memory, thread 0 replays against the global counts (same result, slower).
+// loop (solver.rs:476-555) in rounds and on thread 0, then apply the moves
+// (solver.rs:545-554) with all threads. A list too long for shared memory, or
+// whose cells do not fit the table, goes to k_redist_par (the next launch).
 __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     extern __shared__ __align__(16) unsigned char rsm[];
     unsigned long long* tclaim = (unsigned long long*)rsm;  // kRedistTable: claim stamps of the rounds
@@ -616,6 +620,7 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     uint8_t* tcav = (uint8_t*)(slots + 7 * kRedistSmemCand);  // kRedistTable
     __shared__ int overflow;
     __shared__ uint32_t s_nm;
+    __shared__ uint32_t s_dec[2];  // candidates decided in the current and the next round
     RedistState* rs = a.rs;
     if (!rs->active) return;
     const uint32_t nc_all = rs->ncand;
@@ -663,10 +668,12 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     if (threadIdx.x == 0) {
         overflow = in_smem ? 0 : 1;
         s_nm = 0;
+        s_dec[0] = s_dec[1] = 0;
     }
     __syncthreads();
     if (in_smem) {
         for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
+            if (*(volatile int*)&overflow) break;  // the list goes to k_redist_par
             int c = a.key_cell[cl[m]];
             int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
             int nb[7] = {c, i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
@@ -676,7 +683,7 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 int slot = -1;
                 if (nb[q] >= 0) {
                     uint32_t h = rd_hash((uint32_t)nb[q]);
-                    for (int probe = 0; probe < kRedistTable; ++probe) {
+                    for (int probe = 0; probe < kRedistProbes; ++probe) {
                         int prev = atomicCAS(&tkey[h], -1, nb[q]);
                         if (prev == -1 || prev == nb[q]) {
                             slot = (int)h;
@@ -690,6 +697,10 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
             }
         }
         __syncthreads();
+        if (overflow) {  // the same in every thread: k_redist_par decides the list (in append order, unchanged)
+            if (threadIdx.x == 0) rs->par = 1;
+            return;
+        }
         for (int s = threadIdx.x; s < kRedistTable; s += blockDim.x) {
             int c = tkey[s];
             if (c >= 0) {
@@ -705,10 +716,18 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     // the slots of its neighbours below the cap with a stamp ordering lower
     // indices first, and runs once it holds all of them. The cells such
     // candidates touch are disjoint, so the moves are the sequential ones.
+    // Candidates crowded into a few cells (a fresh jet) decide about one per
+    // cell and round: once a round decides fewer than kRoundsMinDecided,
+    // thread 0 decides the pending rest in index order (below). Every
+    // candidate decided in a round held its cells against all lower pending
+    // ones, so the rest in index order sees the counts the sequential loop sees.
     const uint32_t cap = a.cap;
-    if (!overflow && a.rounds) {
+    bool finish_serial = !a.rounds;
+    if (a.rounds) {
         for (uint32_t round = 1;; ++round) {
             const unsigned long long stamp = (unsigned long long)round << 32;
+            const int rb = (int)(round & 1u);
+            uint32_t dec = 0;
             for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
                 const uint32_t p = scand[m];
                 if (p & kResolved) continue;
@@ -716,6 +735,7 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 const int s0 = sl[0];
                 if (tcnt[s0] <= cap) {  // back at the cap: stays there for this sweep
                     scand[m] = p | kResolved;
+                    ++dec;
                     continue;
                 }
                 const unsigned long long key = stamp | (unsigned long long)(0xFFFFFFFFu - m);
@@ -730,11 +750,13 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 }
                 if (!any) {  // no neighbour with room now, none later
                     scand[m] = p | kResolved;
+                    ++dec;
                     continue;
                 }
                 atomicMax(tclaim + s0, key);
             }
             __syncthreads();
+            if (threadIdx.x == 0) s_dec[rb ^ 1] = 0;  // every thread read it before the barrier above
             int pend = 0;
             for (uint32_t m = threadIdx.x; m < nc; m += blockDim.x) {
                 const uint32_t p = scand[m];
@@ -769,6 +791,7 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                     }
                 }
                 scand[m] = p | kResolved;
+                ++dec;
                 if (best < 0) continue;  // its last neighbour with room was filled this round by a lower candidate
                 tcnt[s0] -= 1;
                 tcnt[best] += 1;
@@ -776,7 +799,12 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 a.moves[2 * slot] = p;
                 a.moves[2 * slot + 1] = (uint32_t)tkey[best];
             }
+            if (dec) atomicAdd(&s_dec[rb], dec);
             if (__syncthreads_count(pend) == 0) break;
+            if (s_dec[rb] < kRoundsMinDecided) {  // the same value in every thread
+                finish_serial = true;
+                break;
+            }
             if (round > nc) {  // cannot happen: the lowest pending candidate always runs
                 if (threadIdx.x == 0) atomicOr(&rs->err, 4u);
                 break;
@@ -786,11 +814,13 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
     }
     if (threadIdx.x == 0) {
         uint32_t nm = s_nm;
-        if (!overflow && !a.rounds) {
-            // One thread in index order: cheaper than rounds when a few cells
-            // hold most candidates (a fresh jet), whose moves can only run one
-            // per round; the moves are the same.
+        if (finish_serial) {
+            // One thread in index order over the candidates no round decided
+            // (all of them without rounds): cheaper than rounds when a few
+            // cells hold most candidates (a fresh jet), whose moves can only
+            // run one per round; the moves are the same.
             for (uint32_t m = 0; m < nc; ++m) {
+                if (cl[m] & kResolved) continue;
                 const short* sl = slots + (size_t)m * 7;
                 const int s0 = sl[0];
                 if (tcnt[s0] <= cap) continue;
@@ -814,38 +844,6 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                     tcnt[best] += 1;
                     a.moves[2 * nm] = cl[m];
                     a.moves[2 * nm + 1] = (uint32_t)tkey[best];
-                    ++nm;
-                }
-            }
-        }
-        if (overflow) {
-            uint32_t* cnt = a.count;  // the histogram is not needed after this sweep
-            for (uint32_t m = 0; m < nc; ++m) {
-                int c = a.key_cell[cl[m]];
-                if (cnt[c] <= cap) continue;
-                int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
-                int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
-                             j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - g.nx * g.ny : -1,
-                             k + 1 < g.nz ? c + g.nx * g.ny : -1};
-                int best = -1;
-                double best_down = -INFINITY;
-                uint32_t best_room = 0;
-                for (int q = 0; q < 6; ++q) {
-                    int s = nb[q];
-                    if (s < 0 || !a.cavity[s] || cnt[s] >= cap) continue;
-                    uint32_t room = cap - cnt[s];
-                    double dn = a.down[q];
-                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                        best = s;
-                        best_down = dn;
-                        best_room = room;
-                    }
-                }
-                if (best >= 0) {
-                    cnt[c] -= 1;
-                    cnt[best] += 1;
-                    a.moves[2 * nm] = cl[m];
-                    a.moves[2 * nm + 1] = (uint32_t)best;
                     ++nm;
                 }
             }

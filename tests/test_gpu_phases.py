@@ -383,6 +383,106 @@ def test_redistribute_long_candidate_list_exact():
     assert d.max() < POS_TOL
 
 
+def test_redistribute_crowded_cells_exact():
+    """A jet's pile-up: 500 particles in each of three adjacent cavity cells
+    deep inside the cavity (a short list, replayed in shared memory). Each
+    round can move one candidate per crowded cell, so the first round decides
+    fewer than 32 and thread 0 decides the pending rest in index order: the
+    same moves as the reference's sequential loop (solver.rs:476-555)."""
+    gpu, orc, res = make_pair()
+    nx, ny, nz = gpu.grid_dims
+    dx = gpu.dx
+    st = gpu.stats()
+    org = np.array([st.origin.x, st.origin.y, st.origin.z])
+    cav = gpu.cavity_mask().reshape(nz, ny, nx).astype(bool)
+    inner = cav.copy()
+    for ax in range(3):
+        for sh in (-1, 1):
+            inner &= np.roll(cav, sh, axis=ax)
+    inner[:, :, :2] = inner[:, :, -2:] = False
+    row = inner[:, :, 1:-1] & inner[:, :, :-2] & inner[:, :, 2:]
+    kk, jj, ii = np.argwhere(row)[len(np.argwhere(row)) // 2]
+    cells = np.array([[ii, jj, kk], [ii + 1, jj, kk], [ii + 2, jj, kk]])
+    rng = np.random.default_rng(3)
+    pos = org + (cells.repeat(500, axis=0) + 0.5 + rng.uniform(-0.3, 0.3, (1500, 3))) * dx
+    pos = f32(pos[rng.permutation(len(pos))])
+    vel = np.zeros_like(pos)
+    gpu.set_particles(pos, vel)
+    orc.set_particles(pos, vel)
+    sync_faces(gpu, orc)
+    gpu.set_profiling(True)
+    gpu.run_phase(_lib.PHASE_REDISTRIBUTE)
+    orc.phase(oracle.PHASE_REDISTRIBUTE)
+    prof = gpu.profile()
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    moved_g = np.any(pg != pos, axis=1)
+    moved_o = np.any(po != pos, axis=1)
+    d = np.max(np.abs(pg - po), axis=1)
+    record("redistribute_crowded", {"particles": int(len(pos)), "candidates": prof["redist_candidates"],
+                                    "sweeps": prof["redist_sweeps"], "long_sweeps": prof["redist_long_sweeps"],
+                                    "moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
+                                    "max_abs_pos": float(d.max())})
+    assert prof["redist_long_sweeps"] == 0
+    assert moved_o.sum() > 20
+    assert np.array_equal(moved_g, moved_o)
+    assert d.max() < POS_TOL
+
+
+def test_redistribute_table_overflow_exact():
+    """A short list (at most 8192 candidates) whose cells do not fit the
+    replay's 4096-slot shared table: 9 to 11 particles in each of 700 cavity
+    cells three apart on every axis (4900 distinct cells with their
+    neighbours), at 0.6 mm. The replay hands the list to k_redist_par, which
+    decides it in rounds: the same moves as the reference's sequential loop."""
+    import re
+
+    from tests.gpu_common import SMOKE_TOML
+    gpu, orc, res = make_pair(re.sub(r"resolution_mm = [0-9.]+", "resolution_mm = 0.6", SMOKE_TOML))
+    nx, ny, nz = gpu.grid_dims
+    dx = gpu.dx
+    st = gpu.stats()
+    org = np.array([st.origin.x, st.origin.y, st.origin.z])
+    cav = gpu.cavity_mask().reshape(nz, ny, nx).astype(bool)
+    inner = cav.copy()
+    for ax in range(3):
+        for sh in (-1, 1):
+            inner &= np.roll(cav, sh, axis=ax)
+    lat = np.zeros_like(inner)
+    lat[1::3, 1::3, 1::3] = True
+    kji = np.argwhere(inner & lat)
+    assert len(kji) >= 700
+    rng = np.random.default_rng(5)
+    kji = kji[np.sort(rng.choice(len(kji), 700, replace=False))]
+    per = rng.integers(9, 12, size=700)
+    ijk = kji[:, ::-1].repeat(per, axis=0)
+    pos = org + (ijk + 0.5 + rng.uniform(-0.3, 0.3, (len(ijk), 3))) * dx
+    pos = f32(pos[rng.permutation(len(pos))])
+    vel = np.zeros_like(pos)
+    gpu.set_particles(pos, vel)
+    orc.set_particles(pos, vel)
+    sync_faces(gpu, orc)
+    gpu.set_profiling(True)
+    gpu.run_phase(_lib.PHASE_REDISTRIBUTE)
+    orc.phase(oracle.PHASE_REDISTRIBUTE)
+    prof = gpu.profile()
+    pg, vg = gpu.particles()
+    po, vo = orc.particles()
+    moved_g = np.any(pg != pos, axis=1)
+    moved_o = np.any(po != pos, axis=1)
+    d = np.max(np.abs(pg - po), axis=1)
+    record("redistribute_table_overflow", {"particles": int(len(pos)), "candidates": prof["redist_candidates"],
+                                           "sweeps": prof["redist_sweeps"],
+                                           "long_sweeps": prof["redist_long_sweeps"],
+                                           "moved_gpu": int(moved_g.sum()), "moved_orc": int(moved_o.sum()),
+                                           "max_abs_pos": float(d.max())})
+    assert len(pos) <= 8192
+    assert prof["redist_long_sweeps"] >= 1
+    assert moved_o.sum() >= 700
+    assert np.array_equal(moved_g, moved_o)
+    assert d.max() < POS_TOL
+
+
 SUB_POS_TOL = 1e-7      # one whole substep: particle positions, metres
 SUB_VEL_TOL = 2e-5      # velocities, relative to the largest speed
 SUB_PRESSURE_TOL = 1e-6  # pressure, relative to its largest value: the f32 faces of P2G move the RHS
