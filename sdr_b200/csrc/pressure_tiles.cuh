@@ -53,6 +53,10 @@ constexpr long long kTwWaitCycles = 1ll << 31;  // ~1.1 s at 1965 MHz
 constexpr uint32_t kTwErrWait = 16u;         // error bit: a sweep or barrier wait gave up
 constexpr uint32_t kTwNoCell = 0xFFFFFFFFu;  // a row entry without a fluid cell
 constexpr int kTwFace = 16;                  // lines of a tile face (either face)
+// Levels a progress-warp poll loads at once: more loads in flight per poll
+// slow the compute warps' shared-memory accesses on the same SM (pool solve
+// at 0.2 mm: 76.3 ms with 2, 77.1 with 4, 79.7 with 8).
+constexpr int kTwPoll = 2;
 static_assert(kTwJ == kTwFace && kTwK == kTwFace, "both tile faces hold kTwFace lines");
 
 struct TwArgs {
@@ -260,7 +264,7 @@ enum { TW_BUILD = 0, TW_FORWARD = 1, TW_BACKWARD = 2 };
 // face how many levels are staged. The values carry their own readiness: every
 // entry of an exchange plane holds kTwEmpty until its producer writes it (the
 // planes are filled when the solve lays out its rows), a lane polls the entries its
-// next levels need (relaxed loads, up to eight levels at a time), and resets
+// next levels need (relaxed loads, kTwPoll levels at a time), and resets
 // each entry it staged to kTwEmpty (the producer writes it again only in the
 // next sweep of this direction, after a grid barrier). So a hand-off costs
 // the producer's store reaching L2 and one poll, with no progress flags and no
@@ -303,11 +307,11 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
         const int mine = (int)ld_acquire_cta_sh(&sh.mine);
         const int lim = min(s_last, mine + kTwRing - 1);  // ring room
         if (next <= lim) {
-            // up to eight levels: an entry per level that needs one, loaded at once
-            double v[8];
-            bool need[8];
+            // up to kTwPoll levels: an entry per level that needs one, loaded at once
+            double v[kTwPoll];
+            bool need[kTwPoll];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < kTwPoll; ++u) {
                 const int sq = next + u;
                 const int L = fwd ? sq : nlevels - 1 - sq;
                 const int i = L - jl - kl;
@@ -315,7 +319,7 @@ __device__ void tw_progress_warp(const TwArgs& t, TwShared& sh, int tile, int nb
                 v[u] = need[u] ? ld_relaxed_gpu_f64(src + (size_t)(sq - 1 - pf) * kTwFace) : 0.0;
             }
             int u = 0;
-            for (; u < 8 && next + u <= lim; ++u) {
+            for (; u < kTwPoll && next + u <= lim; ++u) {
                 if (need[u] && __double_as_longlong(v[u]) == (long long)kTwEmpty) break;  // not written yet
                 const int sq = next + u;
                 const int L = fwd ? sq : nlevels - 1 - sq;
