@@ -581,7 +581,8 @@ struct RedistArgs {
     unsigned long long* claim;  // per cell: the latest claim stamp (k_redist_par); zero at allocation
     int rounds;                 // short lists: parallel rounds (1) or one thread in index order (0)
     double* slots;              // unused by the rounds (kept for the launch layout)
-    uint32_t* pend;             // 2 x cand_cap: the rounds' pending candidate indices, double-buffered
+    uint32_t* pend;             // 2 x cand_cap: the rounds' pending unit heads, double-buffered
+    uint32_t* bits;             // (n_upper + 31) / 32 words: the long list's particle-index bitmap
 };
 
 // A move: the particle goes near the destination centre with its index-keyed
@@ -653,9 +654,8 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
                 __syncthreads();
             }
     } else {
-        // Long lists go to k_redist_par (the next launch) in append order: its
-        // rounds order the candidates by particle index through their claim
-        // stamps, so the list needs no sort.
+        // Long lists go to k_redist_par (the next launch) in append order: it
+        // puts them in index order over all its CTAs.
         if (threadIdx.x == 0) rs->par = 1;
         return;
     }
@@ -932,14 +932,87 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
         base = 0;
         ok = team.sync() && ok;
     }
-    // The candidates still pending after a round go to the other half of
-    // `pend` (any order: a claim's stamp carries the candidate's index), so a
-    // round touches only those; the first round takes every candidate. On the
-    // whole grid, once few remain CTA 0 decides them alone (block barriers
-    // instead of grid barriers) while the others wait at the barrier below.
-    const uint32_t* pa = nullptr;
+    // ---- the list in particle-index order: a bitmap of the candidates'
+    // indices (distinct), counted per CTA chunk of words, then each CTA writes
+    // its chunk's indices in order at its offset, over the list in place
+    const uint32_t nw = (a.n_upper + 31u) / 32u;
+    for (uint32_t w = gt; w < nw; w += G) a.bits[w] = 0u;
+    ok = team.sync() && ok;
+    for (uint32_t q = gt; q < nc; q += G) {
+        const uint32_t p = a.cand[q];
+        atomicOr(a.bits + (p >> 5), 1u << (p & 31u));
+    }
+    ok = team.sync() && ok;
+    __shared__ uint32_t s_scan[kRpBS / 32 + 1];
+    const uint32_t per = (nw + (uint32_t)nct - 1u) / (uint32_t)nct;
+    const uint32_t w0 = min((uint32_t)rank * per, nw), w1 = min(w0 + per, nw);
+    const uint32_t sub = (w1 - w0 + kRpBS - 1u) / kRpBS;  // words of this thread, contiguous
+    const uint32_t tw0 = min(w0 + threadIdx.x * sub, w1), tw1 = min(tw0 + sub, w1);
+    uint32_t mine = 0;
+    for (uint32_t w = tw0; w < tw1; ++w) mine += __popc(__ldcg(a.bits + w));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = mine;  // inclusive scan of this CTA's thread counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_scan[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < kRpBS / 32; ++w) {
+            const uint32_t x = s_scan[w];
+            s_scan[w] = run;
+            run += x;
+        }
+        s_scan[kRpBS / 32] = run;  // this CTA's count
+        team.slots[rank] = (double)run;  // exact: counts are below 2^32
+    }
+    __syncthreads();
+    uint32_t at = s_scan[wid] + incl - mine;  // this thread's first position within the CTA
+    ok = team.sync() && ok;
+    if (threadIdx.x < 32) {  // this CTA's offset: the counts of the CTAs before it
+        double off = 0.0;
+        for (int r = lane; r < rank; r += 32) off += __ldcg(team.slots + r);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+        if (lane == 0) s_scan[kRpBS / 32] = (uint32_t)off;
+    }
+    __syncthreads();
+    at += s_scan[kRpBS / 32];
+    for (uint32_t w = tw0; w < tw1; ++w) {
+        uint32_t b = __ldcg(a.bits + w);
+        while (b) {
+            const int k = __ffs((int)b) - 1;
+            if (at < nc) a.cand[at] = w * 32u + (uint32_t)k;
+            ++at;
+            b &= b - 1u;
+        }
+    }
+    ok = team.sync() && ok;
+    // ---- units: a maximal run of consecutive candidates (index order) in one
+    // cell. The reference's loop (solver.rs:476-555) takes a run's candidates
+    // one after another with no other candidate between them, so a unit is
+    // decided as one: it claims its cell and its neighbours below the cap with
+    // a stamp that orders lower heads first, and once it holds every claim one
+    // thread takes its candidates in index order (the moves are the
+    // sequential ones: no lower pending unit reads or changes those cells).
+    // The first round's list is every unit's head position.
     uint32_t* pb = a.pend;
-    uint32_t na = nc;
+    for (uint32_t q = gt; q < nc; q += G) {
+        const int c = a.key_cell[a.cand[q]];
+        if (q == 0 || a.key_cell[a.cand[q - 1]] != c) pb[atomicAdd(&rs->pend_n[0], 1u)] = q;
+    }
+    ok = team.sync() && ok;
+    // The units still pending after a round go to the other half of `pend`
+    // (any order: a claim's stamp carries the head's index), so a round
+    // touches only those. On the whole grid, once few remain CTA 0 decides
+    // them alone (block barriers instead of grid barriers) while the others
+    // wait at the barrier below.
+    const uint32_t* pa = pb;
+    pb = a.pend + a.cand_cap;
+    uint32_t na = __ldcg(&rs->pend_n[0]);
     uint32_t round = 0;
     bool solo = false;
     uint32_t gt_ = gt, G_ = G;
@@ -955,7 +1028,7 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
         const unsigned long long stamp = (unsigned long long)(base + round) << 32;
         // claims (or leave the list)
         for (uint32_t q = gt_; q < na; q += G_) {
-            const uint32_t m = pa ? pa[q] : q;
+            const uint32_t m = pa[q];
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
             const int c = a.key_cell[p];
@@ -984,10 +1057,10 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
         }
         if (solo) __syncthreads();
         else ok = team.sync() && ok;
-        // candidates holding all their claims run (counts are as in the claim
+        // units holding all their claims run (counts are as in the claim
         // step); the others go on the next round's list
         for (uint32_t q = gt_; q < na; q += G_) {
-            const uint32_t m = pa ? pa[q] : q;
+            const uint32_t m = pa[q];
             const uint32_t p = a.cand[m];
             if (p & kResolved) continue;
             const int c = a.key_cell[p];
@@ -995,44 +1068,47 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
             const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / sxy;
             const int nb[6] = {i > 0 ? c - 1 : -1, i + 1 < g.nx ? c + 1 : -1, j > 0 ? c - g.nx : -1,
                                j + 1 < g.ny ? c + g.nx : -1, k > 0 ? c - sxy : -1, k + 1 < g.nz ? c + sxy : -1};
-            uint32_t cnt[6];
             bool ready = __ldcg(a.claim + c) == key;
 #pragma unroll
             for (int qq = 0; qq < 6; ++qq) {
                 const int n = nb[qq];
-                cnt[qq] = 0xFFFFFFFFu;
-                if (n >= 0 && a.cavity[n]) {
-                    cnt[qq] = __ldcg(a.count + n);
-                    if (cnt[qq] < cap && __ldcg(a.claim + n) != key) ready = false;
-                }
+                if (n >= 0 && a.cavity[n] && __ldcg(a.count + n) < cap && __ldcg(a.claim + n) != key) ready = false;
             }
             if (!ready) {
                 pb[atomicAdd(&rs->pend_n[cur], 1u)] = m;
                 continue;
             }
-            int best = -1;
-            double best_down = -INFINITY;
-            uint32_t best_room = 0;
+            // the unit's candidates in index order: a move each while the cell
+            // is above the cap and a neighbour has room (counts as they change)
+            for (uint32_t u = m; u < nc; ++u) {
+                const uint32_t pu = u == m ? p : (a.cand[u] & ~kResolved);
+                if (u != m && a.key_cell[pu] != c) break;  // the next unit
+                const uint32_t cc = __ldcg(a.count + c);
+                if (cc <= cap) break;
+                int best = -1;
+                double best_down = -INFINITY;
+                uint32_t best_room = 0;
 #pragma unroll
-            for (int qq = 0; qq < 6; ++qq) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
-                if (cnt[qq] >= cap) continue;  // full, outside the cavity, or out of bounds
-                const uint32_t room = cap - cnt[qq];
-                const double dn = a.down[qq];
-                if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                    best = nb[qq];
-                    best_down = dn;
-                    best_room = room;
+                for (int qq = 0; qq < 6; ++qq) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
+                    const int n = nb[qq];
+                    if (n < 0 || !a.cavity[n]) continue;
+                    const uint32_t cn = __ldcg(a.count + n);
+                    if (cn >= cap) continue;
+                    const uint32_t room = cap - cn;
+                    const double dn = a.down[qq];
+                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
+                        best = n;
+                        best_down = dn;
+                        best_room = room;
+                    }
                 }
+                if (best < 0) break;  // rooms only shrink within a sweep: none for the later ones either
+                a.count[c] = cc - 1u;
+                a.count[best] = __ldcg(a.count + best) + 1u;
+                const uint32_t slot = atomicAdd(&rs->nmoves_par, 1u);
+                a.moves[2 * slot] = pu;
+                a.moves[2 * slot + 1] = (uint32_t)best;
             }
-            if (best < 0) {  // its last neighbour with room was filled this round by a lower candidate
-                a.cand[m] = p | kResolved;
-                continue;
-            }
-            a.count[c] = __ldcg(a.count + c) - 1u;
-            a.count[best] = __ldcg(a.count + best) + 1u;
-            const uint32_t slot = atomicAdd(&rs->nmoves_par, 1u);
-            a.moves[2 * slot] = p;
-            a.moves[2 * slot + 1] = (uint32_t)best;
             a.cand[m] = p | kResolved;
         }
         if (solo) __syncthreads();
@@ -1043,7 +1119,7 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
         if (rank == 0 && threadIdx.x == 0) rs->pend_n[cur ^ 1] = 0u;
         pa = pb;
         pb = (pb == a.pend) ? a.pend + a.cand_cap : a.pend;
-        if (na > 0 && round > nc) {  // cannot happen: the lowest pending candidate always runs
+        if (na > 0 && round > nc) {  // cannot happen: the lowest pending unit always runs
             if (rank == 0 && threadIdx.x == 0) atomicOr(&rs->err, 4u);
             break;
         }

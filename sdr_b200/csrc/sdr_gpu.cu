@@ -417,7 +417,8 @@ struct sdr_solver {
     int4 *frec = nullptr, *brec = nullptr;
     // redistribution
     uint32_t* cand = nullptr;
-    uint32_t* rpend = nullptr;  // 2 x cand_n: pending candidates of the long-list rounds
+    uint32_t* rpend = nullptr;  // 2 x cand_n: pending units of the long-list rounds
+    uint32_t* rbits = nullptr;  // particle-index bitmap of the long-list sort: (capacity + 31) / 32 words
     size_t cand_n = 0;      // entries of `cand`
     size_t cand_limit = 0;  // sdr_solver_set_candidate_capacity (0: the particle capacity)
     uint32_t* moves = nullptr;
@@ -572,6 +573,7 @@ struct sdr_solver {
         cand_n = cand_limit ? std::min(ncap, cand_limit) : ncap;
         dalloc(cand, cand_n, st);
         dalloc(rpend, 2 * cand_n, st);
+        dalloc(rbits, (ncap + 31) / 32 + 1, st);
         dalloc(moves, ncap * 2, st);
         dalloc(lrec, ncap, st);
         dalloc(vrec, ncap, st);
@@ -645,7 +647,7 @@ struct sdr_solver {
         dfree(tw_hi, st); dfree(tw_bar, st);
         dfree(rp_slots, st); dfree(rp_bar, st);
         dfree(partials, st); dfree(p_dense, st); dfree(cl_slots, st); dfree(rclaim, st); dfree(tpart, st); dfree(p2g_list, st);
-        dfree(cand, st); dfree(rpend, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
+        dfree(cand, st); dfree(rpend, st); dfree(rbits, st); dfree(moves, st); dfree(rds, st); dfree(lrec, st); dfree(vrec, st);
         dfree(mcell, st); dfree(mpart, st); dfree(mout, st);
         if (hst) hput(hst, 1);
         if (h_epos) hput(h_epos, h_ecap);
@@ -1048,6 +1050,7 @@ struct sdr_solver {
         ra.rounds = shared_gpu ? 0 : 1;  // many scenes: spend no SM time on rounds
         ra.slots = cl_slots;
         ra.pend = rpend;
+        ra.bits = rbits;
         // A GPU of its own: long lists over every SM. On a shared GPU one CTA:
         // a cluster launch waits for a whole GPC of free SMs, which other
         // scenes' solves rarely leave.
