@@ -1078,36 +1078,59 @@ __device__ void redist_par_run(const RedistArgs& a, const Team& team) {
                 pb[atomicAdd(&rs->pend_n[cur], 1u)] = m;
                 continue;
             }
-            // the unit's candidates in index order: a move each while the cell
-            // is above the cap and a neighbour has room (counts as they change)
-            for (uint32_t u = m; u < nc; ++u) {
-                const uint32_t pu = u == m ? p : (a.cand[u] & ~kResolved);
-                if (u != m && a.key_cell[pu] != c) break;  // the next unit
-                const uint32_t cc = __ldcg(a.count + c);
-                if (cc <= cap) break;
-                int best = -1;
-                double best_down = -INFINITY;
-                uint32_t best_room = 0;
+            // The unit's candidates in index order, on its counts held in
+            // registers (the unit holds its cell and every neighbour with room;
+            // a full neighbour stays full within a sweep): each moves while the
+            // cell is above the cap and a neighbour has room, so the first
+            // min(excess, total room, unit length) move, to the neighbours the
+            // reference's rule picks as the counts change.
+            uint32_t cc = __ldcg(a.count + c);
+            uint32_t cn[6];
+            uint32_t room = 0;
 #pragma unroll
-                for (int qq = 0; qq < 6; ++qq) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
-                    const int n = nb[qq];
-                    if (n < 0 || !a.cavity[n]) continue;
-                    const uint32_t cn = __ldcg(a.count + n);
-                    if (cn >= cap) continue;
-                    const uint32_t room = cap - cn;
-                    const double dn = a.down[qq];
-                    if (best < 0 || dn > best_down || (dn == best_down && room > best_room)) {
-                        best = n;
-                        best_down = dn;
-                        best_room = room;
+            for (int qq = 0; qq < 6; ++qq) {
+                const int n = nb[qq];
+                cn[qq] = (n >= 0 && a.cavity[n]) ? __ldcg(a.count + n) : cap;  // outside: full
+                if (cn[qq] < cap) room += cap - cn[qq];
+            }
+            const uint32_t need = min(cc > cap ? cc - cap : 0u, room);
+            uint32_t nmov = need > 0 ? 1u : 0u;  // the head is a member
+            while (nmov < need && m + nmov < nc && a.key_cell[a.cand[m + nmov] & ~kResolved] == c) ++nmov;
+            if (nmov > 0) {
+                const uint32_t slot0 = atomicAdd(&rs->nmoves_par, nmov);
+                uint32_t moved = 0u;  // neighbours that received (bit per direction)
+                for (uint32_t u = 0; u < nmov; ++u) {
+                    int best = -1, best_n = -1;
+                    double best_down = -INFINITY;
+                    uint32_t best_room = 0;
+#pragma unroll
+                    for (int qq = 0; qq < 6; ++qq) {  // solver.rs:519-544: most downhill, then emptiest, then visit order
+                        if (cn[qq] >= cap) continue;
+                        const uint32_t rq = cap - cn[qq];
+                        const double dn = a.down[qq];
+                        if (best < 0 || dn > best_down || (dn == best_down && rq > best_room)) {
+                            best = qq;
+                            best_n = nb[qq];
+                            best_down = dn;
+                            best_room = rq;
+                        }
                     }
+                    if (best < 0) {  // cannot happen (each move takes one unit of the room counted above):
+                        atomicOr(&rs->err, 4u);  // the reserved slot still gets a defined move
+                        best_n = c;
+                    } else {
+#pragma unroll
+                        for (int qq = 0; qq < 6; ++qq)
+                            if (qq == best) cn[qq] += 1u;  // static indices keep cn in registers
+                        moved |= 1u << best;
+                    }
+                    a.moves[2 * (slot0 + u)] = u == 0 ? p : (a.cand[m + u] & ~kResolved);
+                    a.moves[2 * (slot0 + u) + 1] = (uint32_t)best_n;
                 }
-                if (best < 0) break;  // rooms only shrink within a sweep: none for the later ones either
-                a.count[c] = cc - 1u;
-                a.count[best] = __ldcg(a.count + best) + 1u;
-                const uint32_t slot = atomicAdd(&rs->nmoves_par, 1u);
-                a.moves[2 * slot] = pu;
-                a.moves[2 * slot + 1] = (uint32_t)best;
+                a.count[c] = cc - nmov;
+#pragma unroll
+                for (int qq = 0; qq < 6; ++qq)
+                    if (moved >> qq & 1u) a.count[nb[qq]] = cn[qq];
             }
             a.cand[m] = p | kResolved;
         }
