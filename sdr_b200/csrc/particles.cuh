@@ -571,7 +571,7 @@ struct RedistArgs {
     const int* key_cell;
     uint32_t* count;         // histogram at sweep start (k_redist_par's rounds update it)
     const uint8_t* cavity;
-    uint32_t* cand;          // candidate particles (sorted in place when short, in append order when long)
+    uint32_t* cand;          // candidate particles in append order (each decider sorts them in place)
     uint32_t cand_cap;
     uint32_t n_upper;        // bound on the particle count (and on every candidate index)
     uint32_t cap;
@@ -697,7 +697,7 @@ __device__ __forceinline__ void k_redist_replay_body(VB vb_, RedistArgs a) {
             }
         }
         __syncthreads();
-        if (overflow) {  // the same in every thread: k_redist_par decides the list (in append order, unchanged)
+        if (overflow) {  // the same in every thread: k_redist_par decides the list (a.cand is unchanged)
             if (threadIdx.x == 0) rs->par = 1;
             return;
         }
@@ -879,16 +879,17 @@ constexpr size_t kRedistSmem = (size_t)kRedistTable * 8 + (size_t)kRedistTable *
 // are below the cap (changed only by candidates that may choose them); every
 // other neighbour is full or outside the cavity for the rest of the sweep.
 // Each round every pending candidate m claims its cell and each neighbour
-// still below the cap with a stamp that orders lower particle indices first
-// (the list itself stays in append order); m runs
-// when it holds all its claims, i.e. when no lower pending candidate can
-// change what m reads or read what m changes. Those candidates run at once
-// (their cells are disjoint), which is the sequential result. Candidates whose
-// cell is back at the cap, or whose neighbours are all full, can never move
-// again and leave the list. The lowest pending candidate always runs, so the
-// rounds end; a bound on them still records an error bit if they did not.
+// still below the cap with a stamp that orders lower particle indices first;
+// m runs when it holds all its claims, i.e. when no lower pending candidate
+// can change what m reads or read what m changes. Those candidates run at
+// once (their cells are disjoint), which is the sequential result. Candidates
+// whose cell is back at the cap, or whose neighbours are all full, can never
+// move again and leave the list. The lowest pending candidate always runs, so
+// the rounds end; a bound on them still records an error bit if they did not.
+// The long-list form (redist_par_run) decides units of one cell's consecutive
+// candidates the same way.
 constexpr int kRpBS = 512;
-constexpr uint32_t kRpSoloList = 4 * kRpBS;  // pending candidates CTA 0 decides alone on the grid form
+constexpr uint32_t kRpSoloList = 4 * kRpBS;  // pending units CTA 0 decides alone on the grid form
 
 // The CTAs that decide one long list: one thread-block cluster (barrier in
 // hardware), or every CTA of a cooperative launch (a bounded grid barrier;
